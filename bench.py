@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark of the release-site hot path: simulated site-milliseconds per second.
+
+Workload (default): 4096 3D dyads of uneven size (cleft side ~U{40..120}
+nodes at 10 nm x 3 z-layers, 10..100 RyRs on a jittered 31 nm lattice),
+each coupled to a 25^3 cytosol at 40 nm with Ca, ATP and calmodulin,
+two-state power-law RyR gating, dt = 50 ns, FP32 fields with FP64 pools.
+Inputs are seeded synthetic sites (the reference ships no dataset).
+
+One bench step advances every site by --chunk time steps. `value` is timed on
+the device (CUDA events on the library's stream, max over ranks); `e2e` runs
+one batch scenario per step through the public API the way the reference's
+RunSimulations loop does (ResetSystem + InitOpening + Update, --chunk steps,
+outputs read back): host->device the per-site initial jSR Ca and opened RyR,
+device->host every RyR's mouth Ca and state.
+
+    python bench.py                      # 1 GPU
+    python bench.py --impl reference     # reference CPU classes on the host cores
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--sites", type=int, default=0, help="override the number of sites")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--path", default="auto", choices=["auto", "plain", "resident"])
+    ap.add_argument("--chunk", type=int, default=200, help="time steps per bench step")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args, rank=0):
+    from casim_b200 import configs
+    if args.config == "c1":
+        p, s = configs.config1(n_sites=args.sites or 100, seed0=1 + rank * 100000)
+        name = "2D 64x64 cleft, 20 RyR, pool cytosol (config 1 geometry)"
+    elif args.config == "c3":
+        p, s = configs.config3(n_sites=args.sites or 1024, seed=3 + rank)
+        name = "1024 2D 64x64 clefts, 50 RyR, jSR Ca ~U[0.5,1.5] mM"
+    else:
+        p, s = configs.config2(n_sites=args.sites or 4096, seed=2024 + rank)
+        name = "4096 3D dyads side~U{40..120}x3 layers, 10..100 RyR, 25^3 RD cytosol"
+    return p, s, name
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu_index=0):
+        self.samples = []
+        self.proc = None
+        self.idx = gpu_index
+
+    def __enter__(self):
+        q = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + q, "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if "Active" in s[3 + k] and "Not" not in s[3 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes_per_step(sim, sites, params):
+    """Each stored field read once and written once per node-step: cleft
+    (ions + ion-buffer pairs) plus the RD3D cytosol species."""
+    w = 4 if sim.info.precision == 1 else 8
+    F = sim.info.n_ions + sim.info.n_pairs
+    cleft = int(sim.info.total_nodes)
+    cyto = sim.S * sim.info.cyto_nodes
+    CS = sim.info.n_cyto_species if sim.info.cyto_nodes else 0
+    return 2 * w * (cleft * F + cyto * CS)
+
+
+def cpu_baseline(args, params, sites, budget_s):
+    """The CPU restatement (oracle/) on a bounded sample of the same sites,
+    all host threads (one site per thread), timed by wall clock."""
+    from oracle import oracle
+    n_threads = os.cpu_count() or 1
+    S = len(sites["nx"])
+    sample = min(S, max(n_threads, 8))
+    idx = np.arange(sample)
+    off = np.concatenate([[0], np.cumsum(sites["n_ch"])])
+    sub = {k: (v[idx] if (isinstance(v, np.ndarray) and v.shape[:1] == (S,)) else v) for k, v in sites.items()}
+    sub["ch_x"] = np.concatenate([sites["ch_x"][off[i]:off[i + 1]] for i in idx])
+    sub["ch_y"] = np.concatenate([sites["ch_y"][off[i]:off[i + 1]] for i in idx])
+    o = oracle.OracleSim(params, sub)
+    o.start(sub["first_channel"])
+    o.step(2, n_threads)
+    steps, t0 = 0, time.time()
+    n = 5
+    while time.time() - t0 < budget_s:
+        o.step(n, n_threads)
+        steps += n
+        n = min(n * 2, 200)
+    dt = time.time() - t0
+    site_ms = sample * steps * params_dt_ms(params)
+    return {"value": site_ms / dt, "unit": "site-ms/s", "cores": n_threads, "kind": "port",
+            "sample": "%d of the workload's sites x %d time steps (CPU restatement, OpenMP over sites)" % (sample, steps)}
+
+
+def params_dt_ms(params):
+    return float(params["dt, ns"]) * 1e-6
+
+
+def reference_arm(args):
+    """The reference's own CPU classes (oracle/_ref) on the host cores, on the
+    same sites. The reference has no 3D cytosol, so each site runs the
+    reference's 3D cleft (DyadRDCPU) with its well-mixed cytosol pool."""
+    from oracle import ref
+    p, s, name = workload(args)
+    dt_ms = params_dt_ms(p)
+    if not ref.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libcasim_ref.so was not built on this machine"}
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+    n_threads = os.cpu_count() or 1
+    S = len(s["nx"])
+    sample = min(S, n_threads)
+    off = np.concatenate([[0], np.cumsum(s["n_ch"])])
+    td = tempfile.mkdtemp()
+    sims = []
+    for i in range(sample):
+        q = json.loads(json.dumps(p))
+        cpath = os.path.join(td, "c%d.txt" % i)
+        np.savetxt(cpath, np.c_[s["ch_x"][off[i]:off[i + 1]], s["ch_y"][off[i]:off[i + 1]]])
+        d = q["Dyad"]
+        d["Channels"]["RyR"]["Coordinates"] = cpath
+        d["x"] = (int(s["nx"][i]) - 1) * d["dx"]
+        d["y"] = (int(s["ny"][i]) - 1) * d["dy"]
+        d["Seed"] = [int(v) for v in s["seeds"][i]]
+        if "3D" in d["Type"]:
+            d["Type"] = "CPU3D"
+        if q["Cytosol"].get("Type") != "Pool":
+            q["Cytosol"] = {"Type": "Pool", "Leak mult": 2e-06,
+                            "Buffers": q["Cytosol"].get("Buffers", {}), "SERCA": q["Cytosol"].get("SERCA", {})}
+        sim = ref.RefSim(q, 1, 1)
+        sim.start([int(s["first_channel"][i])])
+        sims.append(sim)
+    pool = ThreadPoolExecutor(max_workers=sample)
+    chunk = 20
+    # calibrate the per-step sample so the whole run stays within a few minutes
+    t0 = time.time()
+    list(pool.map(lambda x: x.step(chunk), sims))
+    per = max(time.time() - t0, 1e-3)
+    budget = 10.0
+    per_step = max(chunk, int(chunk * budget / per / max(args.steps + args.warmup, 1)))
+    for _ in range(args.warmup):
+        list(pool.map(lambda x: x.step(per_step), sims))
+    t0 = time.time()
+    for _ in range(args.steps):
+        list(pool.map(lambda x: x.step(per_step), sims))
+    dt = time.time() - t0
+    value = sample * per_step * args.steps * dt_ms / dt
+    sample_txt = "%d sites of the workload (3D clefts, reference pool cytosol) x %d time steps per step" % (sample, per_step)
+    return {
+        "impl": "reference", "metric": "simulated site-ms/s", "value": value, "unit": "site-ms/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": name, "cpu_sample": sample_txt},
+        "cpu_baseline": {"value": value, "unit": "site-ms/s", "cores": sample, "kind": "reference", "sample": sample_txt},
+        "e2e": {"value": value, "unit": "site-ms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(reference_arm(args)))
+        return
+    import torch
+    import casim_b200 as cb
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    p, s, name = workload(args, rank)
+    stream = torch.cuda.Stream()
+    sim = cb.ReleaseSiteBatch(p, s, precision=args.precision, path=args.path)
+    sim.set_stream(stream.cuda_stream)
+    sim.start(s["first_channel"])
+    dt_ms = sim.info.dt_ms
+    for _ in range(args.warmup):
+        sim.step(args.chunk)
+    sim.synchronize()
+    launches_per = sim.last_step_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kernel_ms = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for _ in range(args.steps):
+                sim.step(args.chunk)
+            ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_sites = sim.S * world
+    value = total_sites * args.chunk * args.steps * dt_ms / (ms / 1e3)
+    ok_finite, _ = sim.check_finite()
+    # per-launch kernel time of the dominant kernel (resident path: one kernel per bench step)
+    sim.step(args.chunk)
+    sim.synchronize()
+    kms = sim.last_step_ms()
+    bytes_step = algorithmic_bytes_per_step(sim, s, p)
+    peak, peak_kind = measured_peak_hbm()
+    if sim.path == "resident":
+        achieved = bytes_step * args.chunk / (kms / 1e3) / 1e9
+        kernel_name = "k_resident"
+    else:
+        achieved = bytes_step * args.chunk / (kms / 1e3) / 1e9
+        kernel_name = "plain step (k_pre+k_cyto+k_rd+k_update)"
+    result = {
+        "metric": "simulated site-ms/s", "value": value, "unit": "site-ms/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+        "config": {"workload": name, "sites_per_gpu": sim.S, "time_steps_per_bench_step": args.chunk,
+                   "dt_ns": float(p["dt, ns"]), "path": sim.path, "precision": args.precision,
+                   "l2": "state of %.2f GB per GPU is larger than the 126 MB L2" % (bytes_step / 2 / 1e9)},
+        "gpu_launches": int(launches_per * args.steps),
+        "finite": bool(ok_finite),
+        "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "note": "achieved = algorithmic bytes (2 x field bytes per node-step) / device time; the resident "
+                             "path keeps fields on chip, so this is an effective bandwidth above the HBM traffic"},
+        "clocks": clk.summary(),
+    }
+    if not args.no_e2e:
+        # batch scenarios through the public API: new initial conditions in,
+        # outputs out, as one RunSimulations batch of --chunk steps
+        rng = np.random.default_rng(7 + rank)
+        h2d = d2h = 0
+        n_e2e = max(1, min(args.steps, 5))
+        t0 = time.time()
+        for k in range(n_e2e):
+            first = rng.integers(0, np.asarray(s["n_ch"])).astype(np.int32)
+            jsr = rng.uniform(900.0, 1100.0, size=(sim.S, sim.info.n_ions))
+            sim.set_site_jsr(jsr)
+            sim.start(first)
+            sim.step(args.chunk)
+            mouth = sim.all_mouth(0)
+            states = sim.all_states()
+            h2d = first.nbytes + jsr.nbytes
+            d2h = mouth.nbytes + states.nbytes
+        el = time.time() - t0
+        result["e2e"] = {"value": total_sites * args.chunk * n_e2e * dt_ms / el, "unit": "site-ms/s",
+                         "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": n_e2e}
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            result["cpu_baseline"] = cpu_baseline(args, p, s, args.cpu_seconds)
+        except Exception as e:  # the baseline is reported, never required
+            result["cpu_baseline"] = {"error": str(e)}
+    sim.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,331 @@
+"""casim_b200: B200-native release-site hot path of CaSim.
+
+The compute runs in libcasim_b200.so (CUDA, sm_100a) behind the C ABI declared
+in include/casim_b200.h; this module is a thin ctypes mirror of it. There is no
+CPU fallback: if the library cannot be loaded every call raises.
+
+    from casim_b200 import ReleaseSiteBatch, configs
+    params, sites = configs.config1(n_sites=100)
+    sim = ReleaseSiteBatch(params, sites, precision="fp32")
+    sim.start(sites["first_channel"])
+    sim.step(20000)               # 1 ms at dt = 50 ns
+    ca = sim.field(0, 0)          # Ca of site 0, reference node order
+"""
+import ctypes
+import json
+import os
+
+import numpy as np
+
+from . import configs  # noqa: F401
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcasim_b200.so")
+
+OK, EINVAL, ECUDA, ENOMEM, EUNSTABLE, ETIMEOUT, ENONFINITE, EUNSUPPORTED = range(8)
+FP64, FP32 = 0, 1
+PATH_AUTO, PATH_PLAIN, PATH_RESIDENT = 0, 1, 2
+_STATUS = {OK: "OK", EINVAL: "EINVAL", ECUDA: "ECUDA", ENOMEM: "ENOMEM", EUNSTABLE: "EUNSTABLE",
+           ETIMEOUT: "ETIMEOUT", ENONFINITE: "ENONFINITE", EUNSUPPORTED: "EUNSUPPORTED"}
+
+# every extern "C" symbol of include/casim_b200.h
+EXPORTS = (
+    "casim_b200_create", "casim_b200_destroy", "casim_b200_info", "casim_b200_species_name",
+    "casim_b200_last_error", "casim_b200_set_stream", "casim_b200_reset", "casim_b200_init_opening",
+    "casim_b200_update", "casim_b200_start", "casim_b200_step", "casim_b200_synchronize",
+    "casim_b200_get_field", "casim_b200_set_field", "casim_b200_get_mouth", "casim_b200_get_states",
+    "casim_b200_get_jsr", "casim_b200_get_total_current", "casim_b200_get_efflux", "casim_b200_get_cyto",
+    "casim_b200_get_cyto_field", "casim_b200_get_draws", "casim_b200_get_release", "casim_b200_check_finite",
+    "casim_b200_get_all_mouth", "casim_b200_get_all_states", "casim_b200_last_step_ms",
+    "casim_b200_last_step_launches", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
+)
+
+
+class CasimError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (_STATUS.get(status, str(status)), message))
+        self.status = status
+
+
+class SiteTable(ctypes.Structure):
+    _fields_ = [
+        ("n_sites", ctypes.c_int32),
+        ("nx", ctypes.POINTER(ctypes.c_int32)), ("ny", ctypes.POINTER(ctypes.c_int32)),
+        ("nz", ctypes.POINTER(ctypes.c_int32)), ("n_channels", ctypes.POINTER(ctypes.c_int32)),
+        ("ch_x", ctypes.POINTER(ctypes.c_double)), ("ch_y", ctypes.POINTER(ctypes.c_double)),
+        ("seeds", ctypes.POINTER(ctypes.c_uint32)), ("jsr_init", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [
+        ("n_sites", ctypes.c_int32), ("dim", ctypes.c_int32), ("n_ions", ctypes.c_int32),
+        ("n_pairs", ctypes.c_int32), ("n_buffers", ctypes.c_int32), ("n_cyto_species", ctypes.c_int32),
+        ("cyto_nodes", ctypes.c_int32), ("precision", ctypes.c_int32), ("path", ctypes.c_int32),
+        ("max_channels", ctypes.c_int32), ("total_nodes", ctypes.c_int64), ("dt_ms", ctypes.c_double),
+        ("element_volume", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libcasim_b200.so; raise if it is missing (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libcasim_b200.so is not built; run `python -m casim_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+        dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)
+        for name in EXPORTS:
+            getattr(L, name).restype = ctypes.c_int
+        L.casim_b200_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(SiteTable), ctypes.POINTER(vp)]
+        L.casim_b200_destroy.argtypes = [vp]
+        L.casim_b200_info.argtypes = [vp, ctypes.POINTER(Info)]
+        L.casim_b200_species_name.argtypes = [vp, i32, ctypes.c_char_p, ctypes.c_size_t]
+        L.casim_b200_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+        L.casim_b200_set_stream.argtypes = [vp, vp]
+        L.casim_b200_reset.argtypes = [vp]
+        L.casim_b200_init_opening.argtypes = [vp, i32, i32]
+        L.casim_b200_update.argtypes = [vp]
+        L.casim_b200_start.argtypes = [vp, ip]
+        L.casim_b200_step.argtypes = [vp, i64]
+        L.casim_b200_synchronize.argtypes = [vp]
+        for f in ("get_field", "get_mouth", "get_cyto_field"):
+            getattr(L, "casim_b200_" + f).argtypes = [vp, i32, i32, dp]
+        L.casim_b200_set_field.argtypes = [vp, i32, i32, dp]
+        L.casim_b200_get_states.argtypes = [vp, i32, ip]
+        for f in ("get_jsr", "get_total_current", "get_efflux", "get_cyto", "get_release"):
+            getattr(L, "casim_b200_" + f).argtypes = [vp, i32, dp]
+        L.casim_b200_get_draws.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_uint64)]
+        L.casim_b200_check_finite.argtypes = [vp, ip]
+        L.casim_b200_get_all_mouth.argtypes = [vp, i32, dp]
+        L.casim_b200_get_all_states.argtypes = [vp, ip]
+        L.casim_b200_last_step_ms.argtypes = [vp, dp]
+        L.casim_b200_last_step_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.casim_b200_debug_rng.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]
+        L.casim_b200_set_site_jsr.argtypes = [vp, dp]
+        _lib = L
+    return _lib
+
+
+def last_error(h=None):
+    buf = ctypes.create_string_buffer(4096)
+    lib().casim_b200_last_error(h, buf, 4096)
+    return buf.value.decode()
+
+
+def _p(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def debug_rng(seed, n):
+    """n runif() draws of an MRG32k3a stream, generated on the device."""
+    s = np.ascontiguousarray(seed, dtype=np.uint32)
+    out = np.zeros(n, dtype=np.float64)
+    st = lib().casim_b200_debug_rng(_p(s, ctypes.c_uint32), n, _p(out, ctypes.c_double))
+    if st:
+        raise CasimError(st, last_error())
+    return out
+
+
+class ReleaseSiteBatch:
+    """A batch of independent release sites on the current CUDA device.
+
+    Mirrors the reference's compartment interfaces for the RD path:
+    DyadSeries (CaSim/DyadSeries.h:9-44), SRSeries (CaSim/SRSeries.h:7-16),
+    CytosolSeries (CaSim/CytosolSeries.h:10-21), NSRSeries (CaSim/NSRSeries.h:5-12),
+    stepped together as ParallelHybridSolver does (CaSim/ParallelHybridSolver.cpp:519-548).
+    """
+
+    def __init__(self, params, sites=None, precision="fp64", path="auto", base_dir=None):
+        L = lib()
+        self.params = params
+        prec = {"fp64": FP64, "fp32": FP32}[precision]
+        pth = {"auto": PATH_AUTO, "plain": PATH_PLAIN, "resident": PATH_RESIDENT}[path]
+        self._keep = []
+        tab = None
+        if sites is not None:
+            tab = SiteTable()
+            S = len(sites["nx"])
+            tab.n_sites = S
+
+            def arr(key, dt, ct):
+                v = sites.get(key)
+                if v is None:
+                    return None
+                a = np.ascontiguousarray(v, dtype=dt).reshape(-1)
+                self._keep.append(a)
+                return _p(a, ct)
+            tab.nx = arr("nx", np.int32, ctypes.c_int32)
+            tab.ny = arr("ny", np.int32, ctypes.c_int32)
+            tab.nz = arr("nz", np.int32, ctypes.c_int32)
+            tab.n_channels = arr("n_ch", np.int32, ctypes.c_int32)
+            tab.ch_x = arr("ch_x", np.float64, ctypes.c_double)
+            tab.ch_y = arr("ch_y", np.float64, ctypes.c_double)
+            tab.seeds = arr("seeds", np.uint32, ctypes.c_uint32)
+            tab.jsr_init = arr("jsr_init", np.float64, ctypes.c_double)
+        h = ctypes.c_void_p()
+        st = L.casim_b200_create(json.dumps(params).encode(), (base_dir or "").encode(), prec, pth,
+                                 ctypes.byref(tab) if tab is not None else None, ctypes.byref(h))
+        if st:
+            raise CasimError(st, last_error())
+        self.h = h
+        self.info = Info()
+        L.casim_b200_info(self.h, ctypes.byref(self.info))
+        self.S = self.info.n_sites
+        nch = np.zeros(self.S, dtype=np.int64)
+        if sites is not None and sites.get("n_ch") is not None:
+            nch[:] = np.asarray(sites["n_ch"])
+        else:
+            nch[:] = self.info.max_channels
+        self.n_ch = nch
+        d = params["Dyad"]
+        if sites is not None:
+            nz = sites.get("nz")
+            self._site_dims = [(int(sites["nx"][k]), int(sites["ny"][k]),
+                                int(nz[k]) if (self.info.dim == 3 and nz is not None) else 1) for k in range(self.S)]
+        else:
+            nx = int(d["x"] / d["dx"] + 1)
+            ny = int(d["y"] / d["dy"] + 1)
+            nz = int(d["z"] / d["dz"] + 1) if self.info.dim == 3 else 1
+            self._site_dims = [(nx, ny, nz)] * self.S
+
+    # -- lifecycle --------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            lib().casim_b200_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, st):
+        if st:
+            raise CasimError(st, last_error(self.h))
+
+    @property
+    def path(self):
+        return {PATH_PLAIN: "plain", PATH_RESIDENT: "resident"}.get(self.info.path, "?")
+
+    def species_name(self, k):
+        buf = ctypes.create_string_buffer(256)
+        self._ck(lib().casim_b200_species_name(self.h, k, buf, 256))
+        return buf.value.decode()
+
+    @property
+    def n_species(self):
+        return self.info.n_ions + self.info.n_pairs + self.info.n_buffers
+
+    def set_stream(self, cuda_stream):
+        """Run all work of this batch on the given cudaStream_t (an integer handle)."""
+        self._ck(lib().casim_b200_set_stream(self.h, ctypes.c_void_p(cuda_stream)))
+
+    def set_site_jsr(self, jsr_init):
+        """Initial jSR concentrations (sites x ions) for the next reset/start."""
+        v = np.ascontiguousarray(jsr_init, dtype=np.float64).reshape(self.S, self.info.n_ions)
+        self._ck(lib().casim_b200_set_site_jsr(self.h, _p(v, ctypes.c_double)))
+
+    def reset(self):
+        self._ck(lib().casim_b200_reset(self.h))
+
+    def init_opening(self, site, channel):
+        self._ck(lib().casim_b200_init_opening(self.h, site, channel))
+
+    def update(self):
+        self._ck(lib().casim_b200_update(self.h))
+
+    def start(self, first_channel=None):
+        fc = np.zeros(self.S, dtype=np.int32) if first_channel is None else np.ascontiguousarray(first_channel, dtype=np.int32)
+        self._ck(lib().casim_b200_start(self.h, _p(fc, ctypes.c_int32)))
+
+    def step(self, n):
+        self._ck(lib().casim_b200_step(self.h, int(n)))
+
+    def synchronize(self):
+        self._ck(lib().casim_b200_synchronize(self.h))
+
+    def last_step_ms(self):
+        v = ctypes.c_double()
+        self._ck(lib().casim_b200_last_step_ms(self.h, ctypes.byref(v)))
+        return v.value
+
+    def last_step_launches(self):
+        v = ctypes.c_int64()
+        self._ck(lib().casim_b200_last_step_launches(self.h, ctypes.byref(v)))
+        return v.value
+
+    # -- getters ---------------------------------------------------------
+    def field(self, site, species):
+        nx, ny, nz = self._dims(site)
+        out = np.zeros(nx * ny * nz, dtype=np.float64)
+        self._ck(lib().casim_b200_get_field(self.h, site, species, _p(out, ctypes.c_double)))
+        return out
+
+    def set_field(self, site, species, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._ck(lib().casim_b200_set_field(self.h, site, species, _p(v, ctypes.c_double)))
+
+    def _dims(self, site):
+        return self._site_dims[site]
+
+    def mouth(self, site, species):
+        out = np.zeros(int(self.n_ch[site]), dtype=np.float64)
+        self._ck(lib().casim_b200_get_mouth(self.h, site, species, _p(out, ctypes.c_double)))
+        return out
+
+    def states(self, site):
+        out = np.zeros(int(self.n_ch[site]), dtype=np.int32)
+        self._ck(lib().casim_b200_get_states(self.h, site, _p(out, ctypes.c_int32)))
+        return out
+
+    def all_states(self):
+        out = np.zeros(int(self.n_ch.sum()), dtype=np.int32)
+        self._ck(lib().casim_b200_get_all_states(self.h, _p(out, ctypes.c_int32)))
+        return out
+
+    def all_mouth(self, species):
+        out = np.zeros(int(self.n_ch.sum()), dtype=np.float64)
+        self._ck(lib().casim_b200_get_all_mouth(self.h, species, _p(out, ctypes.c_double)))
+        return out
+
+    def _vec(self, fn, site, n):
+        out = np.zeros(n, dtype=np.float64)
+        self._ck(getattr(lib(), "casim_b200_" + fn)(self.h, site, _p(out, ctypes.c_double)))
+        return out
+
+    def jsr(self, site):
+        return self._vec("get_jsr", site, self.info.n_ions)
+
+    def total_current(self, site):
+        return self._vec("get_total_current", site, self.info.n_ions)
+
+    def efflux(self, site):
+        return self._vec("get_efflux", site, self.info.n_ions + self.info.n_pairs)
+
+    def cyto(self, site):
+        return self._vec("get_cyto", site, self.info.n_cyto_species)
+
+    def cyto_field(self, site, species):
+        out = np.zeros(self.info.cyto_nodes, dtype=np.float64)
+        self._ck(lib().casim_b200_get_cyto_field(self.h, site, species, _p(out, ctypes.c_double)))
+        return out
+
+    def release(self, site):
+        return float(self._vec("get_release", site, 1)[0])
+
+    def draws(self, site):
+        v = ctypes.c_uint64()
+        self._ck(lib().casim_b200_get_draws(self.h, site, ctypes.byref(v)))
+        return int(v.value)
+
+    def check_finite(self):
+        bad = ctypes.c_int32(-1)
+        st = lib().casim_b200_check_finite(self.h, ctypes.byref(bad))
+        return st == OK, bad.value

@@ -1,0 +1,638 @@
+// C ABI of libcasim_b200.so (declared in include/casim_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/casim_b200.h"
+#include "engine.h"
+#include "parse.h"
+#include "mrg32k3a.cuh"
+#include "physics.cuh"
+
+struct casim_b200_sim {
+    cb_config cfg;
+    cb_dev d;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    int path = CASIM_PATH_PLAIN;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0;
+    long long last_launches = 0;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+thread_local std::string g_create_err;
+
+struct cuda_fail : std::runtime_error {
+    cudaError_t code;
+    cuda_fail(cudaError_t c, const std::string& w) : std::runtime_error(w + ": " + cudaGetErrorString(c)), code(c) {}
+};
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw cuda_fail(e, what);
+}
+
+template <typename T>
+T* dalloc(casim_b200_sim* h, size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) throw cuda_fail(e, "cudaMalloc");
+    h->allocs.push_back(p);
+    return (T*)p;
+}
+
+template <typename T>
+T* dupload(casim_b200_sim* h, const std::vector<T>& v) {
+    T* p = dalloc<T>(h, v.size());
+    if (!v.empty()) ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+    return p;
+}
+
+casim_status set_err(casim_b200_sim* h, casim_status s, const std::string& msg) {
+    if (h) h->err = msg;
+    else g_create_err = msg;
+    return s;
+}
+
+#define GUARD(h)                                                            \
+    if (!(h)) return CASIM_EINVAL;                                          \
+    try {
+#define END_GUARD(h)                                                        \
+    }                                                                       \
+    catch (const cuda_fail& e) {                                            \
+        return set_err(h, e.code == cudaErrorMemoryAllocation ? CASIM_ENOMEM : CASIM_ECUDA, e.what()); \
+    }                                                                       \
+    catch (const std::exception& e) {                                       \
+        return set_err(h, CASIM_EINVAL, e.what());                          \
+    }
+
+void check_site(casim_b200_sim* h, int site) {
+    if (site < 0 || site >= h->d.S) throw std::runtime_error("site index " + std::to_string(site) + " out of range");
+}
+
+// node index in the reference order for (x, y, z)
+inline long long ref_index(const cb_site& s, int dim, int x, int y, int z) {
+    return dim == 2 ? (long long)y + (long long)s.ny * x : (long long)z + (long long)s.nz * ((long long)y + (long long)s.ny * x);
+}
+
+void build_device(casim_b200_sim* h, int precision) {
+    const cb_config& cfg = h->cfg;
+    cb_dev& d = h->d;
+    d.m = cfg.m;
+    d.S = (int)cfg.sites.size();
+    d.precision = precision;
+    d.NS = cfg.m.F + cfg.m.n_buf;
+    const size_t rs = precision == 0 ? sizeof(double) : sizeof(float);
+    std::vector<cb_site> sites(d.S);
+    std::vector<int> ch_node, ch_owner;
+    std::vector<cb_site_scalars> sc(d.S);
+    std::vector<int> rim_cnode, dep_ptr, dep_term;
+    long long nb = 0;
+    int choff = 0, rimoff = 0, termoff = 0;
+    const int mc = cfg.m.mc;
+    const bool rd3d = cfg.m.cyto_type == CB_CYTO_RD3D;
+    for (int s = 0; s < d.S; ++s) {
+        const cb_site_host& sh = cfg.sites[s];
+        cb_site& st = sites[s];
+        st.nx = sh.nx;
+        st.ny = sh.ny;
+        st.nz = cfg.m.dim == 3 ? sh.nz : 1;
+        int N = st.nx * st.ny * st.nz;
+        st.npad = (N + 31) / 32 * 32;
+        st.node_base = nb;
+        nb += st.npad;
+        st.n_ch = (int)sh.ch_node_xyz.size() / 3;
+        st.ch_off = choff;
+        choff += st.n_ch;
+        d.max_nodes = std::max(d.max_nodes, st.npad);
+        d.max_ch = std::max(d.max_ch, st.n_ch);
+        int zmax = cfg.m.dim == 2 ? 1 : st.nz - 1;
+        int T = cb_efflux_terms(st.nx, st.ny, zmax);
+        d.max_terms = std::max(d.max_terms, T);
+        std::map<int, int> last_at;
+        for (int c = 0; c < st.n_ch; ++c) {
+            int x = sh.ch_node_xyz[3 * c], y = sh.ch_node_xyz[3 * c + 1], z = sh.ch_node_xyz[3 * c + 2];
+            int node = x + st.nx * (y + st.ny * z);
+            ch_node.push_back(node);
+            last_at[node] = c;
+        }
+        for (int c = 0; c < st.n_ch; ++c) ch_owner.push_back(last_at[ch_node[st.ch_off + c]] == c ? 1 : 0);
+        std::memset(&sc[s], 0, sizeof(cb_site_scalars));
+        for (int i = 0; i < CB_MAX_IONS; ++i) sc[s].jsr0[i] = sh.jsr0[i];
+        for (int i = 0; i < 6; ++i) sc[s].rng[i] = sh.seed[i];
+        if (rd3d) {
+            // rim -> nearest layer-0 cytosol node, clamped to the updated range
+            int nrim = cb_rim_count(st.nx, st.ny);
+            st.rim_off = rimoff;
+            for (int r = 0; r < nrim; ++r) {
+                int x, y;
+                cb_rim_xy(r, st.nx, st.ny, x, y);
+                double px = (x - 0.5 * (st.nx - 1)) * cfg.m.dx, py = (y - 0.5 * (st.ny - 1)) * cfg.m.dy;
+                int ci = (int)std::floor(px / cfg.m.hc + 0.5 * (mc - 1) + 0.5);
+                int cj = (int)std::floor(py / cfg.m.hc + 0.5 * (mc - 1) + 0.5);
+                ci = std::min(std::max(ci, 1), mc - 2);
+                cj = std::min(std::max(cj, 1), mc - 2);
+                rim_cnode.push_back(ci + mc * cj);
+            }
+            rimoff += nrim;
+            // deposit lists: efflux terms grouped by receiving cytosol node, term order kept
+            std::vector<std::vector<int>> lists(mc * mc);
+            for (int t = 0; t < T; ++t) {
+                int x0, y0, x1, y1, x2, y2, z;
+                cb_efflux_term(t, st.nx, st.ny, zmax, x0, y0, x1, y1, x2, y2, z);
+                int r = cb_rim_index(x0, y0, st.nx, st.ny);
+                lists[rim_cnode[st.rim_off + r]].push_back(t);
+            }
+            st.term_off = termoff;
+            int acc = 0;
+            for (int cn = 0; cn < mc * mc; ++cn) {
+                dep_ptr.push_back(acc);
+                for (int t : lists[cn]) dep_term.push_back(t);
+                acc += (int)lists[cn].size();
+            }
+            dep_ptr.push_back(acc);
+            termoff += acc;
+        }
+    }
+    d.total_nodes = nb;
+    d.total_ch = choff;
+    d.sites = dupload(h, sites);
+    d.sc = dupload(h, sc);
+    d.ch_node = dupload(h, ch_node);
+    d.ch_owner = dupload(h, ch_owner);
+    d.ch_state = dalloc<int>(h, (size_t)choff);
+    ck(cudaMemset(d.ch_state, 0, sizeof(int) * (size_t)std::max(choff, 1)), "cudaMemset");
+    d.mouth = dalloc<double>(h, (size_t)choff * d.NS);
+    ck(cudaMemset(d.mouth, 0, sizeof(double) * (size_t)std::max(choff * d.NS, 1)), "cudaMemset");
+    for (int k = 0; k < 2; ++k) d.fields[k] = dalloc<char>(h, (size_t)nb * cfg.m.F * rs);
+    d.curgrid = dalloc<char>(h, (size_t)nb * cfg.m.n_ions * rs);
+    if (rd3d) {
+        d.nc = mc * mc * mc;
+        d.CS = cfg.m.n_ions + cfg.m.c_n_pairs;
+        for (int k = 0; k < 2; ++k) d.cyto[k] = dalloc<char>(h, (size_t)d.S * d.CS * d.nc * rs);
+        d.cin = dalloc<double>(h, (size_t)d.S * d.CS * mc * mc);
+        d.rim_cnode = dupload(h, rim_cnode);
+        d.dep_ptr = dupload(h, dep_ptr);
+        d.dep_term = dupload(h, dep_term);
+    }
+    for (int w = 0; w < 2; ++w)
+        if (!cfg.sp_x[w].empty()) {
+            d.spx[w] = dupload(h, cfg.sp_x[w]);
+            d.spc[w] = dupload(h, cfg.sp_c[w]);
+        }
+    d.err_flag = dalloc<int>(h, 4);
+    ck(cudaMemset(d.err_flag, 0, 4 * sizeof(int)), "cudaMemset");
+}
+
+}  // namespace
+
+extern "C" {
+
+casim_status casim_b200_create(const char* json_text, const char* base_dir, casim_precision precision, casim_path path,
+                               const casim_site_table* sites, casim_h* out) {
+    if (!json_text || !out) return set_err(nullptr, CASIM_EINVAL, "null argument");
+    *out = nullptr;
+    if (precision != CASIM_FP64 && precision != CASIM_FP32) return set_err(nullptr, CASIM_EINVAL, "bad precision");
+    casim_b200_sim* h = new casim_b200_sim();
+    try {
+        h->cfg = cb_parse_config(json_text, base_dir ? base_dir : "", sites);
+        double cfl = cb_cfl_number(h->cfg.m);
+        if (!(cfl <= 1.0)) {
+            std::string msg = "explicit step unstable: dt*D*sum(2/h^2) = " + std::to_string(cfl) + " > 1";
+            delete h;
+            return set_err(nullptr, CASIM_EUNSTABLE, msg);
+        }
+        int dev = 0;
+        ck(cudaGetDevice(&dev), "cudaGetDevice");
+        ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        h->own_stream = true;
+        ck(cudaEventCreate(&h->ev0), "cudaEventCreate");
+        ck(cudaEventCreate(&h->ev1), "cudaEventCreate");
+        build_device(h, precision == CASIM_FP64 ? 0 : 1);
+        int thr = 0;
+        size_t smem = 0;
+        bool fits = cb_resident_fits(h->d, &thr, &smem);
+        if (path == CASIM_PATH_RESIDENT && !fits) {
+            std::string msg = "sites do not fit the resident path's shared memory";
+            casim_b200_destroy(h);
+            return set_err(nullptr, CASIM_EUNSUPPORTED, msg);
+        }
+        h->path = (path == CASIM_PATH_PLAIN || !fits) ? CASIM_PATH_PLAIN : CASIM_PATH_RESIDENT;
+        ck(cb_plain_reset(h->d, h->stream), "reset");
+        ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    } catch (const cuda_fail& e) {
+        std::string msg = e.what();
+        casim_status s = e.code == cudaErrorMemoryAllocation ? CASIM_ENOMEM : CASIM_ECUDA;
+        casim_b200_destroy(h);
+        return set_err(nullptr, s, msg);
+    } catch (const std::exception& e) {
+        std::string msg = e.what();
+        casim_b200_destroy(h);
+        return set_err(nullptr, CASIM_EINVAL, msg);
+    }
+    *out = h;
+    return CASIM_OK;
+}
+
+casim_status casim_b200_destroy(casim_h h) {
+    if (!h) return CASIM_EINVAL;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->d.rs_order) cudaFree(h->d.rs_order);
+    if (h->d.rs_counter) cudaFree(h->d.rs_counter);
+    if (h->d.rs_pow2) cudaFree(h->d.rs_pow2);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return CASIM_OK;
+}
+
+casim_status casim_b200_last_error(casim_h h, char* buf, size_t n) {
+    const std::string& e = h ? h->err : g_create_err;
+    if (buf && n) {
+        size_t k = std::min(n - 1, e.size());
+        std::memcpy(buf, e.data(), k);
+        buf[k] = 0;
+    }
+    return CASIM_OK;
+}
+
+casim_status casim_b200_info(casim_h h, casim_info* o) {
+    if (!h || !o) return CASIM_EINVAL;
+    o->n_sites = h->d.S;
+    o->dim = h->d.m.dim;
+    o->n_ions = h->d.m.n_ions;
+    o->n_pairs = h->d.m.n_pairs;
+    o->n_buffers = h->d.m.n_buf;
+    o->n_cyto_species = h->d.m.n_ions + h->d.m.c_n_pairs;
+    o->cyto_nodes = h->d.nc;
+    o->precision = h->d.precision;
+    o->path = h->path;
+    o->max_channels = h->d.max_ch;
+    long long tn = 0;
+    for (auto& s : h->cfg.sites) tn += (long long)s.nx * s.ny * (h->d.m.dim == 3 ? s.nz : 1);
+    o->total_nodes = tn;
+    o->dt_ms = h->d.m.dt;
+    o->element_volume = h->d.m.V_elem;
+    return CASIM_OK;
+}
+
+casim_status casim_b200_species_name(casim_h h, int32_t index, char* buf, size_t n) {
+    if (!h || !buf || !n) return CASIM_EINVAL;
+    std::string name;
+    const cb_config& c = h->cfg;
+    int ni = (int)c.ion_names.size(), np = (int)c.pair_names.size(), nb = (int)c.buf_names.size();
+    if (index < 0 || index >= ni + np + nb) return set_err(h, CASIM_EINVAL, "species index out of range");
+    name = index < ni ? c.ion_names[index] : index < ni + np ? c.pair_names[index - ni] : c.buf_names[index - ni - np];
+    size_t k = std::min(n - 1, name.size());
+    std::memcpy(buf, name.data(), k);
+    buf[k] = 0;
+    return CASIM_OK;
+}
+
+casim_status casim_b200_set_stream(casim_h h, void* s) {
+    if (!h) return CASIM_EINVAL;
+    cudaStreamSynchronize(h->stream);
+    if (s) {
+        if (h->own_stream) cudaStreamDestroy(h->stream);
+        h->stream = (cudaStream_t)s;
+        h->own_stream = false;
+    }
+    return CASIM_OK;
+}
+
+casim_status casim_b200_reset(casim_h h) {
+    GUARD(h)
+    ck(cb_plain_reset(h->d, h->stream), "reset");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_init_opening(casim_h h, int32_t site, int32_t channel) {
+    GUARD(h)
+    check_site(h, site);
+    int* dfirst = nullptr;
+    ck(cudaMallocAsync(&dfirst, sizeof(int), h->stream), "cudaMallocAsync");
+    ck(cudaMemcpyAsync(dfirst, &channel, sizeof(int), cudaMemcpyHostToDevice, h->stream), "cudaMemcpyAsync");
+    ck(cb_plain_init_opening(h->d, dfirst, site, site + 1, h->stream), "init_opening");
+    ck(cudaFreeAsync(dfirst, h->stream), "cudaFreeAsync");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_update(casim_h h) {
+    GUARD(h)
+    long long l = 0;
+    ck(cb_plain_update(h->d, h->stream, &l), "update");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_start(casim_h h, const int32_t* first_channel) {
+    GUARD(h)
+    if (!first_channel) throw std::runtime_error("first_channel is null");
+    ck(cb_plain_reset(h->d, h->stream), "reset");
+    int* dfirst = dalloc<int>(h, (size_t)h->d.S);
+    ck(cudaMemcpyAsync(dfirst, first_channel, sizeof(int) * h->d.S, cudaMemcpyHostToDevice, h->stream), "cudaMemcpyAsync");
+    ck(cb_plain_init_opening(h->d, dfirst, 0, h->d.S, h->stream), "init_opening");
+    long long l = 0;
+    ck(cb_plain_update(h->d, h->stream, &l), "update");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    cudaFree(dfirst);
+    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)dfirst), h->allocs.end());
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_set_site_jsr(casim_h h, const double* jsr) {
+    GUARD(h)
+    if (!jsr) throw std::runtime_error("jsr_init is null");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    std::vector<cb_site_scalars> sc(h->d.S);
+    ck(cudaMemcpy(sc.data(), h->d.sc, sizeof(cb_site_scalars) * h->d.S, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    for (int s = 0; s < h->d.S; ++s)
+        for (int i = 0; i < h->d.m.n_ions; ++i) sc[s].jsr0[i] = jsr[(size_t)s * h->d.m.n_ions + i];
+    ck(cudaMemcpy(h->d.sc, sc.data(), sizeof(cb_site_scalars) * h->d.S, cudaMemcpyHostToDevice), "cudaMemcpy");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_step(casim_h h, int64_t n) {
+    GUARD(h)
+    if (n < 0) throw std::runtime_error("negative step count");
+    long long launches = 0;
+    ck(cudaEventRecord(h->ev0, h->stream), "cudaEventRecord");
+    if (h->path == CASIM_PATH_RESIDENT) ck(cb_resident_step(h->d, n, h->stream, &launches), "resident step");
+    else ck(cb_plain_step(h->d, n, h->stream, &launches), "plain step");
+    ck(cudaEventRecord(h->ev1, h->stream), "cudaEventRecord");
+    h->last_launches = launches;
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_synchronize(casim_h h) {
+    GUARD(h)
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) h->last_ms = ms;
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_last_step_ms(casim_h h, double* out) {
+    if (!h || !out) return CASIM_EINVAL;
+    *out = h->last_ms;
+    return CASIM_OK;
+}
+
+casim_status casim_b200_last_step_launches(casim_h h, int64_t* out) {
+    if (!h || !out) return CASIM_EINVAL;
+    *out = h->last_launches;
+    return CASIM_OK;
+}
+
+casim_status casim_b200_get_field(casim_h h, int32_t site, int32_t species, double* out) {
+    GUARD(h)
+    check_site(h, site);
+    const cb_model& m = h->d.m;
+    if (species < 0 || species >= m.F + m.n_buf) throw std::runtime_error("species out of range");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    cb_site st;
+    ck(cudaMemcpy(&st, h->d.sites + site, sizeof(cb_site), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    std::vector<double> blk((size_t)m.F * st.npad);
+    size_t rs = h->d.precision == 0 ? 8 : 4;
+    std::vector<char> raw(blk.size() * rs);
+    const char* base = (const char*)h->d.fields[h->d.cur] + (size_t)st.node_base * m.F * rs;
+    ck(cudaMemcpy(raw.data(), base, raw.size(), cudaMemcpyDeviceToHost), "cudaMemcpy D2H");
+    for (size_t k = 0; k < blk.size(); ++k)
+        blk[k] = rs == 8 ? ((const double*)raw.data())[k] : (double)((const float*)raw.data())[k];
+    for (int z = 0; z < st.nz; ++z)
+        for (int y = 0; y < st.ny; ++y)
+            for (int x = 0; x < st.nx; ++x) {
+                int n = x + st.nx * (y + st.ny * z);
+                double v;
+                if (species < m.F) {
+                    v = blk[(size_t)species * st.npad + n];
+                } else {
+                    int b = species - m.F;
+                    v = m.Ctot[b];
+                    for (int p = 0; p < m.n_pairs; ++p)
+                        if (m.pair_buf[p] == b) v -= blk[(size_t)(m.n_ions + p) * st.npad + n];
+                }
+                out[ref_index(st, m.dim, x, y, z)] = v;
+            }
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_set_field(casim_h h, int32_t site, int32_t species, const double* in) {
+    GUARD(h)
+    check_site(h, site);
+    const cb_model& m = h->d.m;
+    if (species < 0 || species >= m.F) throw std::runtime_error("species out of range (stored species only)");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    cb_site st;
+    ck(cudaMemcpy(&st, h->d.sites + site, sizeof(cb_site), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    size_t rs = h->d.precision == 0 ? 8 : 4;
+    std::vector<char> raw((size_t)st.npad * rs, 0);
+    for (int z = 0; z < st.nz; ++z)
+        for (int y = 0; y < st.ny; ++y)
+            for (int x = 0; x < st.nx; ++x) {
+                int n = x + st.nx * (y + st.ny * z);
+                double v = in[ref_index(st, m.dim, x, y, z)];
+                if (rs == 8) ((double*)raw.data())[n] = v;
+                else ((float*)raw.data())[n] = (float)v;
+            }
+    char* base = (char*)h->d.fields[h->d.cur] + ((size_t)st.node_base * m.F + (size_t)species * st.npad) * rs;
+    ck(cudaMemcpy(base, raw.data(), raw.size(), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+static casim_status get_scalars(casim_h h, int32_t site, cb_site_scalars& q) {
+    check_site(h, site);
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    ck(cudaMemcpy(&q, h->d.sc + site, sizeof(cb_site_scalars), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CASIM_OK;
+}
+
+casim_status casim_b200_get_mouth(casim_h h, int32_t site, int32_t species, double* out) {
+    GUARD(h)
+    check_site(h, site);
+    if (species < 0 || species >= h->d.NS) throw std::runtime_error("species out of range");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    const cb_site_host& sh = h->cfg.sites[site];
+    int nch = (int)sh.ch_node_xyz.size() / 3;
+    cb_site st;
+    ck(cudaMemcpy(&st, h->d.sites + site, sizeof(cb_site), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    std::vector<double> mo((size_t)nch * h->d.NS);
+    ck(cudaMemcpy(mo.data(), h->d.mouth + (size_t)st.ch_off * h->d.NS, mo.size() * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    for (int c = 0; c < nch; ++c) out[c] = mo[(size_t)c * h->d.NS + species];
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_get_states(casim_h h, int32_t site, int32_t* out) {
+    GUARD(h)
+    check_site(h, site);
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    cb_site st;
+    ck(cudaMemcpy(&st, h->d.sites + site, sizeof(cb_site), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    ck(cudaMemcpy(out, h->d.ch_state + st.ch_off, sizeof(int) * st.n_ch, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_get_all_states(casim_h h, int32_t* out) {
+    GUARD(h)
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    ck(cudaMemcpy(out, h->d.ch_state, sizeof(int) * (size_t)h->d.total_ch, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_get_all_mouth(casim_h h, int32_t species, double* out) {
+    GUARD(h)
+    if (species < 0 || species >= h->d.NS) throw std::runtime_error("species out of range");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    std::vector<double> mo((size_t)h->d.total_ch * h->d.NS);
+    ck(cudaMemcpy(mo.data(), h->d.mouth, mo.size() * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    for (long long c = 0; c < h->d.total_ch; ++c) out[c] = mo[(size_t)c * h->d.NS + species];
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_get_jsr(casim_h h, int32_t site, double* out) {
+    GUARD(h)
+    cb_site_scalars q;
+    get_scalars(h, site, q);
+    for (int i = 0; i < h->d.m.n_ions; ++i) out[i] = q.jsr_new[i];
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_get_total_current(casim_h h, int32_t site, double* out) {
+    GUARD(h)
+    cb_site_scalars q;
+    get_scalars(h, site, q);
+    for (int i = 0; i < h->d.m.n_ions; ++i) out[i] = q.total[i];
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_get_efflux(casim_h h, int32_t site, double* out) {
+    GUARD(h)
+    cb_site_scalars q;
+    get_scalars(h, site, q);
+    for (int i = 0; i < h->d.m.F; ++i) out[i] = q.efflux[i];
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_get_cyto(casim_h h, int32_t site, double* out) {
+    GUARD(h)
+    cb_site_scalars q;
+    get_scalars(h, site, q);
+    for (int i = 0; i < h->d.m.n_ions; ++i) out[i] = q.c_ions[i];
+    for (int p = 0; p < h->d.m.c_n_pairs; ++p) out[h->d.m.n_ions + p] = q.c_pairs[p];
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_get_cyto_field(casim_h h, int32_t site, int32_t species, double* out) {
+    GUARD(h)
+    check_site(h, site);
+    if (h->d.m.cyto_type != CB_CYTO_RD3D) throw std::runtime_error("the cytosol is not RD3D");
+    if (species < 0 || species >= h->d.CS) throw std::runtime_error("species out of range");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    size_t rs = h->d.precision == 0 ? 8 : 4;
+    std::vector<char> raw((size_t)h->d.nc * rs);
+    const char* base = (const char*)h->d.cyto[h->d.ccur] + ((size_t)site * h->d.CS + species) * h->d.nc * rs;
+    ck(cudaMemcpy(raw.data(), base, raw.size(), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    for (int n = 0; n < h->d.nc; ++n) out[n] = rs == 8 ? ((double*)raw.data())[n] : (double)((float*)raw.data())[n];
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_get_draws(casim_h h, int32_t site, uint64_t* out) {
+    GUARD(h)
+    cb_site_scalars q;
+    get_scalars(h, site, q);
+    *out = q.draws;
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_get_release(casim_h h, int32_t site, double* out) {
+    GUARD(h)
+    cb_site_scalars q;
+    get_scalars(h, site, q);
+    *out = q.release;
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_check_finite(casim_h h, int32_t* bad_site) {
+    GUARD(h)
+    if (bad_site) *bad_site = -1;
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    const cb_model& m = h->d.m;
+    size_t rs = h->d.precision == 0 ? 8 : 4;
+    std::vector<cb_site> st(h->d.S);
+    ck(cudaMemcpy(st.data(), h->d.sites, sizeof(cb_site) * h->d.S, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    std::vector<char> raw;
+    for (int s = 0; s < h->d.S; ++s) {
+        raw.resize((size_t)st[s].npad * m.F * rs);
+        const char* base = (const char*)h->d.fields[h->d.cur] + (size_t)st[s].node_base * m.F * rs;
+        ck(cudaMemcpy(raw.data(), base, raw.size(), cudaMemcpyDeviceToHost), "cudaMemcpy");
+        size_t n = raw.size() / rs;
+        for (size_t k = 0; k < n; ++k) {
+            double v = rs == 8 ? ((double*)raw.data())[k] : (double)((float*)raw.data())[k];
+            if (!std::isfinite(v)) {
+                if (bad_site) *bad_site = s;
+                return set_err(h, CASIM_ENONFINITE, "non-finite value in site " + std::to_string(s));
+            }
+        }
+    }
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+}  // extern "C"
+
+namespace {
+__global__ void k_debug_rng(cbrng::State g, long long n, double* out) {
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (long long k = 0; k < n; ++k) out[k] = cbrng::u01d(g);
+}
+}  // namespace
+
+extern "C" casim_status casim_b200_debug_rng(const uint32_t seed[6], int64_t n, double* out) {
+    if (!seed || !out || n < 0) return set_err(nullptr, CASIM_EINVAL, "bad argument");
+    try {
+        cbrng::State g;
+        for (int i = 0; i < 6; ++i) g.s[i] = seed[i];
+        double* d = nullptr;
+        ck(cudaMalloc(&d, sizeof(double) * (size_t)std::max<int64_t>(n, 1)), "cudaMalloc");
+        k_debug_rng<<<1, 1>>>(g, n, d);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(out, d, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost);
+        cudaFree(d);
+        ck(e, "debug_rng");
+    } catch (const cuda_fail& e) {
+        return set_err(nullptr, CASIM_ECUDA, e.what());
+    }
+    return CASIM_OK;
+}

@@ -1,0 +1,57 @@
+// Device state of one batch of release sites and the launch entry points of
+// the two stepping paths. Internal to libcasim_b200.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "model.h"
+
+struct cb_dev {
+    cb_model m;
+    int S = 0;              // sites
+    int precision = 0;      // 0 = FP64 fields, 1 = FP32 fields
+    int NS = 0;             // mouth species per RyR: ions + pairs + free buffers
+    int max_nodes = 0;      // largest padded node count of a site
+    int max_ch = 0;
+    int max_terms = 0;      // largest efflux term count of a site
+    long long total_nodes = 0;  // sum of npad
+    long long total_ch = 0;
+    cb_site* sites = nullptr;         // [S]
+    cb_site_scalars* sc = nullptr;    // [S]
+    void* fields[2] = {nullptr, nullptr};  // ping-pong field storage (R = double or float)
+    int cur = 0;                      // which of fields[] holds the current state
+    void* curgrid = nullptr;          // RyR current per node (R), n_ions blocks per site
+    int* ch_node = nullptr;           // local node index (x fastest) per RyR
+    int* ch_owner = nullptr;          // 1 if the RyR is the highest-index one at its node
+    int* ch_state = nullptr;          // open (1) / closed (0)
+    double* mouth = nullptr;          // [(ch)*NS + species]
+    // RD3D cytosol
+    int nc = 0;                       // nodes per site cytosol (mc^3)
+    int CS = 0;                       // cytosol species: ions + cytosol pairs
+    void* cyto[2] = {nullptr, nullptr};  // ping-pong, [site][species][node]
+    int ccur = 0;
+    double* cin = nullptr;            // efflux deposit into layer 0, [site][species][mc*mc]
+    int* rim_cnode = nullptr;         // cytosol layer-0 node (i + mc*j) per rim entry
+    int* dep_ptr = nullptr;           // per site (mc*mc + 1) CSR offsets into dep_term
+    int* dep_term = nullptr;          // efflux term indices, oracle order
+    // spline tables
+    double* spx[2] = {nullptr, nullptr};
+    double* spc[2] = {nullptr, nullptr};
+    // bookkeeping
+    int* err_flag = nullptr;          // device-side error word
+    // resident path: work queue (sites by decreasing size), its counter and
+    // the MRG32k3a jump table A^(2^k), k < 64; allocated on first use
+    int* rs_order = nullptr;
+    int* rs_counter = nullptr;
+    unsigned long long* rs_pow2 = nullptr;
+};
+
+// plain path (plain.cu)
+cudaError_t cb_plain_reset(cb_dev& d, cudaStream_t st);
+cudaError_t cb_plain_init_opening(cb_dev& d, const int* d_first, int site_lo, int site_hi, cudaStream_t st);
+cudaError_t cb_plain_update(cb_dev& d, cudaStream_t st, long long* launches);
+cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);
+
+// resident path (resident.cu)
+bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem);
+cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);

@@ -1,0 +1,500 @@
+// Plain path: one time step = one launch sequence over HBM-resident fields.
+//
+//   k_pre     one thread per site: cytosol pool ODE (CaSim/CytosolPool.cpp:217-268),
+//             jSR pool ODE (CaSim/SRPool.cpp:70-89), two-state gating
+//             (CaSim/DyadChannels.cpp:97-130) with the site's MRG32k3a stream
+//   k_cyto    RD3D cytosol stencil (this project's 3D cytosol; no reference analog)
+//   k_rd      cleft RD step of every interior node (CaSim/DyadRD2DCPU.cpp:394-490,
+//             CaSim/DyadRDCPU.cpp:404-506), ping-pong buffers
+//   k_update  one block per site: mouth gather, Dirichlet edges, efflux,
+//             RyR currents, jSR coupling (CaSim/ParallelHybridSolver.cpp:270-286)
+//
+// This is the straightforward GPU formulation of the reference step and the
+// denominator of the resident path's speed-up; it handles any site size.
+#include <algorithm>
+
+#include "engine.h"
+#include "mrg32k3a.cuh"
+#include "physics.cuh"
+
+namespace {
+
+template <typename R>
+__global__ void k_reset(cb_model m, const cb_site* __restrict__ sites, R* __restrict__ A, R* __restrict__ B,
+                        R* __restrict__ cur, cb_site_scalars* __restrict__ sc, int* __restrict__ ch_state) {
+    const int s = blockIdx.y;
+    const cb_site st = sites[s];
+    const int F = m.F;
+    R* a = A + st.node_base * F;
+    R* b = B + st.node_base * F;
+    R* c = cur + st.node_base * m.n_ions;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < st.npad; n += gridDim.x * blockDim.x) {
+        for (int f = 0; f < F; ++f) {
+            R v = (R)(f < m.n_ions ? m.Cb[f] : m.pair_init[f - m.n_ions]);
+            a[(long long)f * st.npad + n] = v;
+            b[(long long)f * st.npad + n] = v;
+        }
+        for (int j = 0; j < m.n_ions; ++j) c[(long long)j * st.npad + n] = (R)0;
+    }
+    if (blockIdx.x == 0) {
+        for (int k = threadIdx.x; k < st.n_ch; k += blockDim.x) ch_state[st.ch_off + k] = 0;
+        if (threadIdx.x == 0) {
+            cb_site_scalars& q = sc[s];
+            for (int i = 0; i < CB_MAX_IONS; ++i) {
+                q.jsr[i] = q.jsr_new[i] = q.jsr0[i];
+                q.IjSR[i] = 0;
+                q.nsr[i] = q.jsr0[i];
+                q.total[i] = 0;
+                q.c_ions[i] = i < m.n_ions ? m.c_bg[i] : 0.0;
+            }
+            for (int k = 0; k < CB_MAX_SPECIES; ++k) q.efflux[k] = 0;
+            for (int b2 = 0; b2 < m.c_n_buf; ++b2) q.c_free[b2] = m.c_Ctot[b2];
+            for (int p = 0; p < m.c_n_pairs; ++p) {
+                q.c_pairs[p] = m.c_init[p];
+                q.c_free[m.c_pair_buf[p]] -= m.c_init[p];
+            }
+            for (int p = 0; p < m.n_pairs; ++p)
+                q.c_bnd[p] = m.dyad_c_pair[p] >= 0 ? m.c_init[m.dyad_c_pair[p]] : m.pair_init[p];
+            q.release = 0;
+        }
+    }
+}
+
+template <typename R>
+__global__ void k_cyto_reset(cb_model m, int nc, R* __restrict__ A, R* __restrict__ B, double* __restrict__ cin) {
+    const int s = blockIdx.y;
+    const int CS = m.n_ions + m.c_n_pairs;
+    const int mc2 = m.mc * m.mc;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nc; n += gridDim.x * blockDim.x)
+        for (int k = 0; k < CS; ++k) {
+            R v = (R)(k < m.n_ions ? m.c_bg[k] : m.c_init[k - m.n_ions]);
+            long long o = ((long long)s * CS + k) * nc + n;
+            A[o] = v;
+            B[o] = v;
+            if (n < mc2) cin[((long long)s * CS + k) * mc2 + n] = 0.0;
+        }
+}
+
+__global__ void k_init_open(const cb_site* __restrict__ sites, const int* __restrict__ first, int lo, int hi,
+                            cb_site_scalars* __restrict__ sc, int* __restrict__ ch_state) {
+    int s = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= hi) return;
+    const cb_site st = sites[s];
+    cb_site_scalars& q = sc[s];
+    cbrng::State g;
+    for (int i = 0; i < 6; ++i) g.s[i] = q.rng[i];
+    // CaSim/DyadChannels.cpp:83-95: one draw per channel (SetMacroState(0, .)),
+    // then one more for the channel that is opened
+    for (int c = 0; c < st.n_ch; ++c) {
+        (void)cbrng::u01d(g);
+        ch_state[st.ch_off + c] = 0;
+    }
+    (void)cbrng::u01d(g);
+    int f = first[s - lo];
+    if (f >= 0 && f < st.n_ch) ch_state[st.ch_off + f] = 1;
+    q.draws += (unsigned long long)st.n_ch + 1;
+    for (int i = 0; i < 6; ++i) q.rng[i] = g.s[i];
+}
+
+// Cytosol pool ODE of one site (CaSim/CytosolPool.cpp:217-288).
+__device__ void pool_step(const cb_model& m, cb_site_scalars& q, double dt) {
+    double evo_i[CB_MAX_IONS], evo_p[CB_MAX_CPAIRS];
+    int ipd = 0, is = 0;
+    for (int j = 0; j < m.n_ions; ++j) {
+        double react = 0;
+        for (int p = 0; p < m.c_n_pairs; ++p) {
+            if (m.c_pair_ion[p] != j) continue;
+            double R1 = m.c_koff[p] * q.c_pairs[p] - m.c_kon[p] * q.c_ions[j] * q.c_free[m.c_pair_buf[p]];
+            evo_p[p] = -R1;
+            react += R1;
+            if (m.c_in_dyad[p]) {
+                evo_p[p] += q.efflux[m.n_ions + ipd];
+                ++ipd;
+            }
+        }
+        evo_i[j] = react + q.efflux[j];
+        if (m.c_serca[j]) {
+            double i2 = q.c_ions[j] * q.c_ions[j];
+            double K2 = m.c_Kup[is] * m.c_Kup[is];
+            double b2 = m.c_bg[is] * m.c_bg[is];
+            evo_i[j] -= m.c_Jmax[is] * (i2 / (i2 + K2) - b2 / (b2 + K2));
+            ++is;
+        }
+    }
+    for (int j = 0; j < m.n_ions; ++j) {
+        evo_i[j] -= m.c_onetau_ion[j] * (q.c_ions[j] - m.c_bg[j]);
+        q.c_ions[j] += evo_i[j] * dt;
+    }
+    ipd = 0;
+    for (int p = 0; p < m.c_n_pairs; ++p) {
+        evo_p[p] -= m.c_onetau_pair[p] * (q.c_pairs[p] - m.c_init[p]);
+        q.c_pairs[p] += evo_p[p] * dt;
+        if (m.c_in_dyad[p]) q.c_bnd[ipd++] = q.c_pairs[p];
+    }
+    for (int b = 0; b < m.c_n_buf; ++b) q.c_free[b] = m.c_Ctot[b];
+    for (int p = 0; p < m.c_n_pairs; ++p) q.c_free[m.c_pair_buf[p]] -= q.c_pairs[p];
+}
+
+// jSR pool ODE of one site (CaSim/SRPool.cpp:70-89) with the site's own beta.
+__device__ __forceinline__ void jsr_step(const cb_model& m, cb_site_scalars& q, double dt) {
+    if (m.jsr_const) return;
+    double beta = 1;
+    for (int j = 0; j < m.n_ions; ++j)
+        beta += m.nCQ[j] * m.K_CQ[j] * m.CQ / ((m.K_CQ[j] + q.jsr[j]) * (m.K_CQ[j] + q.jsr[j]));
+    for (int i = 0; i < m.n_ions; ++i) {
+        double Iref = 1 / m.tau_refill[i] * (q.nsr[i] - q.jsr[i]);
+        q.jsr_new[i] = q.jsr[i] + dt / beta * (Iref - q.IjSR[i] / m.V_jsr);
+    }
+    if (m.ca_idx >= 0) q.release += q.IjSR[m.ca_idx] * dt;
+}
+
+__global__ void k_pre(cb_model m, int S, int NS, const cb_site* __restrict__ sites, cb_site_scalars* __restrict__ sc,
+                      int* __restrict__ ch_state, const double* __restrict__ mouth, const double* __restrict__ spx0,
+                      const double* __restrict__ spc0, const double* __restrict__ spx1, const double* __restrict__ spc1) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const cb_site st = sites[s];
+    cb_site_scalars& q = sc[s];
+    const double dt = m.dt;
+    if (m.cyto_type == CB_CYTO_POOL) pool_step(m, q, dt);
+    jsr_step(m, q, dt);
+    cbrng::State g;
+    for (int i = 0; i < 6; ++i) g.s[i] = q.rng[i];
+    unsigned long long draws = 0;
+    for (int c = 0; c < st.n_ch; ++c) {
+        const double* mo = mouth + (long long)(st.ch_off + c) * NS;
+        double ca = mo[m.ca_idx];
+        double mg = m.mg_idx >= 0 ? mo[m.mg_idx] : 0.0;
+        int state = ch_state[st.ch_off + c];
+        double r = cb_rate(m, spx0, spc0, spx1, spc1, state, ca, mg);
+        ++draws;
+        if (cbrng::u01d(g) < r * dt) {
+            (void)cbrng::u01d(g);
+            ++draws;
+            ch_state[st.ch_off + c] = 1 - state;
+        }
+    }
+    q.draws += draws;
+    for (int i = 0; i < 6; ++i) q.rng[i] = g.s[i];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_cyto(cb_model m, int nc, const R* __restrict__ in, R* __restrict__ out,
+                                              const double* __restrict__ cin) {
+    const int s = blockIdx.y;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nc) return;
+    const int mc = m.mc, mc2 = mc * mc;
+    const int i = n % mc, j = (n / mc) % mc, k = n / mc2;
+    if (i == 0 || i == mc - 1 || j == 0 || j == mc - 1 || k == mc - 1) return;
+    const int CS = m.n_ions + m.c_n_pairs;
+    const R* u = in + (long long)s * CS * nc;
+    R* o = out + (long long)s * CS * nc;
+    const int zl = k == 0 ? n + mc2 : n - mc2, zr = n + mc2;
+    const R ih2 = (R)m.inv_hc2;
+    R evo[CB_MAX_CSPECIES];
+    for (int c = 0; c < CS; ++c) {
+        const R* v = u + (long long)c * nc;
+        R D = (R)(c < m.n_ions ? m.D_ion[c] : m.c_D_pair[c - m.n_ions]);
+        R cc = v[n];
+        evo[c] = D * ((v[n + 1] - 2 * cc + v[n - 1]) * ih2 + (v[n + mc] - 2 * cc + v[n - mc]) * ih2 + (v[zr] - 2 * cc + v[zl]) * ih2);
+    }
+    R fr[CB_MAX_CBUF];
+    for (int b = 0; b < m.c_n_buf; ++b) fr[b] = (R)m.c_Ctot[b];
+    for (int p = 0; p < m.c_n_pairs; ++p) fr[m.c_pair_buf[p]] -= u[(long long)(m.n_ions + p) * nc + n];
+    int is = 0;
+    for (int j2 = 0; j2 < m.n_ions; ++j2) {
+        R ion = u[(long long)j2 * nc + n];
+        R react = 0;
+        for (int p = 0; p < m.c_n_pairs; ++p) {
+            if (m.c_pair_ion[p] != j2) continue;
+            R B = u[(long long)(m.n_ions + p) * nc + n];
+            R R1 = (R)m.c_koff[p] * B - (R)m.c_kon[p] * ion * fr[m.c_pair_buf[p]];
+            evo[m.n_ions + p] += -R1;
+            react += R1;
+        }
+        evo[j2] += react;
+        if (m.c_serca[j2]) {
+            R i2 = ion * ion;
+            R K2 = (R)(m.c_Kup[is] * m.c_Kup[is]);
+            R b2 = (R)(m.c_bg[is] * m.c_bg[is]);
+            evo[j2] -= (R)m.c_Jmax[is] * (i2 / (i2 + K2) - b2 / (b2 + K2));
+            ++is;
+        }
+    }
+    const R dt = (R)m.dt;
+    for (int c = 0; c < CS; ++c) {
+        R e = evo[c];
+        if (k == 0) e += (R)cin[((long long)s * CS + c) * mc2 + n];
+        o[(long long)c * nc + n] = u[(long long)c * nc + n] + e * dt;
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_rd(cb_model m, const cb_site* __restrict__ sites, const R* __restrict__ in,
+                                            R* __restrict__ out, const R* __restrict__ curg) {
+    const int s = blockIdx.y;
+    const cb_site st = sites[s];
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nxy = st.nx * st.ny;
+    if (n >= nxy * st.nz) return;
+    const int F = m.F;
+    const R* u = in + st.node_base * F;
+    R* o = out + st.node_base * F;
+    const int x = n % st.nx, y = (n / st.nx) % st.ny, z = n / nxy;
+    if (x == 0 || x == st.nx - 1 || y == 0 || y == st.ny - 1) {
+        for (int f = 0; f < F; ++f) o[(long long)f * st.npad + n] = u[(long long)f * st.npad + n];
+        return;
+    }
+    const R idx2 = (R)m.inv_dx2, idy2 = (R)m.inv_dy2, idz2 = (R)m.inv_dz2;
+    int zl = n, zr = n;
+    if (m.dim == 3) {
+        zl = z == 0 ? n + nxy : n - nxy;
+        zr = z == st.nz - 1 ? n - nxy : n + nxy;
+    }
+    R val[CB_MAX_SPECIES], evo[CB_MAX_SPECIES];
+    for (int f = 0; f < F; ++f) {
+        const R* v = u + (long long)f * st.npad;
+        R c = v[n];
+        val[f] = c;
+        R D = (R)(f < m.n_ions ? m.D_ion[f] : m.D_pair[f - m.n_ions]);
+        if (D != (R)0) {
+            R lap = (v[n + 1] - 2 * c + v[n - 1]) * idx2 + (v[n + st.nx] - 2 * c + v[n - st.nx]) * idy2;
+            if (m.dim == 3) lap = lap + (v[zr] - 2 * c + v[zl]) * idz2;
+            evo[f] = D * lap;
+        } else {
+            evo[f] = 0;
+        }
+    }
+    R fr[CB_MAX_BUF];
+    for (int b = 0; b < m.n_buf; ++b) fr[b] = (R)m.Ctot[b];
+    for (int p = 0; p < m.n_pairs; ++p) fr[m.pair_buf[p]] -= val[m.n_ions + p];
+    R Rj[CB_MAX_IONS];
+    for (int j = 0; j < m.n_ions; ++j) Rj[j] = 0;
+    for (int p = 0; p < m.n_pairs; ++p) {
+        int j = m.pair_ion[p];
+        R R1 = (R)m.koff[p] * val[m.n_ions + p] - (R)m.kon[p] * val[j] * fr[m.pair_buf[p]];
+        evo[m.n_ions + p] += -R1;
+        Rj[j] += R1;
+    }
+    const R dt = (R)m.dt;
+    const R* cg = curg + st.node_base * m.n_ions;
+    const bool sl_layer = (m.dim == 2) || (z == st.nz - 1);
+    for (int j = 0; j < m.n_ions; ++j) {
+        R e = evo[j] + Rj[j];
+        e += cg[(long long)j * st.npad + n];
+        if (sl_layer && m.has_sl[j]) {
+            R s1 = (R)m.K1[j] + val[j];
+            R s2 = (R)m.K2[j] + val[j];
+            e *= (R)1 / ((R)1 + (R)(m.N1[j] * m.K1[j]) / (s1 * s1) + (R)(m.N2[j] * m.K2[j]) / (s2 * s2));
+        }
+        o[(long long)j * st.npad + n] = val[j] + e * dt;
+    }
+    for (int p = 0; p < m.n_pairs; ++p) o[(long long)(m.n_ions + p) * st.npad + n] = val[m.n_ions + p] + evo[m.n_ions + p] * dt;
+}
+
+// Deterministic block sum of `v` (blockDim.x == 256).
+__device__ double block_sum(double v, double* red) {
+    red[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = blockDim.x >> 1; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_update(cb_model m, int NS, const cb_site* __restrict__ sites, R* __restrict__ fld,
+                                                R* __restrict__ curg, const int* __restrict__ ch_node,
+                                                const int* __restrict__ ch_owner, const int* __restrict__ ch_state,
+                                                double* __restrict__ mouth, cb_site_scalars* __restrict__ sc, int nc,
+                                                const R* __restrict__ cyto, double* __restrict__ cin,
+                                                const int* __restrict__ rim_cnode, const int* __restrict__ dep_ptr,
+                                                const int* __restrict__ dep_term) {
+    extern __shared__ double smem[];
+    double* red = smem;            // 256
+    double* terms = smem + 256;    // RD3D: max_terms * F deposit values
+    const int s = blockIdx.x;
+    const cb_site st = sites[s];
+    cb_site_scalars& q = sc[s];
+    const int F = m.F;
+    R* u = fld + st.node_base * F;
+    const int nx = st.nx, ny = st.ny, nz = st.nz, nxy = nx * ny;
+    const long long np = st.npad;
+    // 1. mouth values: ions, pairs, free buffers (CaSim/DyadRD2DCPU.cpp:361-380)
+    for (int c = threadIdx.x; c < st.n_ch; c += blockDim.x) {
+        int node = ch_node[st.ch_off + c];
+        double* mo = mouth + (long long)(st.ch_off + c) * NS;
+        double fr[CB_MAX_BUF];
+        for (int b = 0; b < m.n_buf; ++b) fr[b] = m.Ctot[b];
+        for (int f = 0; f < F; ++f) {
+            double v = (double)u[f * np + node];
+            mo[f] = v;
+            if (f >= m.n_ions) fr[m.pair_buf[f - m.n_ions]] -= v;
+        }
+        for (int b = 0; b < m.n_buf; ++b) mo[F + b] = fr[b];
+    }
+    __syncthreads();
+    // 2. Dirichlet edges from the cytosol (CaSim/DyadRD2DCPU.cpp:274-303)
+    const int nrim = cb_rim_count(nx, ny);
+    const int CS = m.n_ions + m.c_n_pairs;
+    const R* cy = cyto ? cyto + (long long)s * CS * nc : nullptr;
+    for (int t = threadIdx.x; t < nrim * nz; t += blockDim.x) {
+        int r = t % nrim, z = t / nrim, x, y;
+        cb_rim_xy(r, nx, ny, x, y);
+        int node = x + nx * y + nxy * z;
+        if (m.cyto_type == CB_CYTO_POOL) {
+            for (int j = 0; j < m.n_ions; ++j) u[j * np + node] = (R)q.c_ions[j];
+            for (int p = 0; p < m.n_pairs; ++p) u[(m.n_ions + p) * np + node] = (R)q.c_bnd[p];
+        } else {
+            int cn = rim_cnode[st.rim_off + r];
+            for (int j = 0; j < m.n_ions; ++j) u[j * np + node] = cy[(long long)j * nc + cn];
+            for (int p = 0; p < m.n_pairs; ++p) {
+                int cq = m.dyad_c_pair[p];
+                u[(m.n_ions + p) * np + node] = cq >= 0 ? cy[(long long)(m.n_ions + cq) * nc + cn] : (R)m.pair_init[p];
+            }
+        }
+    }
+    __syncthreads();
+    // 3. efflux (CaSim/DyadRD2DCPU.cpp:305-350): per-term values, block sums
+    const int zmax = m.dim == 2 ? 1 : nz - 1;
+    const int T = cb_efflux_terms(nx, ny, zmax);
+    double part[CB_MAX_SPECIES];
+    for (int f = 0; f < F; ++f) part[f] = 0;
+    const bool rd3d = m.cyto_type == CB_CYTO_RD3D;
+    for (int t = threadIdx.x; t < T; t += blockDim.x) {
+        int x0, y0, x1, y1, x2, y2, z;
+        int sel = cb_efflux_term(t, nx, ny, zmax, x0, y0, x1, y1, x2, y2, z);
+        double sf = sel == 0 ? m.sx : m.sy;
+        int n0 = x0 + nx * y0 + nxy * z, n1 = x1 + nx * y1 + nxy * z, n2 = x2 + nx * y2 + nxy * z;
+        for (int f = 0; f < F; ++f) {
+            double D = f < m.n_ions ? m.D_ion[f] : m.D_pair[f - m.n_ions];
+            double g = 2 * (double)u[f * np + n1] - 1.5 * (double)u[f * np + n0] - 0.5 * (double)u[f * np + n2];
+            if (!rd3d) {
+                part[f] += D * m.grad_mult * sf * g;
+            } else {
+                double v = D * sf * g * m.inv_hc3;
+                part[f] += v;
+                terms[(long long)t * F + f] = v;
+            }
+        }
+    }
+    for (int f = 0; f < F; ++f) {
+        double tot = block_sum(part[f], red);
+        if (threadIdx.x == 0) q.efflux[f] = tot;
+    }
+    // 4. RD3D: deposit into the cytosol layer z = 0 in term order
+    if (rd3d) {
+        __syncthreads();
+        const int mc2 = m.mc * m.mc;
+        const int* ptr = dep_ptr + (long long)s * (mc2 + 1);
+        for (int cn = threadIdx.x; cn < mc2; cn += blockDim.x) {
+            int lo = ptr[cn], hi = ptr[cn + 1];
+            for (int c = 0; c < CS; ++c) {
+                int f = c < m.n_ions ? c : m.c_dyad_pair[c - m.n_ions];
+                if (f >= 0 && c >= m.n_ions) f += m.n_ions;
+                double acc = 0;
+                if (f >= 0)
+                    for (int k = lo; k < hi; ++k) acc += terms[(long long)dep_term[st.term_off + k] * F + f];
+                cin[((long long)s * CS + c) * mc2 + cn] = acc;
+            }
+        }
+    }
+    // 5. RyR currents (CaSim/DyadRD2DCPU.cpp:243-264, CaSim/PassiveIonChannel.cpp:28-34)
+    R* cg = curg + st.node_base * m.n_ions;
+    double tot[CB_MAX_IONS];
+    for (int j = 0; j < m.n_ions; ++j) tot[j] = 0;
+    for (int c = threadIdx.x; c < st.n_ch; c += blockDim.x) {
+        int node = ch_node[st.ch_off + c];
+        int state = ch_state[st.ch_off + c];
+        for (int j = 0; j < m.n_ions; ++j) {
+            double flux = state * (m.g[j] * (q.jsr_new[j] - (double)u[j * np + node]));
+            if (ch_owner[st.ch_off + c]) cg[j * np + node] = (R)flux;
+            tot[j] += flux;
+        }
+    }
+    for (int j = 0; j < m.n_ions; ++j) {
+        double t = block_sum(tot[j], red);
+        if (threadIdx.x == 0) q.total[j] = t;
+    }
+    // 6. jSR coupling (CaSim/SRPool.cpp:55-68)
+    if (threadIdx.x == 0 && !m.jsr_const)
+        for (int i = 0; i < m.n_ions; ++i) {
+            q.IjSR[i] = q.total[i] * m.V_elem;
+            q.nsr[i] = m.nsr[i];
+            q.jsr[i] = q.jsr_new[i];
+        }
+}
+
+template <typename R>
+cudaError_t launch_update(cb_dev& d, cudaStream_t st) {
+    size_t smem = 256 * sizeof(double);
+    if (d.m.cyto_type == CB_CYTO_RD3D) smem += (size_t)d.max_terms * d.m.F * sizeof(double);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    k_update<R><<<d.S, 256, smem, st>>>(d.m, d.NS, d.sites, (R*)d.fields[d.cur], (R*)d.curgrid, d.ch_node, d.ch_owner,
+                                        d.ch_state, d.mouth, d.sc, d.nc, (const R*)d.cyto[d.ccur], d.cin, d.rim_cnode,
+                                        d.dep_ptr, d.dep_term);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_step(cb_dev& d, cudaStream_t st) {
+    k_pre<<<(d.S + 127) / 128, 128, 0, st>>>(d.m, d.S, d.NS, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0],
+                                               d.spx[1], d.spc[1]);
+    if (d.m.cyto_type == CB_CYTO_RD3D) {
+        dim3 g((d.nc + 255) / 256, d.S);
+        k_cyto<R><<<g, 256, 0, st>>>(d.m, d.nc, (const R*)d.cyto[d.ccur], (R*)d.cyto[1 - d.ccur], d.cin);
+        d.ccur ^= 1;
+    }
+    dim3 g((d.max_nodes + 255) / 256, d.S);
+    k_rd<R><<<g, 256, 0, st>>>(d.m, d.sites, (const R*)d.fields[d.cur], (R*)d.fields[1 - d.cur], (const R*)d.curgrid);
+    d.cur ^= 1;
+    return launch_update<R>(d, st);
+}
+
+template <typename R>
+cudaError_t reset_impl(cb_dev& d, cudaStream_t st) {
+    dim3 g(std::max(1, std::min(64, (d.max_nodes + 255) / 256)), d.S);
+    k_reset<R><<<g, 256, 0, st>>>(d.m, d.sites, (R*)d.fields[0], (R*)d.fields[1], (R*)d.curgrid, d.sc, d.ch_state);
+    d.cur = 0;
+    if (d.m.cyto_type == CB_CYTO_RD3D) {
+        dim3 gc((d.nc + 255) / 256, d.S);
+        k_cyto_reset<R><<<gc, 256, 0, st>>>(d.m, d.nc, (R*)d.cyto[0], (R*)d.cyto[1], d.cin);
+        d.ccur = 0;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t cb_plain_reset(cb_dev& d, cudaStream_t st) {
+    return d.precision == 0 ? reset_impl<double>(d, st) : reset_impl<float>(d, st);
+}
+
+cudaError_t cb_plain_init_opening(cb_dev& d, const int* d_first, int lo, int hi, cudaStream_t st) {
+    int n = hi - lo;
+    if (n <= 0) return cudaSuccess;
+    k_init_open<<<(n + 127) / 128, 128, 0, st>>>(d.sites, d_first, lo, hi, d.sc, d.ch_state);
+    return cudaGetLastError();
+}
+
+cudaError_t cb_plain_update(cb_dev& d, cudaStream_t st, long long* launches) {
+    if (launches) *launches += 1;
+    return d.precision == 0 ? launch_update<double>(d, st) : launch_update<float>(d, st);
+}
+
+cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* launches) {
+    const int per = 3 + (d.m.cyto_type == CB_CYTO_RD3D ? 1 : 0);
+    for (long long i = 0; i < n; ++i) {
+        cudaError_t e = d.precision == 0 ? launch_step<double>(d, st) : launch_step<float>(d, st);
+        if (e != cudaSuccess) return e;
+        if (launches) *launches += per;
+    }
+    return cudaSuccess;
+}

@@ -1,0 +1,176 @@
+/*
+ * casim_b200 — C ABI of the B200-native CaSim release-site hot path.
+ *
+ * One handle owns a batch of independent release sites (dyads) resident on one
+ * GPU: the cleft reaction-diffusion fields, RyR gating states and their
+ * MRG32k3a streams, the jSR pool and the cytosol (well-mixed pool or 3D grid).
+ * A call to casim_b200_step() advances every site by n explicit time steps
+ * entirely on the device; nothing crosses PCIe inside the time loop.
+ *
+ * Plain C types only. Every call returns a casim_status; on failure
+ * casim_b200_last_error() describes it. Handles are not thread-safe: one host
+ * thread drives one handle (the reference drives its GPU classes from one
+ * thread too, CaSim/ParallelHybridSolver.cpp:497-508).
+ *
+ * Node order used by every field getter/setter is the reference's:
+ *   2D: y + ny*x            (CaSim/DyadRD2DCPU.cpp:270-272)
+ *   3D: z + nz*(y + ny*x)   (CaSim/DyadRDCPU.cpp:277-279)
+ * Species order: ions (JSON key order), then ion-buffer pairs (ion-major,
+ * buffer-minor, CaSim/DyadRD2DCPU.cpp:83-99), then free buffers.
+ */
+#ifndef CASIM_B200_H
+#define CASIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct casim_b200_sim* casim_h;
+
+typedef enum {
+    CASIM_OK = 0,
+    CASIM_EINVAL = 1,      /* malformed JSON, bad argument, out-of-range site/channel */
+    CASIM_ECUDA = 2,       /* a CUDA runtime call failed (message carries cudaGetErrorString) */
+    CASIM_ENOMEM = 3,      /* device allocation failed */
+    CASIM_EUNSTABLE = 4,   /* explicit scheme violates dt*sum(2D/h^2) <= 1 for some species */
+    CASIM_ETIMEOUT = 5,    /* a bounded device wait gave up */
+    CASIM_ENONFINITE = 6,  /* a NaN/Inf was found in the state by casim_b200_check_finite */
+    CASIM_EUNSUPPORTED = 7 /* configuration outside this build's limits */
+} casim_status;
+
+typedef enum { CASIM_FP64 = 0, CASIM_FP32 = 1 } casim_precision;
+
+/* Which device path steps the batch.
+ * PLAIN:    one time step per launch sequence (cytosol/jSR/gating, RD stencil,
+ *           coupling), fields in HBM. Any site size.
+ * RESIDENT: each site lives in one thread block's shared memory for the whole
+ *           call; all time steps run inside one persistent launch.
+ * AUTO:     RESIDENT when every site fits, else PLAIN. */
+typedef enum { CASIM_PATH_AUTO = 0, CASIM_PATH_PLAIN = 1, CASIM_PATH_RESIDENT = 2 } casim_path;
+
+/* Optional per-site table (struct of arrays). Any NULL member falls back to
+ * the JSON: grid extents from x/dx+1, y/dy+1, z/dz+1 (CaSim/DyadRD2DCPU.cpp:17-18),
+ * RyR coordinates from the "Coordinates" file, seeds from "Seed", jSR from
+ * "jSR"/"Ions"/<ion>/"Concentration". */
+typedef struct casim_site_table {
+    int32_t n_sites;
+    const int32_t* nx;         /* grid nodes along x per site */
+    const int32_t* ny;
+    const int32_t* nz;         /* 3D only */
+    const int32_t* n_channels; /* RyRs per site */
+    const double* ch_x;        /* RyR coordinates in nm, concatenated site after site */
+    const double* ch_y;
+    const uint32_t* seeds;     /* 6 MRG32k3a seed words per site */
+    const double* jsr_init;    /* n_ions values per site */
+} casim_site_table;
+
+typedef struct casim_info {
+    int32_t n_sites;
+    int32_t dim;               /* 2 or 3 */
+    int32_t n_ions;
+    int32_t n_pairs;
+    int32_t n_buffers;
+    int32_t n_cyto_species;    /* cytosol pool: n_ions + cytosol pairs; RD3D: same, per node */
+    int32_t cyto_nodes;        /* RD3D nodes per site (mc^3), 0 for the pool */
+    int32_t precision;
+    int32_t path;              /* the path actually used */
+    int32_t max_channels;
+    int64_t total_nodes;       /* cleft nodes over all sites */
+    double dt_ms;
+    double element_volume;     /* nm^3, as DyadSeries::GetElementVolume */
+} casim_info;
+
+/* Build a batch from a reference-schema Parameters.json text.
+ * Replaces the compartment construction in ParallelHybridSolver's constructor
+ * (CaSim/ParallelHybridSolver.cpp:169-241) for the dyad, jSR, nSR and cytosol.
+ * base_dir resolves relative "Coordinates" paths (may be NULL = cwd).
+ * sites may be NULL: then "NumBatch" identical sites are built. */
+casim_status casim_b200_create(const char* json_text, const char* base_dir, casim_precision precision,
+                               casim_path path, const casim_site_table* sites, casim_h* out);
+casim_status casim_b200_destroy(casim_h h);
+casim_status casim_b200_info(casim_h h, casim_info* out);
+/* Name of species `index` (ions, pairs as "<ion>-<buffer>", free buffers). */
+casim_status casim_b200_species_name(casim_h h, int32_t index, char* buf, size_t n);
+casim_status casim_b200_last_error(casim_h h, char* buf, size_t n);
+
+/* Use this CUDA stream (a cudaStream_t) for all work of the handle; NULL = the
+ * handle's own stream. */
+casim_status casim_b200_set_stream(casim_h h, void* cuda_stream);
+
+/* Reset every compartment to its initial state.
+ * Replaces DyadSeries::Reset, SRSeries::Reset, CytosolSeries::Reset, NSRSeries::Reset
+ * (CaSim/DyadSeries.h:19, CaSim/SRSeries.h:9, CaSim/CytosolSeries.h:15, CaSim/NSRSeries.h:8). */
+casim_status casim_b200_reset(casim_h h);
+/* DyadSeries::InitOpening(site, channel) (CaSim/DyadSeries.h:20, CaSim/DyadChannels.cpp:83-95):
+ * consumes n_channels + 1 draws of the site's stream and opens `channel`. */
+casim_status casim_b200_init_opening(casim_h h, int32_t site, int32_t channel);
+/* The solver's Update() (CaSim/ParallelHybridSolver.cpp:270-286): mouth
+ * gather, Dirichlet edges, efflux, RyR currents, pool coupling. */
+casim_status casim_b200_update(casim_h h);
+/* reset + init_opening(site, first_channel[site]) for every site + update, as
+ * at the start of each batch in RunSimulations* (CaSim/ParallelHybridSolver.cpp:525-529). */
+casim_status casim_b200_start(casim_h h, const int32_t* first_channel);
+/* Per-site initial jSR concentrations (n_ions values per site) used by the
+ * next reset/start: a new batch scenario without rebuilding the handle. */
+casim_status casim_b200_set_site_jsr(casim_h h, const double* jsr_init);
+/* Advance every site by n_steps time steps: per step the cytosol, dyad RD,
+ * jSR, gating and Update of CaSim/ParallelHybridSolver.cpp:532-540.
+ * Replaces DyadSeries::RunRD + RunMC + Update, SRSeries::Run/Update and
+ * CytosolSeries::RunRD/Update for the whole batch. Asynchronous on the stream. */
+casim_status casim_b200_step(casim_h h, int64_t n_steps);
+casim_status casim_b200_synchronize(casim_h h);
+
+/* ---- getters (synchronous; copy device state to host) ---- */
+/* DyadSeries::GetConcentrations (CaSim/DyadSeries.h:29): one species of one
+ * site, reference node order, nx*ny(*nz) doubles. */
+casim_status casim_b200_get_field(casim_h h, int32_t site, int32_t species, double* out);
+/* write one species of one site (reference node order); for tests and restarts */
+casim_status casim_b200_set_field(casim_h h, int32_t site, int32_t species, const double* in);
+/* DyadSeries::GetIonsNearChannels (CaSim/DyadSeries.h:31): mouth value of
+ * `species` at every RyR of the site, as gathered by the last Update. */
+casim_status casim_b200_get_mouth(casim_h h, int32_t site, int32_t species, double* out);
+/* DyadSeries::GetChannelsStates (CaSim/DyadSeries.h:30): 0/1 per RyR. */
+casim_status casim_b200_get_states(casim_h h, int32_t site, int32_t* out);
+/* SRSeries::GetIons (CaSim/SRSeries.h:12): jSR concentration per ion. */
+casim_status casim_b200_get_jsr(casim_h h, int32_t site, double* out);
+/* DyadSeries::GetTotalSRCurrent (CaSim/DyadSeries.h:24): per ion. */
+casim_status casim_b200_get_total_current(casim_h h, int32_t site, double* out);
+/* DyadSeries::GetEffluxes (CaSim/DyadSeries.h:23): n_ions + n_pairs values. */
+casim_status casim_b200_get_efflux(casim_h h, int32_t site, double* out);
+/* CytosolSeries::GetConcentrations (CaSim/CytosolSeries.h:19) for the pool:
+ * n_ions + cytosol pairs values. */
+casim_status casim_b200_get_cyto(casim_h h, int32_t site, double* out);
+/* RD3D cytosol: one species of one site, mc^3 values, x fastest. */
+casim_status casim_b200_get_cyto_field(casim_h h, int32_t site, int32_t species, double* out);
+/* runif() draws consumed so far by the site's stream */
+casim_status casim_b200_get_draws(casim_h h, int32_t site, uint64_t* out);
+/* Ca released from the jSR so far (FP64 accumulator), in uM*nm^3 */
+casim_status casim_b200_get_release(casim_h h, int32_t site, double* out);
+
+/* Scan every field for NaN/Inf; returns CASIM_ENONFINITE and the first bad
+ * site in *bad_site (or -1). */
+casim_status casim_b200_check_finite(casim_h h, int32_t* bad_site);
+
+/* Batched host views for drop-in output (CaSim/ParallelHybridSolver.cpp:427-448):
+ * all sites' mouth Ca and channel states in one call each. */
+casim_status casim_b200_get_all_mouth(casim_h h, int32_t species, double* out);  /* sum of channels */
+casim_status casim_b200_get_all_states(casim_h h, int32_t* out);
+
+/* Device timing of the last casim_b200_step call in milliseconds (CUDA events
+ * recorded on the handle's stream around the launch sequence). */
+casim_status casim_b200_last_step_ms(casim_h h, double* out);
+/* Number of kernel launches issued by the last casim_b200_step call. */
+casim_status casim_b200_last_step_launches(casim_h h, int64_t* out);
+
+/* Diagnostic: n runif() draws of the MRG32k3a stream with the given seed,
+ * generated by a device kernel (the generator every site's gating uses).
+ * Reproduces RngStream::RandU01 with incPrec = true (CaSim/rngstream.cpp:271-283). */
+casim_status casim_b200_debug_rng(const uint32_t seed[6], int64_t n, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -226,7 +226,10 @@ def build_model(params):
     for i, (name, p) in enumerate(ions):
         m.c_bg[i] = p["Concentration"]
         m.c_onetau_ion[i] = leak * p["D"]
-    cbufs = [(n, b, True) for n, b in bufs] + [(n, b, False) for n, b in _sorted_items(c.get("Buffers", {}))]
+    # RD3D keeps only diffusing dyad buffers in the cytosol (this project's definition)
+    dyad_cb = [(n, b, True) for n, b in bufs
+               if m.cyto_type == CYTO_POOL or any(k["D"] > 0 for k in b["Ions"].values())]
+    cbufs = dyad_cb + [(n, b, False) for n, b in _sorted_items(c.get("Buffers", {}))]
     m.c_n_buf = len(cbufs)
     ceq = {n: _equilibrium(ion_cb, b, start_eq) for n, b, _ in cbufs}
     cp = 0

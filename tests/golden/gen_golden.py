@@ -1,0 +1,145 @@
+"""Generate the golden fixtures in this directory from the reference's OWN CPU
+classes (oracle/_ref/libcasim_ref.so, built by `make -C oracle ref` from the
+reference tree). Run in a container that has the reference mounted:
+
+    python tests/golden/gen_golden.py
+
+Each fixture is one NumBatch = 1 reference run (CaSim/ParallelHybridSolver.cpp:519-548
+loop body, driven by oracle/ref_capi.cpp) with snapshots of the dyad fields,
+RyR states, mouth Ca, jSR and cytosol pool after given step counts, plus the
+first draws of RngStream::RandU01 for a few seeds.
+"""
+import ctypes
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import ref  # noqa: E402
+
+REF_INPUT = "/root/reference/CaSim/test_input/Parameters.json"
+REF_COORDS = "/root/reference/CaSim/test_input/Jayasinghe.txt"
+
+
+def reference_params():
+    with open(REF_INPUT) as f:
+        return json.load(f)
+
+
+def coords_text():
+    with open(REF_COORDS) as f:
+        return f.read()
+
+
+def run_case(name, params, coords, steps, seed, first=0):
+    """Run the reference and store snapshots after each entry of `steps` (cumulative)."""
+    with tempfile.TemporaryDirectory() as td:
+        cpath = os.path.join(td, "coords.txt")
+        with open(cpath, "w") as f:
+            f.write(coords)
+        p = json.loads(json.dumps(params))
+        p["Dyad"]["Channels"]["RyR"]["Coordinates"] = cpath
+        p["Dyad"]["Seed"] = list(seed)
+        sim = ref.RefSim(p, 1, 1)
+        sim.start([first])
+        out = {"params": np.frombuffer(json.dumps(params).encode(), dtype=np.uint8),
+               "coords": np.loadtxt(cpath), "seed": np.asarray(seed, dtype=np.uint32),
+               "first": np.int32(first), "steps": np.asarray(steps, dtype=np.int64), "dims": np.asarray(sim.dims)}
+        ions = sorted(p["Dyad"]["Ions"].keys())
+        bufs = sorted(p["Dyad"]["Buffers"].keys())
+        done = 0
+        for k, n in enumerate(steps):
+            sim.step(n - done)
+            done = n
+            for ion in ions:
+                out["f%d_%s" % (k, ion)] = sim.get("dyad:" + ion)
+                out["m%d_%s" % (k, ion)] = sim.get("mouth:" + ion)
+            for b in bufs:
+                for ion in ions:
+                    if ion in p["Dyad"]["Buffers"][b]["Ions"]:
+                        out["f%d_%s-%s" % (k, ion, b)] = sim.get("dyadbuf:%s|%s-%s" % (b, ion, b))
+            out["s%d" % k] = sim.states()
+            out["sr%d" % k] = sim.get("sr")
+            out["cy%d" % k] = sim.get("cyto:Calcium")
+            out["tc%d" % k] = sim.get("total_sr_current")
+        sim.close()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print("wrote", name, {k: v.shape for k, v in out.items() if hasattr(v, "shape") and v.size > 6})
+
+
+def run_trajectory(name, params, coords, n_steps, every, seed, first=0):
+    """States of every RyR (and mouth Ca, jSR Ca) every `every` steps, fields at the end."""
+    with tempfile.TemporaryDirectory() as td:
+        cpath = os.path.join(td, "coords.txt")
+        with open(cpath, "w") as f:
+            f.write(coords)
+        p = json.loads(json.dumps(params))
+        p["Dyad"]["Channels"]["RyR"]["Coordinates"] = cpath
+        p["Dyad"]["Seed"] = list(seed)
+        sim = ref.RefSim(p, 1, 1)
+        sim.start([first])
+        states, mouth, jsr = [], [], []
+        for k in range(n_steps // every):
+            sim.step(every)
+            states.append(sim.states())
+            mouth.append(sim.get("mouth:Calcium"))
+            jsr.append(sim.get("sr")[0])
+        out = {"params": np.frombuffer(json.dumps(params).encode(), dtype=np.uint8),
+               "coords": np.loadtxt(cpath), "seed": np.asarray(seed, dtype=np.uint32), "first": np.int32(first),
+               "every": np.int64(every), "states": np.asarray(states, dtype=np.int8),
+               "mouth": np.asarray(mouth), "jsr": np.asarray(jsr), "dims": np.asarray(sim.dims),
+               "ca_final": sim.get("dyad:Calcium")}
+        sim.close()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    flips = int(np.abs(np.diff(out["states"].astype(int), axis=0)).sum())
+    print("wrote", name, "transitions", flips)
+
+
+def rng_fixture():
+    L = ref.lib()
+    seeds = [[3] * 6, [1, 2, 3, 4, 5, 6], [4294967086, 4294967086, 4294967086, 4294944442, 4294944442, 4294944442]]
+    out = {}
+    for k, s in enumerate(seeds):
+        n = 4096
+        arr = np.zeros(n)
+        L.casimref_rng_draws((ctypes.c_ulong * 6)(*s), n, arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        out["seed%d" % k] = np.asarray(s, dtype=np.uint32)
+        out["draws%d" % k] = arr
+    np.savez_compressed(os.path.join(HERE, "rng.npz"), **out)
+    print("wrote rng")
+
+
+def main():
+    if not ref.available():
+        raise SystemExit("oracle/_ref/libcasim_ref.so missing: run `make -C oracle ref`")
+    rng_fixture()
+    base = reference_params()
+    # 2D test config of the reference (SheepCannell, Ca + Mg, 3 buffers, sarcolemmal buffer)
+    run_case("ref2d_sheep", base, coords_text(), [1, 500, 3000], [7] * 6)
+    # the same run longer with another seed (gating events inside the window)
+    run_case("ref2d_sheep_s3", base, coords_text(), [12000, 16000], [3] * 6, first=5)
+    # 3D cleft: 3 layers (dz = 7.5 nm keeps the explicit step stable)
+    p3 = json.loads(json.dumps(base))
+    p3["Dyad"]["Type"] = "CPU3D"
+    p3["Dyad"]["dz"] = 7.5
+    run_case("ref3d_sheep", p3, coords_text(), [1, 400, 1500], [5] * 6)
+    # two-state MWC gating with Mg inhibition (CaSim/TwoStateMWC.cpp)
+    pm = json.loads(json.dumps(base))
+    pm["Dyad"]["Channels"]["RyR"]["Model"] = "TwoStateMWC"
+    pm["Dyad"]["Channels"]["RyR"]["Parameters"] = {"fCa": 0.00583687, "KCa": 4.1834575, "fMg": 3.2517014,
+                                                    "KMg": 92.2954937, "KO0": 10800, "KMgI": 546.4, "kclose": 0.59}
+    run_case("ref2d_mwc", pm, coords_text(), [1, 2000], [11] * 6, first=3)
+    # fast gating: many open/close events in 4000 steps (identical trajectories expected)
+    pf = json.loads(json.dumps(base))
+    pf["Dyad"]["Channels"]["RyR"]["Parameters"].update({"kopen0": 4e5, "ncaopen": 0.5, "kopenmax": 8e5, "kclose0": 245.0 * 40})
+    run_trajectory("ref2d_fastgating", pf, coords_text(), 4000, 50, [21] * 6, first=2)
+
+
+if __name__ == "__main__":
+    main()

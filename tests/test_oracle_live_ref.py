@@ -1,0 +1,41 @@
+"""The CPU restatement against the live reference build (oracle/_ref), on
+cases beyond the committed fixtures. Skipped where the reference build is
+absent (it is built only where the reference tree is mounted)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle, ref
+from casim_b200 import configs
+
+pytestmark = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+
+
+def _run_both(params, sites, steps, tmp_path):
+    cpath = os.path.join(str(tmp_path), "c.txt")
+    np.savetxt(cpath, np.c_[sites["ch_x"], sites["ch_y"]])
+    p = json.loads(json.dumps(params))
+    p["Dyad"]["Channels"]["RyR"]["Coordinates"] = cpath
+    p["Dyad"]["Seed"] = [int(v) for v in sites["seeds"][0]]
+    r = ref.RefSim(p, 1, 1)
+    r.start([int(sites["first_channel"][0])])
+    o = oracle.OracleSim(params, sites)
+    o.start(sites["first_channel"])
+    r.step(steps)
+    o.step(steps)
+    return r, o
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_config1_like_site_matches_reference(dim, tmp_path):
+    params, sites = configs.config1(n_sites=1, seed0=9, nx=24, ny=28, n_ryr=6)
+    if dim == 3:
+        params["Dyad"]["Type"] = "CPU3D"
+        params["Dyad"]["dz"] = 7.5
+        sites["nz"][:] = 3
+    r, o = _run_both(params, sites, 800, tmp_path)
+    assert np.array_equal(r.get("dyad:Calcium"), o.field(0, 0))
+    assert np.array_equal(r.states(), o.states(0))
+    assert r.get("sr")[0] == o.jsr(0)[0]
