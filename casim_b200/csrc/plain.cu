@@ -437,8 +437,9 @@ cudaError_t launch_update(cb_dev& d, cudaStream_t st) {
         cudaError_t e = cudaFuncSetAttribute(k_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
+    // the rim reads the cytosol as it was before its latest step (RD3D coupling)
     k_update<R><<<d.S, 256, smem, st>>>(d.m, d.NS, d.sites, (R*)d.fields[d.cur], (R*)d.curgrid, d.ch_node, d.ch_owner,
-                                        d.ch_state, d.mouth, d.sc, d.nc, (const R*)d.cyto[d.ccur], d.cin, d.rim_cnode,
+                                        d.ch_state, d.mouth, d.sc, d.nc, (const R*)d.cyto[1 - d.ccur], d.cin, d.rim_cnode,
                                         d.dep_ptr, d.dep_term);
     return cudaGetLastError();
 }

@@ -468,7 +468,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
             __syncthreads();
 
             // ---------------------------------------------------- phase B: Update
-            // Dirichlet rim from the cytosol (CaSim/DyadRD2DCPU.cpp:274-303)
+            // Dirichlet rim from the cytosol (CaSim/DyadRD2DCPU.cpp:274-303); the RD3D
+            // cytosol is read as it was at the start of the step (ca)
             for (int t = tid; t < nrim * nz; t += blockDim.x) {
                 int r = t % nrim, z = t / nrim, x, y;
                 cb_rim_xy(r, nx, ny, x, y);
@@ -478,10 +479,10 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                     for (int p = 0; p < m.n_pairs; ++p) fb[(NI + p) * np + n] = (R)q.c_bnd[p];
                 } else {
                     const int cn = a.rim_cnode[st.rim_off + r];
-                    for (int j = 0; j < NI; ++j) fb[j * np + n] = cb[j * nc + cn];
+                    for (int j = 0; j < NI; ++j) fb[j * np + n] = ca[j * nc + cn];
                     for (int p = 0; p < m.n_pairs; ++p) {
                         int cq = m.dyad_c_pair[p];
-                        fb[(NI + p) * np + n] = cq >= 0 ? cb[(NI + cq) * nc + cn] : (R)m.pair_init[p];
+                        fb[(NI + p) * np + n] = cq >= 0 ? ca[(NI + cq) * nc + cn] : (R)m.pair_init[p];
                     }
                 }
             }
@@ -498,7 +499,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                     double cv = mv;
                     if (rim) {
                         if (!rd3d) cv = (double)(R)q.c_ions[j];
-                        else cv = (double)cb[j * nc + a.rim_cnode[st.rim_off + cb_rim_index(x, y, nx, ny)]];
+                        else cv = (double)ca[j * nc + a.rim_cnode[st.rim_off + cb_rim_index(x, y, nx, ny)]];
                     }
                     double fl = stc * (m.g[j] * (q.jsr_new[j] - cv));
                     flux[c * NI + j] = (R)fl;
@@ -537,7 +538,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                             u0 = f < NI ? (double)(R)q.c_ions[f] : (double)(R)q.c_bnd[f - NI];
                         } else {
                             int cq = f < NI ? f : m.dyad_c_pair[f - NI];
-                            u0 = f < NI ? (double)cb[f * nc + cn] : cq >= 0 ? (double)cb[(NI + cq) * nc + cn] : (double)(R)m.pair_init[f - NI];
+                            u0 = f < NI ? (double)ca[f * nc + cn] : cq >= 0 ? (double)ca[(NI + cq) * nc + cn] : (double)(R)m.pair_init[f - NI];
                         }
                         const double D = f < NI ? m.D_ion[f] : m.D_pair[f - NI];
                         const double gr = 2 * (double)fb[f * np + n1] - 1.5 * u0 - 0.5 * (double)fb[f * np + n2];

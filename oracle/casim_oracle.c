@@ -26,7 +26,10 @@
  *     clears ion 0 only, CaSim/DyadRD2DCPU.cpp:247; identical while the
  *     other ions' conductances are zero, as in every shipped config);
  *   - the RD3D cytosol (a 3D Cartesian cytosol coupled to the cleft rim) has
- *     no reference counterpart and follows this project's own definition.
+ *     no reference counterpart and follows this project's own definition:
+ *     Update(n) sets the rim from the cytosol as it was at the start of step
+ *     n (before the cytosol's own step n), and the efflux of Update(n) is
+ *     deposited into cytosol layer 0 during step n + 1.
  * Arithmetic is written in the reference's operation order so that the FP64
  * restatement tracks the reference to rounding.
  */
@@ -161,6 +164,7 @@ typedef struct {
     double c_ions[OR_MAX_IONS], c_pairs[OR_MAX_CPAIRS], c_free[OR_MAX_CBUF], c_bnd[OR_MAX_PAIRS];
     /* rd3d cytosol */
     double* cf;      /* [(n_ions + c_n_pairs)][mc^3] */
+    double* cf_prev; /* cytosol at the start of the current step (read by Update) */
     double* cf_evo;
     double* cf_in;   /* efflux deposit [(n_ions + c_n_pairs)][mc^3] */
     int* rim_map;    /* cytosol node for each cleft (x,y) rim position, [nx*ny] */
@@ -213,6 +217,7 @@ or_sim* or_create(const or_model* m, int n_sites, const int* nx, const int* ny, 
             long nc = (long)m->mc * m->mc * m->mc;
             int ns = m->n_ions + m->c_n_pairs;
             t->cf = (double*)calloc((size_t)(ns * nc), sizeof(double));
+            t->cf_prev = (double*)calloc((size_t)(ns * nc), sizeof(double));
             t->cf_evo = (double*)calloc((size_t)(ns * nc), sizeof(double));
             t->cf_in = (double*)calloc((size_t)(ns * nc), sizeof(double));
             t->rim_map = (int*)calloc((size_t)(t->nx * t->ny), sizeof(int));
@@ -241,7 +246,7 @@ void or_destroy(or_sim* s) {
         free(t->cx); free(t->cy); free(t->cz);
         free(t->ions); free(t->pairs); free(t->freeb); free(t->evo_i); free(t->evo_p);
         free(t->cur); free(t->state); free(t->mouth);
-        free(t->cf); free(t->cf_evo); free(t->cf_in); free(t->rim_map);
+        free(t->cf); free(t->cf_prev); free(t->cf_evo); free(t->cf_in); free(t->rim_map);
     }
     free(s->site);
     free(s);
@@ -300,6 +305,7 @@ void or_reset(or_sim* s) {
                 double v = sp < m->n_ions ? m->c_bg[sp] : m->c_init[sp - m->n_ions];
                 for (long n = 0; n < nc; ++n) {
                     t->cf[sp * nc + n] = v;
+                    t->cf_prev[sp * nc + n] = v;
                     t->cf_in[sp * nc + n] = 0;
                 }
             }
@@ -525,7 +531,7 @@ static void cyto_rd3d(const or_model* m, site_t* t, double dt) {
     const long nc = (long)mc * mc * mc;
     const double h = m->hc;
     const int ns = m->n_ions + m->c_n_pairs;
-    (void)ns;
+    memcpy(t->cf_prev, t->cf, sizeof(double) * (size_t)(ns * nc));
     for (int k = 0; k < mc - 1; ++k)
         for (int j = 1; j < mc - 1; ++j)
             for (int i = 1; i < mc - 1; ++i) {
@@ -638,12 +644,12 @@ static void dyad_update(const or_model* m, site_t* t) {
                     } else {
                         long cn = t->rim_map[x * ny + y];
                         long nc = (long)m->mc * m->mc * m->mc;
-                        for (int j = 0; j < m->n_ions; ++j) t->ions[j * N + q] = t->cf[j * nc + cn];
+                        for (int j = 0; j < m->n_ions; ++j) t->ions[j * N + q] = t->cf_prev[j * nc + cn];
                         for (int p = 0; p < m->n_pairs; ++p) {
                             int cp = -1;
                             for (int r = 0; r < m->c_n_pairs; ++r)
                                 if (m->c_dyad_pair[r] == p) cp = r;
-                            t->pairs[p * N + q] = cp >= 0 ? t->cf[(m->n_ions + cp) * nc + cn] : m->pair_init[p];
+                            t->pairs[p * N + q] = cp >= 0 ? t->cf_prev[(m->n_ions + cp) * nc + cn] : m->pair_init[p];
                         }
                     }
                 }

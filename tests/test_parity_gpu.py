@@ -107,7 +107,10 @@ def _compare_batch(sim, orc, tol, scale_rel=False, check_states=True):
             assert np.array_equal(sim.states(s), orc.states(s)), "site %d" % s
             assert sim.draws(s) == orc.draws(s), "site %d" % s
         assert rel_err(sim.jsr(s), orc.jsr(s)) <= max(tol, 1e-12)
-        assert rel_err(sim.efflux(s)[:1], orc.efflux(s)[:1]) <= max(tol * 100, 1e-9)
+        if not scale_rel:
+            # FP64: the efflux (a difference of nearly equal rim values) matches too;
+            # in FP32 its integrated effect is checked through the cytosol state
+            assert rel_err(sim.efflux(s)[:1], orc.efflux(s)[:1]) <= 1e-9
         assert abs(sim.release(s) - orc.release(s)) <= max(tol, 1e-12) * max(abs(orc.release(s)), 1.0)
     print("worst per species", worst)
     for sp, err in worst.items():
@@ -148,6 +151,13 @@ def test_fp32_batch_close_to_oracle(cuda_device, dim, cytosol, path):
     sim.step(300)
     orc.step(300)
     _compare_batch(sim, orc, FP32_TOL, scale_rel=True, check_states=False)
+    for s in range(orc.S):
+        if cytosol == "RD3D":
+            for c in range(sim.info.n_cyto_species):
+                a, b = sim.cyto_field(s, c), orc.cyto_field(s, c)
+                assert np.max(np.abs(a - b)) <= FP32_TOL * np.max(np.abs(b))
+        else:
+            assert rel_err(sim.cyto(s), orc.cyto(s)) <= 1e-6
 
 
 @pytest.mark.parametrize("path", PATHS)
