@@ -38,6 +38,7 @@ EXPORTS = (
     "casim_b200_get_cyto_field", "casim_b200_get_draws", "casim_b200_get_release", "casim_b200_check_finite",
     "casim_b200_get_all_mouth", "casim_b200_get_all_states", "casim_b200_last_step_ms",
     "casim_b200_last_step_launches", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
+    "casim_b200_rng_draws_static",
 )
 
 
@@ -108,6 +109,7 @@ def lib():
         L.casim_b200_last_step_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.casim_b200_debug_rng.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]
         L.casim_b200_set_site_jsr.argtypes = [vp, dp]
+        L.casim_b200_rng_draws_static.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]
         _lib = L
     return _lib
 

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcasim_b200.so")
-SOURCES = ["capi.cu", "plain.cu", "resident.cu", "parse.cpp"]
+SOURCES = ["capi.cu", "plain.cu", "resident.cu", "noalloc.cu", "parse.cpp"]
 HEADERS = ["model.h", "engine.h", "physics.cuh", "mrg32k3a.cuh", "parse.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

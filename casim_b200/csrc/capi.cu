@@ -196,6 +196,9 @@ void build_device(casim_b200_sim* h, int precision) {
 
 }  // namespace
 
+// error text for calls that have no handle (read back through casim_b200_last_error(NULL, ...))
+void cb_set_create_error(const std::string& msg) { g_create_err = msg; }
+
 extern "C" {
 
 casim_status casim_b200_create(const char* json_text, const char* base_dir, casim_precision precision, casim_path path,

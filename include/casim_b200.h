@@ -170,6 +170,18 @@ casim_status casim_b200_last_step_launches(casim_h h, int64_t* out);
  * Reproduces RngStream::RandU01 with incPrec = true (CaSim/rngstream.cpp:271-283). */
 casim_status casim_b200_debug_rng(const uint32_t seed[6], int64_t n, double* out);
 
+/* The generator of casim_b200_debug_rng for callers that cannot allocate
+ * device memory (code inside another framework's memory pool, fixed-budget
+ * real-time hosts, processes that must not grow their device footprint after
+ * start-up). No counterpart in the reference. Its device staging buffer is a
+ * fixed array of 262144 doubles (2 MiB) that every GPU loading the library
+ * holds until exit; n above that is rejected with CASIM_EINVAL. Calls no
+ * allocator. The first call on a device resolves the array's device address
+ * with that device current; make it before any stream capture. All calls on a
+ * device share the array: calls that overlap on the GPU race. out is host
+ * memory. */
+casim_status casim_b200_rng_draws_static(const uint32_t seed[6], int64_t n, double* out);
+
 #ifdef __cplusplus
 }
 #endif
