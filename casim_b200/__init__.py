@@ -38,7 +38,7 @@ EXPORTS = (
     "casim_b200_get_cyto_field", "casim_b200_get_draws", "casim_b200_get_release", "casim_b200_check_finite",
     "casim_b200_get_all_mouth", "casim_b200_get_all_states", "casim_b200_last_step_ms",
     "casim_b200_last_step_launches", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
-    "casim_b200_rng_draws_static",
+    "casim_b200_rng_draws_static", "casim_b200_path_note",
 )
 
 
@@ -109,6 +109,7 @@ def lib():
         L.casim_b200_last_step_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.casim_b200_debug_rng.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]
         L.casim_b200_set_site_jsr.argtypes = [vp, dp]
+        L.casim_b200_path_note.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         L.casim_b200_rng_draws_static.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]
         _lib = L
     return _lib
@@ -215,6 +216,12 @@ class ReleaseSiteBatch:
     @property
     def path(self):
         return {PATH_PLAIN: "plain", PATH_RESIDENT: "resident"}.get(self.info.path, "?")
+
+    def path_note(self):
+        """How the resident path splits the batch into cluster classes, or why it runs plain."""
+        buf = ctypes.create_string_buffer(1024)
+        self._ck(lib().casim_b200_path_note(self.h, buf, 1024))
+        return buf.value.decode()
 
     def species_name(self, k):
         buf = ctypes.create_string_buffer(256)

@@ -26,6 +26,7 @@ struct casim_b200_sim {
     double last_ms = 0;
     long long last_launches = 0;
     std::vector<void*> allocs;
+    std::string resident_why;  // how the resident path splits the batch, or why it was not chosen
 };
 
 namespace {
@@ -91,6 +92,7 @@ void build_device(casim_b200_sim* h, int precision) {
     d.m = cfg.m;
     d.S = (int)cfg.sites.size();
     d.precision = precision;
+    d.min_cluster = cfg.min_cluster;
     d.NS = cfg.m.F + cfg.m.n_buf;
     const size_t rs = precision == 0 ? sizeof(double) : sizeof(float);
     std::vector<cb_site> sites(d.S);
@@ -224,9 +226,11 @@ casim_status casim_b200_create(const char* json_text, const char* base_dir, casi
         build_device(h, precision == CASIM_FP64 ? 0 : 1);
         int thr = 0;
         size_t smem = 0;
-        bool fits = cb_resident_fits(h->d, &thr, &smem);
+        std::string why;
+        bool fits = cb_resident_fits(h->d, &thr, &smem, &why);
+        h->resident_why = why;
         if (path == CASIM_PATH_RESIDENT && !fits) {
-            std::string msg = "sites do not fit the resident path's shared memory";
+            std::string msg = "resident path unavailable: " + why;
             casim_b200_destroy(h);
             return set_err(nullptr, CASIM_EUNSUPPORTED, msg);
         }
@@ -392,6 +396,14 @@ casim_status casim_b200_synchronize(casim_h h) {
     if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) h->last_ms = ms;
     return CASIM_OK;
     END_GUARD(h)
+}
+
+casim_status casim_b200_path_note(casim_h h, char* buf, size_t n) {
+    if (!h || !buf || !n) return CASIM_EINVAL;
+    size_t k = std::min(n - 1, h->resident_why.size());
+    std::memcpy(buf, h->resident_why.data(), k);
+    buf[k] = 0;
+    return CASIM_OK;
 }
 
 casim_status casim_b200_last_step_ms(casim_h h, double* out) {

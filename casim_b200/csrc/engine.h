@@ -4,12 +4,15 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "model.h"
 
 struct cb_dev {
     cb_model m;
     int S = 0;              // sites
     int precision = 0;      // 0 = FP64 fields, 1 = FP32 fields
+    int min_cluster = 1;    // smallest thread-block cluster per site on the resident path
     int NS = 0;             // mouth species per RyR: ions + pairs + free buffers
     int max_nodes = 0;      // largest padded node count of a site
     int max_ch = 0;
@@ -53,5 +56,5 @@ cudaError_t cb_plain_update(cb_dev& d, cudaStream_t st, long long* launches);
 cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);
 
 // resident path (resident.cu)
-bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem);
+bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* why);
 cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);

@@ -184,6 +184,11 @@ cb_config cb_parse_config(const std::string& json_text, const std::string& base_
     m.dt = num(j, "dt, ns", "Parameters") * 1e-6;
     if (!(m.dx > 0 && m.dy > 0 && m.dz > 0 && m.dt > 0 && m.R > 0)) fail("dx, dy, dz, dt and Radius must be positive");
     cfg.num_batch = j.contains("NumBatch") ? j.at("NumBatch").get<int>() : 1;
+    if (j.contains("B200") && j.at("B200").contains("MinClusterSize")) {
+        cfg.min_cluster = j.at("B200").at("MinClusterSize").get<int>();
+        if (cfg.min_cluster != 1 && cfg.min_cluster != 2 && cfg.min_cluster != 4 && cfg.min_cluster != 8 && cfg.min_cluster != 16)
+            fail("B200.MinClusterSize must be 1, 2, 4, 8 or 16");
+    }
 
     // ions (sorted keys)
     const json& ions = need(d, "Ions", "Dyad");

@@ -21,6 +21,7 @@ struct cb_config {
     // spline tables: knots x and per-interval cubic coefficients (a, b, c, d)
     std::vector<double> sp_x[2], sp_c[2];
     int num_batch = 1;
+    int min_cluster = 1;  // "B200": {"MinClusterSize": C}: smallest cluster per site on the resident path
 };
 
 // Throws std::runtime_error with a readable message on any schema problem.

@@ -28,9 +28,12 @@ __device__ __forceinline__ double cb_rate(const cb_model& m, const double* __res
     const double* p = m.ch_par;
     switch (m.ch_model) {
     case CB_SHEEP_CANNELL: {
-        if (state) return p[3] * pow(ca * 1e-3, p[4]) * 1e-3;
-        double ko = p[0] * pow(ca * 1e-3, p[1]);
-        return (p[2] < ko ? p[2] : ko) * 1e-3;
+        // one pow per lane whatever the state (no divergence between open and
+        // closed channels); pow(x, 0) == 1 exactly, so a zero exponent skips it
+        const double k0 = state ? p[3] : p[0];
+        const double ex = state ? p[4] : p[1];
+        const double k = k0 * (ex == 0.0 ? 1.0 : pow(ca * 1e-3, ex));
+        return (state ? k : (p[2] < k ? p[2] : k)) * 1e-3;
     }
     case CB_TWO_STATE_MWC: {
         double kclose = p[6];

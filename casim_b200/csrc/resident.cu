@@ -1,48 +1,58 @@
-// Resident path: every site lives in one thread block's shared memory for all
-// K time steps of a launch, so HBM is touched once per site per launch.
+// Resident path: each site lives in the shared memory of a thread-block
+// cluster (1..16 blocks, one per SM) for all K time steps of a launch, so HBM
+// is touched once per site per launch.
 //
-// One persistent launch walks the packed site table through an atomic work
-// queue (sites pre-sorted by decreasing cost). Per site:
-//   load     fields, RyR table, site scalars, cytosol (pool scalars or RD3D grid)
-//   K steps  phase A: warp 0 = control (efflux/current reductions of the last
-//                     Update, jSR coupling, cytosol pool ODE, jSR ODE, RyR gating);
-//                     warps 1.. = cleft stencil (and RD3D cytosol stencil),
-//                     ping-pong between two smem copies of the fields
-//            __syncthreads
-//            phase B: all warps = Update: Dirichlet rim, mouth gather, RyR
-//                     currents, efflux partials (warp shuffles)
-//            __syncthreads
-//   store    fields, scalars, RyR states, currents, RNG state
-//
-// The step semantics are the reference loop body (CaSim/ParallelHybridSolver.cpp:532-540)
-// followed by Update() (:270-286): cytosol (CaSim/CytosolPool.cpp:217-288), dyad RD
-// (CaSim/DyadRD2DCPU.cpp:394-490, CaSim/DyadRDCPU.cpp:404-506), jSR (CaSim/SRPool.cpp:70-89),
-// gating (CaSim/DyadChannels.cpp:97-130) and coupling (CaSim/DyadRD2DCPU.cpp:243-392).
+// Layout of a site over the C blocks (ranks) of its cluster:
+//   cleft   rows y in [lo_r, hi_r) per rank (lo_r = r*ny/C), stored with one halo
+//           row on each side, all x and z, every stored species, ping-pong;
+//   RD3D    cytosol planes k in [plo_r, phi_r) of the updated range [0, mc-1),
+//           stored with one halo plane on each side, ping-pong.
+// Per step (the reference loop body CaSim/ParallelHybridSolver.cpp:532-540
+// followed by Update(), :270-286):
+//   phase A  warp 0 of every rank: reductions of the previous Update, jSR
+//            coupling, cytosol pool ODE (CaSim/CytosolPool.cpp:217-288), jSR ODE
+//            (CaSim/SRPool.cpp:70-89), RyR gating (CaSim/DyadChannels.cpp:97-130);
+//            these run redundantly and bit-identically on every rank.
+//            other warps: cleft stencil of the rank's rows (CaSim/DyadRD2DCPU.cpp:394-490,
+//            CaSim/DyadRDCPU.cpp:404-506) and the RD3D cytosol planes.
+//   phase B  Dirichlet rim, mouth gather, RyR currents, efflux
+//            (CaSim/DyadRD2DCPU.cpp:243-392) of the rank's rows; halo rows and
+//            planes, mouth values, partial sums and RD3D coupling values are
+//            stored into the peers' shared memory (DSMEM) in slots double-
+//            buffered by step parity.
+//   one cluster barrier (release/acquire) per step.
 //
 // RyR gating consumes the site's MRG32k3a stream in exactly the reference's
-// order (one draw per channel, a second one per transition) but without the
-// reference's serial loop: warp 0 keeps a ring of pre-generated draws (32
-// lanes x 16 contiguous draws per refill, lanes jump-ahead by matrix powers)
-// and resolves a chunk of 32 channels with one ballot per transition.
+// order without its serial loop: warp 0 keeps a ring of pre-generated draws
+// (32 lanes x 16 contiguous draws per refill, lanes jumped ahead by matrix
+// powers) and resolves 32 channels per ballot, re-evaluating after each
+// transition, which consumes one extra draw.
+#include <cooperative_groups.h>
+
 #include <algorithm>
+#include <string>
 #include <vector>
 
 #include "engine.h"
 #include "mrg32k3a.cuh"
 #include "physics.cuh"
 
+namespace cg = cooperative_groups;
+
 namespace {
 
-constexpr int RING = 1024;                // pre-generated draws held per site
-constexpr int LANE_DRAWS = 16;            // contiguous draws per lane per refill
-constexpr int WINDOW = 32 * LANE_DRAWS;   // draws per refill
+constexpr int RING = 1024;               // pre-generated draws per site
+constexpr int LANE_DRAWS = 16;           // contiguous draws per lane per refill
+constexpr int WINDOW = 32 * LANE_DRAWS;  // draws per refill
 constexpr int MAX_THREADS = 512;
+constexpr int MAX_WARPS = MAX_THREADS / 32;
+constexpr int JUMP_ROW = 64;             // pow table row holding A^(2*31*LANE_DRAWS)
 
 struct rs_args {
     cb_model m;
     const cb_site* sites;
-    const int* order;
-    int S;
+    const int* order;  // sites of this launch, largest first
+    int S;             // sites in order[]
     int* counter;
     void* fields;
     void* curgrid;
@@ -58,40 +68,81 @@ struct rs_args {
     const int* dep_ptr;
     const int* dep_term;
     int nc;
-    const unsigned long long* pow2;  // [64][2][9]: A1^(2^k), A2^(2^k)
+    const unsigned long long* pow2;  // [65][2][9]: A^(2^k) for k < 64, then the refill jump
     const double* spx0;
     const double* spc0;
     const double* spx1;
     const double* spc1;
     long long nsteps;
-    // smem carve (bytes), identical for every site of the launch
-    int np;  // padded node capacity per species
-    int max_ch, max_terms;
-    int off_fb, off_ca, off_cb, off_terms, off_cin, off_mask, off_chn, off_chs, off_cho, off_flux, off_fluxd,
-        off_mi, off_ring, off_red, off_sc, smem_bytes;
+    // shared-memory carve (bytes, identical for every block of the launch)
+    int cap_cleft;  // stored cleft nodes per species per rank
+    int cap_cyto;   // stored cytosol nodes per species per rank
+    int max_ch, max_terms, FD;
+    int off_fb, off_ca, off_cb, off_mask, off_chn, off_chs, off_cho, off_flux, off_fluxd, off_mi, off_ring,
+        off_redw, off_rede, off_redt, off_lay0, off_terms, off_sc, smem_bytes;
 };
 
-// ---- MRG32k3a jump-ahead on the device ------------------------------------
-__device__ __forceinline__ void mat_apply(const unsigned long long* A, unsigned int* v, unsigned long long m) {
+// ---- MRG32k3a arithmetic by folding: m1 = 2^32 - 209, m2 = 2^32 - 22853 ----
+template <unsigned long long M>
+__device__ __forceinline__ unsigned long long fold_mod(unsigned long long x) {
+    constexpr unsigned long long c = (1ULL << 32) - M;
+    unsigned long long t = (x >> 32) * c + (x & 0xffffffffULL);
+    t = (t >> 32) * c + (t & 0xffffffffULL);
+    return t >= M ? t - M : t;
+}
+
+__device__ __forceinline__ double u01_fast(cbrng::State& g) {
+    unsigned long long a = fold_mod<cbrng::M1>(cbrng::A12 * g.s[1]);
+    unsigned long long b = fold_mod<cbrng::M1>(cbrng::A13N * g.s[0]);
+    unsigned long long p1 = a >= b ? a - b : a + cbrng::M1 - b;
+    g.s[0] = g.s[1];
+    g.s[1] = g.s[2];
+    g.s[2] = (unsigned int)p1;
+    a = fold_mod<cbrng::M2>(cbrng::A21 * g.s[5]);
+    b = fold_mod<cbrng::M2>(cbrng::A23N * g.s[3]);
+    unsigned long long p2 = a >= b ? a - b : a + cbrng::M2 - b;
+    g.s[3] = g.s[4];
+    g.s[4] = g.s[5];
+    g.s[5] = (unsigned int)p2;
+    const double norm = 1.0 / (4294967087.0 + 1.0);
+    double d1 = (double)p1, d2 = (double)p2;
+    return (p1 > p2) ? __dmul_rn(d1 - d2, norm) : __dmul_rn(__dadd_rn(d1 - d2, 4294967087.0), norm);
+}
+
+// RandU01 with incPrec (CaSim/rngstream.cpp:271-283), no FMA contraction
+__device__ __forceinline__ double u01d_fast(cbrng::State& g) {
+    double u = u01_fast(g);
+    double v = u01_fast(g);
+    u = __dadd_rn(u, __dmul_rn(v, 5.9604644775390625e-8));
+    return (u < 1.0) ? u : (u - 1.0);
+}
+
+template <unsigned long long M>
+__device__ __forceinline__ void mat_apply(const unsigned long long* A, unsigned int* v) {
     unsigned long long r[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         unsigned long long acc = 0;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) acc = (acc + (A[3 * i + k] * (unsigned long long)v[k]) % m) % m;
+        for (int k = 0; k < 3; ++k) {
+            acc += fold_mod<M>(A[3 * i + k] * (unsigned long long)v[k]);
+            if (acc >= M) acc -= M;
+        }
         r[i] = acc;
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i) v[i] = (unsigned int)r[i];
 }
 
+__device__ __forceinline__ void jump_row(const unsigned long long* pow2, cbrng::State& g, int k) {
+    mat_apply<cbrng::M1>(pow2 + 18 * k, g.s);
+    mat_apply<cbrng::M2>(pow2 + 18 * k + 9, g.s + 3);
+}
+
 // advance by `steps` recurrence steps (binary powering with the 2^k table)
 __device__ void rng_jump(const unsigned long long* pow2, cbrng::State& g, unsigned long long steps) {
     for (int k = 0; steps; ++k, steps >>= 1)
-        if (steps & 1ULL) {
-            mat_apply(pow2 + 18 * k, g.s, cbrng::M1);
-            mat_apply(pow2 + 18 * k + 9, g.s + 3, cbrng::M2);
-        }
+        if (steps & 1ULL) jump_row(pow2, g, k);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -100,89 +151,142 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-__device__ __forceinline__ bool is_rim(int x, int y, int nx, int ny) { return x == 0 || y == 0 || x == nx - 1 || y == ny - 1; }
+template <int C>
+__device__ __forceinline__ void cluster_barrier() {
+    if constexpr (C == 1) __syncthreads();
+    else cg::this_cluster().sync();
+}
 
-template <typename R, int FM>
+// pointer to `p` (this block's shared memory) in the shared memory of rank r
+template <int C, typename T>
+__device__ __forceinline__ T* peer(T* p, int r) {
+    if constexpr (C == 1) return p;
+    else return cg::this_cluster().map_shared_rank(p, r);
+}
+
+__device__ __forceinline__ int row_lo(int r, int ny, int C) { return (int)(((long long)r * ny) / C); }
+
+template <typename R, int NI, int NPM, int C>
 __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_constant__ rs_args a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_site;
     const cb_model& m = a.m;
-    const int F = m.F, NI = m.n_ions;
+    const int NP = m.n_pairs, F = NI + NP;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, W = blockDim.x >> 5;
+    int rank = 0;
+    if constexpr (C > 1) rank = (int)cg::this_cluster().block_rank();
     const bool rd3d = m.cyto_type == CB_CYTO_RD3D;
     const int mc = m.mc, mc2 = mc * mc, nc = a.nc, CS = m.n_ions + m.c_n_pairs;
+    const int FD = a.FD;  // dyad species with a cytosol counterpart (RD3D deposit slots)
 
     R* fa = (R*)smem;
     R* fb = (R*)(smem + a.off_fb);
     R* ca = (R*)(smem + a.off_ca);
     R* cb = (R*)(smem + a.off_cb);
-    double* terms = (double*)(smem + a.off_terms);
-    double* cin_s = (double*)(smem + a.off_cin);
     unsigned int* chmask = (unsigned int*)(smem + a.off_mask);
-    int* chn = (int*)(smem + a.off_chn);
-    int* chs = (int*)(smem + a.off_chs);
-    int* cho = (int*)(smem + a.off_cho);
+    int* chn = (int*)(smem + a.off_chn);   // local node of own RyRs, -1 otherwise
+    int* chs = (int*)(smem + a.off_chs);   // state of every RyR of the site
+    int* cho = (int*)(smem + a.off_cho);   // site node (x + nx*(y + ny*z)) | owner flag in bit 30
     R* flux = (R*)(smem + a.off_flux);
     double* fluxd = (double*)(smem + a.off_fluxd);
-    double* mi = (double*)(smem + a.off_mi);
+    double* mi = (double*)(smem + a.off_mi);        // [2][max_ch][NI]
     double* ring = (double*)(smem + a.off_ring);
-    double* red = (double*)(smem + a.off_red);
+    double* redw = (double*)(smem + a.off_redw);    // [MAX_WARPS][F + NI]
+    double* rede = (double*)(smem + a.off_rede);    // [2][C][F]
+    double* redt = (double*)(smem + a.off_redt);    // [2][C][NI]
+    R* lay0 = (R*)(smem + a.off_lay0);              // [2][CS][mc2]
+    R* terms = (R*)(smem + a.off_terms);            // [2][max_terms][FD]
     cb_site_scalars& q = *(cb_site_scalars*)(smem + a.off_sc);
 
     const double dt = m.dt;
     const R dtR = (R)dt;
+    const int FDn = F + NI;
+    // deposit slot of dyad species f (its index among species with a cytosol counterpart), or -1
+    auto dslot = [&](int f) -> int {
+        int k = 0;
+        for (int g = 0; g < f; ++g)
+            if (g < NI || m.dyad_c_pair[g - NI] >= 0) ++k;
+        return (f < NI || m.dyad_c_pair[f - NI] >= 0) ? k : -1;
+    };
 
     for (;;) {
-        if (tid == 0) s_site = atomicAdd(a.counter, 1);
-        __syncthreads();
-        if (s_site >= a.S) break;
-        const int s = a.order[s_site];
+        if (rank == 0 && tid == 0) {
+            int v = atomicAdd(a.counter, 1);
+            for (int r = 0; r < C; ++r) *peer<C>(&s_site, r) = v;
+        }
+        cluster_barrier<C>();
+        const int qsite = s_site;
+        if (qsite >= a.S) break;
+        const int s = a.order[qsite];
         const cb_site st = a.sites[s];
-        const int nx = st.nx, ny = st.ny, nz = st.nz, nxy = nx * ny, N = nxy * nz, np = st.npad;
+        const int nx = st.nx, ny = st.ny, nz = st.nz, nxy = nx * ny, np = st.npad;
         const int nch = st.n_ch;
         const int zmax = m.dim == 2 ? 1 : nz - 1;
-        const int T = cb_efflux_terms(nx, ny, zmax);
-        const int nrim = cb_rim_count(nx, ny);
+        // this rank's rows and stored rows
+        const int lo = row_lo(rank, ny, C), hi = row_lo(rank + 1, ny, C);
+        const int slo = lo > 0 ? lo - 1 : 0, shi = hi < ny ? hi + 1 : ny;
+        const int nr = shi - slo;
+        const int lstride = nx * nr;  // z stride in local storage
+        const int nloc = lstride * nz;
+        // cytosol planes (updated range [0, mc-1); plane mc-1 holds resting values)
+        const int nplanes = mc - 1;
+        const int plo = rd3d ? (int)(((long long)rank * nplanes) / C) : 0;
+        const int phi = rd3d ? (int)(((long long)(rank + 1) * nplanes) / C) : 0;
+        const int splo = plo > 0 ? plo - 1 : 0, sphi = phi + 1;
+        const int cloc = (sphi - splo) * mc2;
+        const int cap = a.cap_cleft, ccap = a.cap_cyto;
 
         // ---------------------------------------------------------- load
         {
-            const int4* src = (const int4*)((const R*)a.fields + st.node_base * F);
-            int4* dst = (int4*)fa;
-            const int n16 = (int)((size_t)F * np * sizeof(R) / 16);
-            for (int k = tid; k < n16; k += blockDim.x) dst[k] = src[k];
-            for (int k = tid; k < (np + 31) / 32; k += blockDim.x) chmask[k] = 0u;
+            const R* g = (const R*)a.fields + st.node_base * F;
+            for (int f = 0; f < F; ++f)
+                for (int z = 0; z < nz; ++z) {
+                    const R* src = g + (long long)f * np + (long long)nx * (slo + (long long)ny * z);
+                    for (int k = tid; k < lstride; k += blockDim.x) {
+                        const R v = src[k];
+                        fa[f * cap + lstride * z + k] = v;
+                        fb[f * cap + lstride * z + k] = v;
+                    }
+                }
+            for (int k = tid; k < (nloc + 31) / 32; k += blockDim.x) chmask[k] = 0u;
             const unsigned int* qs = (const unsigned int*)(a.sc + s);
             unsigned int* qd = (unsigned int*)&q;
             for (int k = tid; k < (int)(sizeof(cb_site_scalars) / 4); k += blockDim.x) qd[k] = qs[k];
             if (rd3d) {
                 const R* cs = (const R*)a.cyto + (size_t)s * CS * nc;
-                for (int k = tid; k < CS * nc; k += blockDim.x) {
-                    R v = cs[k];
-                    ca[k] = v;
-                    cb[k] = v;
-                }
-                for (int k = tid; k < CS * mc2; k += blockDim.x) cin_s[k] = a.cin[(size_t)s * CS * mc2 + k];
+                for (int c = 0; c < CS; ++c)
+                    for (int k = tid; k < cloc; k += blockDim.x) {
+                        const R v = cs[(size_t)c * nc + (size_t)splo * mc2 + k];
+                        ca[c * ccap + k] = v;
+                        cb[c * ccap + k] = v;
+                    }
+                // cytosol layer 0 at entry: the rim values of the first step (parity-1 slot)
+                for (int c = 0; c < CS; ++c)
+                    for (int k = tid; k < mc2; k += blockDim.x) lay0[(CS + c) * mc2 + k] = cs[(size_t)c * nc + k];
             }
         }
         __syncthreads();
         for (int c = tid; c < nch; c += blockDim.x) {
-            int node = a.ch_node[st.ch_off + c];
-            chn[c] = node;
+            const int gnode = a.ch_node[st.ch_off + c];
+            const int x = gnode % nx, y = (gnode / nx) % ny, z = gnode / nxy;
             chs[c] = a.ch_state[st.ch_off + c];
-            cho[c] = a.ch_owner[st.ch_off + c];
-            atomicOr(&chmask[node >> 5], 1u << (node & 31));
+            cho[c] = gnode | (a.ch_owner[st.ch_off + c] ? (1 << 30) : 0);
+            const bool own = y >= lo && y < hi;
+            const int ln = own ? x + nx * ((y - slo) + nr * z) : -1;
+            chn[c] = ln;
             const double* mo = a.mouth + (size_t)(st.ch_off + c) * a.NS;
-            for (int j = 0; j < NI; ++j) {
-                mi[c * NI + j] = mo[j];
-                // current of the last Update: state * g * (jSR - Ca at the node)
-                double fl = chs[c] * (m.g[j] * (q.jsr_new[j] - (double)fa[j * np + node]));
-                flux[c * NI + j] = (R)fl;
-                fluxd[c * NI + j] = fl;
+            for (int j = 0; j < NI; ++j) mi[(a.max_ch + c) * NI + j] = mo[j];  // parity-1 slot
+            if (own) {
+                atomicOr(&chmask[ln >> 5], 1u << (ln & 31));
+                for (int j = 0; j < NI; ++j) {
+                    // current of the last Update: state * g * (jSR - Ca at the node)
+                    const double fl = chs[c] * (m.g[j] * (q.jsr_new[j] - (double)fa[j * cap + ln]));
+                    flux[c * NI + j] = (R)fl;
+                    fluxd[c * NI + j] = fl;
+                }
             }
         }
-
-        // RNG (warp 0): lane l holds the stream at draw D0 + l*LANE_DRAWS of the
-        // next window; ring slot k % RING holds draw k (counted from entry)
+        // RNG (warp 0): lane l holds the stream at draw D + l*LANE_DRAWS of the next window
         cbrng::State g0, gl;
         long long D = 0, we = 0;
         if (warp == 0) {
@@ -190,25 +294,24 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
             gl = g0;
             rng_jump(a.pow2, gl, 2ULL * LANE_DRAWS * lane);
         }
-        __syncthreads();
+        cluster_barrier<C>();
 
         // ---------------------------------------------------------- steps
         for (long long it = 0; it < a.nsteps; ++it) {
+            const int par = (int)(it & 1), prv = par ^ 1;
             const bool last = it == a.nsteps - 1;
             if (warp == 0) {
-                // ---- control warp
                 if (it > 0) {
-                    // reductions of the previous Update (fixed order -> deterministic)
+                    // reductions of the previous Update, in rank order on every rank
                     for (int f = lane; f < F; f += 32) {
                         double e = 0;
-                        for (int w = 0; w < W; ++w) e += red[w * FM + f];
+                        for (int r = 0; r < C; ++r) e += rede[(prv * C + r) * F + f];
                         q.efflux[f] = e;
                     }
-                    for (int j = 0; j < NI; ++j) {
+                    for (int j = lane; j < NI; j += 32) {
                         double t = 0;
-                        for (int c = lane; c < nch; c += 32) t += fluxd[c * NI + j];
-                        t = warp_sum(t);
-                        if (lane == 0) q.total[j] = t;
+                        for (int r = 0; r < C; ++r) t += redt[(prv * C + r) * NI + j];
+                        q.total[j] = t;
                     }
                     __syncwarp();
                     if (lane == 0 && !m.jsr_const)
@@ -228,16 +331,16 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                             double react = 0;
                             for (int p = 0; p < m.c_n_pairs; ++p) {
                                 if (m.c_pair_ion[p] != j) continue;
-                                double R1 = m.c_koff[p] * q.c_pairs[p] - m.c_kon[p] * q.c_ions[j] * q.c_free[m.c_pair_buf[p]];
+                                const double R1 = m.c_koff[p] * q.c_pairs[p] - m.c_kon[p] * q.c_ions[j] * q.c_free[m.c_pair_buf[p]];
                                 evo_p[p] = -R1;
                                 react += R1;
                                 if (m.c_in_dyad[p]) evo_p[p] += q.efflux[NI + ipd++];
                             }
                             evo_i[j] = react + q.efflux[j];
                             if (m.c_serca[j]) {
-                                double i2 = q.c_ions[j] * q.c_ions[j];
-                                double K2 = m.c_Kup[is] * m.c_Kup[is];
-                                double b2 = m.c_bg[is] * m.c_bg[is];
+                                const double i2 = q.c_ions[j] * q.c_ions[j];
+                                const double K2 = m.c_Kup[is] * m.c_Kup[is];
+                                const double b2 = m.c_bg[is] * m.c_bg[is];
                                 evo_i[j] -= m.c_Jmax[is] * (i2 / (i2 + K2) - b2 / (b2 + K2));
                                 ++is;
                             }
@@ -261,23 +364,22 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                         for (int j = 0; j < NI; ++j)
                             beta += m.nCQ[j] * m.K_CQ[j] * m.CQ / ((m.K_CQ[j] + q.jsr[j]) * (m.K_CQ[j] + q.jsr[j]));
                         for (int i = 0; i < NI; ++i) {
-                            double Iref = 1 / m.tau_refill[i] * (q.nsr[i] - q.jsr[i]);
+                            const double Iref = 1 / m.tau_refill[i] * (q.nsr[i] - q.jsr[i]);
                             q.jsr_new[i] = q.jsr[i] + dt / beta * (Iref - q.IjSR[i] / m.V_jsr);
                         }
                         if (m.ca_idx >= 0) q.release += q.IjSR[m.ca_idx] * dt;
                     }
                 }
-                // ---- ring refill: keep at least 2 draws per channel available
+                // ring refill: at least two draws per channel available
                 if (we - D < 2LL * nch) {
-                    long long base = we + (long long)lane * LANE_DRAWS;
-                    for (int i = 0; i < LANE_DRAWS; ++i) ring[(base + i) & (RING - 1)] = cbrng::u01d(gl);
-                    // jump from the end of this lane's chunk to its chunk in the next window
-                    rng_jump(a.pow2, gl, 2ULL * LANE_DRAWS * 31);
+                    const long long base = we + (long long)lane * LANE_DRAWS;
+                    for (int i = 0; i < LANE_DRAWS; ++i) ring[(base + i) & (RING - 1)] = u01d_fast(gl);
+                    jump_row(a.pow2, gl, JUMP_ROW);  // to this lane's chunk of the next window
                     we += WINDOW;
-                    __syncwarp();
                 }
-                // ---- gating (CaSim/DyadChannels.cpp:97-130): draw D+i tests channel i
-                // until a transition consumes one extra draw; one ballot per transition
+                __syncwarp();
+                // gating: draw D+i tests channel i until a transition takes one more draw
+                const double* mprev = mi + prv * a.max_ch * NI;
                 for (int base = 0; base < nch; base += 32) {
                     const int c = base + lane;
                     const int cnt = min(32, nch - base);
@@ -286,20 +388,20 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                     int stt = 0;
                     if (act) {
                         stt = chs[c];
-                        double cam = mi[c * NI + m.ca_idx];
-                        double mgm = m.mg_idx >= 0 ? mi[c * NI + m.mg_idx] : 0.0;
+                        const double cam = mprev[c * NI + m.ca_idx];
+                        const double mgm = m.mg_idx >= 0 ? mprev[c * NI + m.mg_idx] : 0.0;
                         p = cb_rate(m, a.spx0, a.spc0, a.spx1, a.spc1, stt, cam, mgm) * dt;
                     }
                     int start = 0;
                     while (start < cnt) {
                         const bool rem = act && lane >= start;
-                        double u = rem ? ring[(D + (lane - start)) & (RING - 1)] : 2.0;
-                        unsigned int t = __ballot_sync(0xffffffffu, rem && (u < p));
+                        const double u = rem ? ring[(D + (lane - start)) & (RING - 1)] : 2.0;
+                        const unsigned int t = __ballot_sync(0xffffffffu, rem && (u < p));
                         if (t == 0u) {
                             D += cnt - start;
                             break;
                         }
-                        int f = __ffs(t) - 1;
+                        const int f = __ffs(t) - 1;
                         if (lane == f) chs[c] = 1 - stt;
                         D += (f - start) + 2;
                         start = f + 1;
@@ -307,45 +409,41 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                 }
                 __syncwarp();
             } else {
-                // ---- worker warps: cleft stencil fa -> fb on interior nodes
-                const int wt = tid - 32, NW = blockDim.x - 32;
+                // ---- worker warps: cleft stencil of this rank's interior rows
+                const int wk = warp - 1, NW = W - 1;
                 const R idx2 = (R)m.inv_dx2, idy2 = (R)m.inv_dy2, idz2 = (R)m.inv_dz2;
-                const int ix = nx - 2, ncol = ix * (ny - 2);
-                for (int i = wt; i < ncol; i += NW) {
-                    const int x = 1 + i % ix, y = 1 + i / ix;
+                const int ylo = max(lo, 1), yhi = min(hi, ny - 1);
+                const int XB = (nx - 2 + 31) >> 5;
+                const int ntask = (yhi - ylo) * XB;
+                for (int t = wk; t < ntask; t += NW) {
+                    const int ry = t / XB;
+                    const int x = 1 + ((t - ry * XB) << 5) + lane;
+                    if (x > nx - 2) continue;
+                    const int lrow = ylo + ry - slo;
                     for (int z = 0; z < nz; ++z) {
-                        const int n = x + nx * y + nxy * z;
+                        const int n = x + nx * (lrow + nr * z);
                         int zl = n, zr = n;
                         if (m.dim == 3) {
-                            zl = z == 0 ? n + nxy : n - nxy;
-                            zr = z == nz - 1 ? n - nxy : n + nxy;
+                            zl = z == 0 ? n + lstride : n - lstride;
+                            zr = z == nz - 1 ? n - lstride : n + lstride;
                         }
-                        // ions (j) and ion-buffer pairs (p) kept in separate register
-                        // arrays indexed only by unrolled constants
-                        R vi[CB_MAX_IONS], ei[CB_MAX_IONS], vp[FM], ep[FM];
+                        R vi[NI], ei[NI], vp[NPM], ep[NPM];
 #pragma unroll
-                        for (int j = 0; j < CB_MAX_IONS; ++j) {
-                            vi[j] = 0;
-                            ei[j] = 0;
-                            if (j < NI) {
-                                const R* v = fa + j * np;
-                                R cc = v[n];
-                                vi[j] = cc;
-                                const R D = (R)m.D_ion[j];
-                                if (D != (R)0) {
-                                    R lap = (v[n + 1] - 2 * cc + v[n - 1]) * idx2 + (v[n + nx] - 2 * cc + v[n - nx]) * idy2;
-                                    if (m.dim == 3) lap = lap + (v[zr] - 2 * cc + v[zl]) * idz2;
-                                    ei[j] = D * lap;
-                                }
-                            }
+                        for (int j = 0; j < NI; ++j) {
+                            const R* v = fa + j * cap;
+                            const R cc = v[n];
+                            vi[j] = cc;
+                            R lap = (v[n + 1] - 2 * cc + v[n - 1]) * idx2 + (v[n + nx] - 2 * cc + v[n - nx]) * idy2;
+                            if (m.dim == 3) lap = lap + (v[zr] - 2 * cc + v[zl]) * idz2;
+                            ei[j] = (R)m.D_ion[j] * lap;
                         }
 #pragma unroll
-                        for (int p = 0; p < FM; ++p) {
+                        for (int p = 0; p < NPM; ++p) {
                             vp[p] = 0;
                             ep[p] = 0;
-                            if (p < m.n_pairs) {
-                                const R* v = fa + (NI + p) * np;
-                                R cc = v[n];
+                            if (p < NP) {
+                                const R* v = fa + (NI + p) * cap;
+                                const R cc = v[n];
                                 vp[p] = cc;
                                 const R D = (R)m.D_pair[p];
                                 if (D != (R)0) {
@@ -355,29 +453,38 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                                 }
                             }
                         }
-                        // reactions: free buffer of each pair's buffer (total minus its
-                        // pairs in pair order), R1 = koff*B - kon*ion*free
-                        R r1[FM];
+                        // reactions: R1 = koff*B - kon*ion*free, free = total minus the
+                        // buffer's pairs in pair order (CaSim/DyadRD2DCPU.cpp:415-456)
+                        R Rj[NI];
 #pragma unroll
-                        for (int p = 0; p < FM; ++p) {
-                            r1[p] = 0;
-                            if (p < m.n_pairs) {
+                        for (int j = 0; j < NI; ++j) Rj[j] = 0;
+#pragma unroll
+                        for (int p = 0; p < NPM; ++p) {
+                            if (p < NP) {
                                 const int b = m.pair_buf[p];
                                 R fr = (R)m.Ctot[b];
 #pragma unroll
-                                for (int p2 = 0; p2 < FM; ++p2)
-                                    if (p2 < m.n_pairs && m.pair_buf[p2] == b) fr -= vp[p2];
-                                R ion = 0;
+                                for (int p2 = 0; p2 < NPM; ++p2)
+                                    if (p2 < NP && m.pair_buf[p2] == b) fr -= vp[p2];
+                                R ion = vi[0];
+                                if constexpr (NI > 1) {
 #pragma unroll
-                                for (int j = 0; j < CB_MAX_IONS; ++j)
-                                    if (j == m.pair_ion[p]) ion = vi[j];
-                                r1[p] = (R)m.koff[p] * vp[p] - (R)m.kon[p] * ion * fr;
-                                ep[p] += -r1[p];
+                                    for (int j = 1; j < NI; ++j)
+                                        if (m.pair_ion[p] == j) ion = vi[j];
+                                }
+                                const R r1 = (R)m.koff[p] * vp[p] - (R)m.kon[p] * ion * fr;
+                                ep[p] += -r1;
+                                if constexpr (NI == 1) {
+                                    Rj[0] += r1;
+                                } else {
+#pragma unroll
+                                    for (int j = 0; j < NI; ++j)
+                                        if (m.pair_ion[p] == j) Rj[j] += r1;
+                                }
                             }
                         }
-                        const bool has_ch = (chmask[n >> 5] >> (n & 31)) & 1u;
                         int cown = -1;
-                        if (has_ch)
+                        if ((chmask[n >> 5] >> (n & 31)) & 1u)
                             for (int c = nch - 1; c >= 0; --c)
                                 if (chn[c] == n) {
                                     cown = c;
@@ -385,62 +492,63 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                                 }
                         const bool sl_layer = (m.dim == 2) || (z == nz - 1);
 #pragma unroll
-                        for (int j = 0; j < CB_MAX_IONS; ++j) {
-                            if (j < NI) {
-                                R Rj = 0;
-#pragma unroll
-                                for (int p = 0; p < FM; ++p)
-                                    if (p < m.n_pairs && m.pair_ion[p] == j) Rj += r1[p];
-                                R e = ei[j] + Rj;
-                                if (cown >= 0) e += flux[cown * NI + j];
-                                if (sl_layer && m.has_sl[j]) {
-                                    R s1 = (R)m.K1[j] + vi[j];
-                                    R s2 = (R)m.K2[j] + vi[j];
-                                    e *= (R)1 / ((R)1 + (R)(m.N1[j] * m.K1[j]) / (s1 * s1) + (R)(m.N2[j] * m.K2[j]) / (s2 * s2));
-                                }
-                                fb[j * np + n] = vi[j] + e * dtR;
+                        for (int j = 0; j < NI; ++j) {
+                            R e = ei[j] + Rj[j];
+                            if (cown >= 0) e += flux[cown * NI + j];
+                            if (sl_layer && m.has_sl[j]) {
+                                const R s1 = (R)m.K1[j] + vi[j];
+                                const R s2 = (R)m.K2[j] + vi[j];
+                                e *= (R)1 / ((R)1 + (R)(m.N1[j] * m.K1[j]) / (s1 * s1) + (R)(m.N2[j] * m.K2[j]) / (s2 * s2));
                             }
+                            fb[j * cap + n] = vi[j] + e * dtR;
                         }
 #pragma unroll
-                        for (int p = 0; p < FM; ++p)
-                            if (p < m.n_pairs) fb[(NI + p) * np + n] = vp[p] + ep[p] * dtR;
+                        for (int p = 0; p < NPM; ++p)
+                            if (p < NP) fb[(NI + p) * cap + n] = vp[p] + ep[p] * dtR;
                     }
                 }
                 if (rd3d) {
-                    // RD3D cytosol stencil ca -> cb (no reference analog; see the oracle)
+                    // RD3D cytosol planes of this rank (no reference analog; see the oracle)
                     const R ih2 = (R)m.inv_hc2;
                     const int* ptr = a.dep_ptr + (size_t)s * (mc2 + 1);
-                    for (int n = wt; n < nc; n += NW) {
-                        const int i = n % mc, j = (n / mc) % mc, k = n / mc2;
-                        if (i == 0 || i == mc - 1 || j == 0 || j == mc - 1 || k == mc - 1) continue;
-                        const int zl = k == 0 ? n + mc2 : n - mc2, zr = n + mc2;
-                        R evo[CB_MAX_CSPECIES], u[CB_MAX_CSPECIES];
+                    const int wt = tid - 32, NWT = blockDim.x - 32;
+                    const int ninner = (mc - 2) * (mc - 2);
+                    const int ntot = (phi - plo) * ninner;
+                    for (int t = wt; t < ntot; t += NWT) {
+                        const int kk = t / ninner;
+                        const int rem = t - kk * ninner;
+                        const int jj = 1 + rem / (mc - 2), ii = 1 + rem % (mc - 2);
+                        const int k = plo + kk;
+                        const int ln = ii + mc * jj + mc2 * (k - splo);
+                        const int zl = k == 0 ? ln + mc2 : ln - mc2, zr = ln + mc2;
+                        R u[CB_MAX_CSPECIES], evo[CB_MAX_CSPECIES];
                         for (int c = 0; c < CS; ++c) {
-                            const R* v = ca + c * nc;
-                            R D = (R)(c < NI ? m.D_ion[c] : m.c_D_pair[c - NI]);
-                            R cc = v[n];
+                            const R* v = ca + c * ccap;
+                            const R D = (R)(c < NI ? m.D_ion[c] : m.c_D_pair[c - NI]);
+                            const R cc = v[ln];
                             u[c] = cc;
-                            evo[c] = D * ((v[n + 1] - 2 * cc + v[n - 1]) * ih2 + (v[n + mc] - 2 * cc + v[n - mc]) * ih2 +
+                            evo[c] = D * ((v[ln + 1] - 2 * cc + v[ln - 1]) * ih2 + (v[ln + mc] - 2 * cc + v[ln - mc]) * ih2 +
                                           (v[zr] - 2 * cc + v[zl]) * ih2);
                         }
-                        R fr[CB_MAX_CBUF];
-                        for (int b = 0; b < m.c_n_buf; ++b) fr[b] = (R)m.c_Ctot[b];
-                        for (int p = 0; p < m.c_n_pairs; ++p) fr[m.c_pair_buf[p]] -= u[NI + p];
                         int is = 0;
                         for (int j2 = 0; j2 < NI; ++j2) {
-                            R ion = u[j2];
+                            const R ion = u[j2];
                             R react = 0;
                             for (int p = 0; p < m.c_n_pairs; ++p) {
                                 if (m.c_pair_ion[p] != j2) continue;
-                                R R1 = (R)m.c_koff[p] * u[NI + p] - (R)m.c_kon[p] * ion * fr[m.c_pair_buf[p]];
+                                const int b = m.c_pair_buf[p];
+                                R fr = (R)m.c_Ctot[b];
+                                for (int p2 = 0; p2 < m.c_n_pairs; ++p2)
+                                    if (m.c_pair_buf[p2] == b) fr -= u[NI + p2];
+                                const R R1 = (R)m.c_koff[p] * u[NI + p] - (R)m.c_kon[p] * ion * fr;
                                 evo[NI + p] += -R1;
                                 react += R1;
                             }
                             evo[j2] += react;
                             if (m.c_serca[j2]) {
-                                R i2 = ion * ion;
-                                R K2 = (R)(m.c_Kup[is] * m.c_Kup[is]);
-                                R b2 = (R)(m.c_bg[is] * m.c_bg[is]);
+                                const R i2 = ion * ion;
+                                const R K2 = (R)(m.c_Kup[is] * m.c_Kup[is]);
+                                const R b2 = (R)(m.c_bg[is] * m.c_bg[is]);
                                 evo[j2] -= (R)m.c_Jmax[is] * (i2 / (i2 + K2) - b2 / (b2 + K2));
                                 ++is;
                             }
@@ -448,19 +556,21 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                         for (int c = 0; c < CS; ++c) {
                             R e = evo[c];
                             if (k == 0) {
-                                double dep;
+                                // deposit of the previous Update, summed in the oracle's term order
+                                const int cn = ii + mc * jj;
+                                double dep = 0;
                                 if (it == 0) {
-                                    dep = cin_s[c * mc2 + n];
+                                    dep = a.cin[((size_t)s * CS + c) * mc2 + cn];
                                 } else {
-                                    int f = c < NI ? c : m.c_dyad_pair[c - NI];
-                                    if (f >= 0 && c >= NI) f += NI;
-                                    dep = 0;
-                                    if (f >= 0)
-                                        for (int kk = ptr[n]; kk < ptr[n + 1]; ++kk) dep += terms[a.dep_term[st.term_off + kk] * FM + f];
+                                    const int f = c < NI ? c : (m.c_dyad_pair[c - NI] >= 0 ? NI + m.c_dyad_pair[c - NI] : -1);
+                                    const int sl = f >= 0 ? dslot(f) : -1;
+                                    if (sl >= 0)
+                                        for (int q2 = ptr[cn]; q2 < ptr[cn + 1]; ++q2)
+                                            dep += (double)terms[((size_t)prv * a.max_terms + a.dep_term[st.term_off + q2]) * FD + sl];
                                 }
                                 e += (R)dep;
                             }
-                            cb[c * nc + n] = u[c] + e * dtR;
+                            cb[c * ccap + ln] = u[c] + e * dtR;
                         }
                     }
                 }
@@ -468,113 +578,226 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
             __syncthreads();
 
             // ---------------------------------------------------- phase B: Update
-            // Dirichlet rim from the cytosol (CaSim/DyadRD2DCPU.cpp:274-303); the RD3D
-            // cytosol is read as it was at the start of the step (ca)
-            for (int t = tid; t < nrim * nz; t += blockDim.x) {
-                int r = t % nrim, z = t / nrim, x, y;
-                cb_rim_xy(r, nx, ny, x, y);
-                const int n = x + nx * y + nxy * z;
-                if (!rd3d) {
-                    for (int j = 0; j < NI; ++j) fb[j * np + n] = (R)q.c_ions[j];
-                    for (int p = 0; p < m.n_pairs; ++p) fb[(NI + p) * np + n] = (R)q.c_bnd[p];
-                } else {
-                    const int cn = a.rim_cnode[st.rim_off + r];
-                    for (int j = 0; j < NI; ++j) fb[j * np + n] = ca[j * nc + cn];
-                    for (int p = 0; p < m.n_pairs; ++p) {
-                        int cq = m.dyad_c_pair[p];
-                        fb[(NI + p) * np + n] = cq >= 0 ? ca[(NI + cq) * nc + cn] : (R)m.pair_init[p];
+            const R* lprev = lay0 + prv * CS * mc2;  // cytosol layer 0 at the start of this step
+            auto rim_value = [&](int f, int x, int y) -> R {
+                if (!rd3d) return f < NI ? (R)q.c_ions[f] : (R)q.c_bnd[f - NI];
+                const int cn = a.rim_cnode[st.rim_off + cb_rim_index(x, y, nx, ny)];
+                if (f < NI) return lprev[f * mc2 + cn];
+                const int cq = m.dyad_c_pair[f - NI];
+                return cq >= 0 ? lprev[(NI + cq) * mc2 + cn] : (R)m.pair_init[f - NI];
+            };
+            // Dirichlet rim of this rank's rows (CaSim/DyadRD2DCPU.cpp:274-303)
+            {
+                const int nxe = 2 * (hi - lo);                                     // x = 0 / nx-1 columns
+                const int nye = (lo == 0 ? nx - 2 : 0) + (hi == ny ? nx - 2 : 0);  // inner nodes of rows 0 / ny-1
+                const int per_z = nxe + nye;
+                for (int t = tid; t < per_z * nz; t += blockDim.x) {
+                    const int z = t / per_z, k = t - z * per_z;
+                    int x, y;
+                    if (k < nxe) {
+                        y = lo + (k >> 1);
+                        x = (k & 1) ? nx - 1 : 0;
+                    } else {
+                        int kk = k - nxe;
+                        if (lo == 0 && kk < nx - 2) {
+                            y = 0;
+                        } else {
+                            if (lo == 0) kk -= nx - 2;
+                            y = ny - 1;
+                        }
+                        x = 1 + kk;
                     }
+                    const int n = x + nx * ((y - slo) + nr * z);
+                    for (int f = 0; f < F; ++f) fb[f * cap + n] = rim_value(f, x, y);
                 }
             }
-            // mouth gather and RyR currents (CaSim/DyadRD2DCPU.cpp:243-264, 361-380)
+            // mouth gather and RyR currents of own channels (CaSim/DyadRD2DCPU.cpp:243-264, 361-380)
+            double tpart[NI];
+#pragma unroll
+            for (int j = 0; j < NI; ++j) tpart[j] = 0;
+            double* mcur = mi + par * a.max_ch * NI;
             for (int c = tid; c < nch; c += blockDim.x) {
                 const int n = chn[c];
-                const int x = n % nx, y = (n / nx) % ny;
-                const bool rim = is_rim(x, y, nx, ny);
-                const R* src = rim ? fa : fb;  // mouth is gathered before the rim is reset
+                if (n < 0) continue;
+                const int gnode = cho[c] & ((1 << 30) - 1);
+                const int x = gnode % nx, y = (gnode / nx) % ny;
+                const bool rim = x == 0 || y == 0 || x == nx - 1 || y == ny - 1;
+                const R* src = rim ? fa : fb;  // the mouth is gathered before the rim is reset
                 const int stc = chs[c];
+#pragma unroll
                 for (int j = 0; j < NI; ++j) {
-                    double mv = (double)src[j * np + n];
-                    mi[c * NI + j] = mv;
-                    double cv = mv;
-                    if (rim) {
-                        if (!rd3d) cv = (double)(R)q.c_ions[j];
-                        else cv = (double)ca[j * nc + a.rim_cnode[st.rim_off + cb_rim_index(x, y, nx, ny)]];
-                    }
-                    double fl = stc * (m.g[j] * (q.jsr_new[j] - cv));
+                    const double mv = (double)src[j * cap + n];
+                    for (int r = 0; r < C; ++r) peer<C>(mcur, r)[c * NI + j] = mv;
+                    const double cv = rim ? (double)rim_value(j, x, y) : mv;
+                    const double fl = stc * (m.g[j] * (q.jsr_new[j] - cv));
                     flux[c * NI + j] = (R)fl;
                     fluxd[c * NI + j] = fl;
+                    tpart[j] += fl;
                 }
                 if (last) {
                     double* mo = a.mouth + (size_t)(st.ch_off + c) * a.NS;
                     double fr[CB_MAX_BUF];
                     for (int b = 0; b < m.n_buf; ++b) fr[b] = m.Ctot[b];
                     for (int f = 0; f < F; ++f) {
-                        double v = (double)src[f * np + n];
+                        const double v = (double)src[f * cap + n];
                         mo[f] = v;
                         if (f >= NI) fr[m.pair_buf[f - NI]] -= v;
                     }
                     for (int b = 0; b < m.n_buf; ++b) mo[F + b] = fr[b];
                 }
             }
-            // efflux partials (CaSim/DyadRD2DCPU.cpp:305-350); the rim value u0 is
-            // the cytosol value just written
+            // efflux of this rank's rim terms (CaSim/DyadRD2DCPU.cpp:305-350); u0 is the rim value
+            double epart[NI + NPM];
+#pragma unroll
+            for (int f = 0; f < NI + NPM; ++f) epart[f] = 0;
             {
-                double part[FM];
-#pragma unroll
-                for (int f = 0; f < FM; ++f) part[f] = 0;
-                for (int t = tid; t < T; t += blockDim.x) {
-                    int x0, y0, x1, y1, x2, y2, z;
-                    int sel = cb_efflux_term(t, nx, ny, zmax, x0, y0, x1, y1, x2, y2, z);
-                    const double sf = sel == 0 ? m.sx : m.sy;
-                    const int n1 = x1 + nx * y1 + nxy * z, n2 = x2 + nx * y2 + nxy * z;
-                    int cn = 0;
-                    if (rd3d) cn = a.rim_cnode[st.rim_off + cb_rim_index(x0, y0, nx, ny)];
-#pragma unroll
-                    for (int f = 0; f < FM; ++f) {
-                        if (f >= F) break;
-                        double u0;
-                        if (!rd3d) {
-                            u0 = f < NI ? (double)(R)q.c_ions[f] : (double)(R)q.c_bnd[f - NI];
+                const int ylo = max(lo, 1), yhi = min(hi, ny - 1);
+                const int nxr = max(yhi - ylo, 0);
+                const int nxt = 2 * nxr;                                   // x-edge terms per z
+                const int nyt = (lo == 0 ? nx : 0) + (hi == ny ? nx : 0);  // y-edge terms per z
+                const int per_z = nxt + nyt;
+                R* t0 = peer<C>(terms + (size_t)par * a.max_terms * FD, 0);
+                for (int t = tid; t < per_z * zmax; t += blockDim.x) {
+                    const int z = t / per_z, k = t - z * per_z;
+                    int x0, y0, dxs, dys, gterm;
+                    double sf;
+                    if (k < nxt) {
+                        const int e = k / nxr, y = ylo + (k - e * nxr);
+                        x0 = e ? nx - 1 : 0;
+                        y0 = y;
+                        dxs = e ? -1 : 1;
+                        dys = 0;
+                        sf = m.sx;
+                        gterm = (e * (ny - 2) + (y - 1)) * zmax + z;
+                    } else {
+                        int kk = k - nxt;
+                        int e;
+                        if (lo == 0 && kk < nx) {
+                            e = 0;
                         } else {
-                            int cq = f < NI ? f : m.dyad_c_pair[f - NI];
-                            u0 = f < NI ? (double)ca[f * nc + cn] : cq >= 0 ? (double)ca[(NI + cq) * nc + cn] : (double)(R)m.pair_init[f - NI];
+                            if (lo == 0) kk -= nx;
+                            e = 1;
                         }
-                        const double D = f < NI ? m.D_ion[f] : m.D_pair[f - NI];
-                        const double gr = 2 * (double)fb[f * np + n1] - 1.5 * u0 - 0.5 * (double)fb[f * np + n2];
-                        if (!rd3d) {
-                            part[f] += D * m.grad_mult * sf * gr;
-                        } else {
-                            double v = D * sf * gr * m.inv_hc3;
-                            part[f] += v;
-                            terms[t * FM + f] = v;
+                        x0 = kk;
+                        y0 = e ? ny - 1 : 0;
+                        dxs = 0;
+                        dys = e ? -1 : 1;
+                        sf = m.sy;
+                        gterm = (2 * (ny - 2) + e * nx + kk) * zmax + z;
+                    }
+                    const int n1 = (x0 + dxs) + nx * ((y0 + dys - slo) + nr * z);
+                    const int n2 = (x0 + 2 * dxs) + nx * ((y0 + 2 * dys - slo) + nr * z);
+#pragma unroll
+                    for (int f = 0; f < NI + NPM; ++f) {
+                        if (f < F) {
+                            const double u0 = (double)rim_value(f, x0, y0);
+                            const double D = f < NI ? m.D_ion[f] : m.D_pair[f - NI];
+                            const double gr = 2 * (double)fb[f * cap + n1] - 1.5 * u0 - 0.5 * (double)fb[f * cap + n2];
+                            if (!rd3d) {
+                                epart[f] += D * m.grad_mult * sf * gr;
+                            } else {
+                                const double v = D * sf * gr * m.inv_hc3;
+                                epart[f] += v;
+                                const int sl = dslot(f);
+                                if (sl >= 0) t0[(size_t)gterm * FD + sl] = (R)v;
+                            }
                         }
                     }
                 }
-#pragma unroll
-                for (int f = 0; f < FM; ++f) {
-                    if (f >= F) break;
-                    double v = warp_sum(part[f]);
-                    if (lane == 0) red[warp * FM + f] = v;
+            }
+            if constexpr (C > 1) {
+                // halo rows into the neighbours' write buffers; rim columns carry the
+                // rim value because the rim stores above may not be visible yet
+                for (int side = 0; side < 2; ++side) {
+                    const int nb = side == 0 ? rank - 1 : rank + 1;
+                    if (nb < 0 || nb >= C) continue;
+                    const int y = side == 0 ? lo : hi - 1;
+                    const int nlo = row_lo(nb, ny, C), nhi = row_lo(nb + 1, ny, C);
+                    const int nslo = nlo > 0 ? nlo - 1 : 0;
+                    const int nnr = (nhi < ny ? nhi + 1 : ny) - nslo;
+                    R* dst = peer<C>(fb, nb);
+                    for (int k = tid; k < F * nx * nz; k += blockDim.x) {
+                        const int f = k / (nx * nz), rem = k - f * nx * nz;
+                        const int z = rem / nx, x = rem - z * nx;
+                        const R v = (x == 0 || x == nx - 1 || y == 0 || y == ny - 1) ? rim_value(f, x, y)
+                                                                                    : fb[f * cap + x + nx * ((y - slo) + nr * z)];
+                        dst[f * cap + x + nx * ((y - nslo) + nnr * z)] = v;
+                    }
+                }
+                if (rd3d && phi > plo) {
+                    // cytosol halo planes
+                    for (int side = 0; side < 2; ++side) {
+                        const int nb = side == 0 ? rank - 1 : rank + 1;
+                        if (nb < 0 || nb >= C) continue;
+                        const int k = side == 0 ? plo : phi - 1;
+                        const int nplo = (int)(((long long)nb * nplanes) / C);
+                        const int nsplo = nplo > 0 ? nplo - 1 : 0;
+                        R* dst = peer<C>(cb, nb);
+                        for (int t = tid; t < CS * mc2; t += blockDim.x) {
+                            const int c = t / mc2, e = t - c * mc2;
+                            dst[c * ccap + (k - nsplo) * mc2 + e] = cb[c * ccap + (k - splo) * mc2 + e];
+                        }
+                    }
                 }
             }
+            if (rd3d && rank == 0) {
+                // cytosol layer 0 after this step: the rim values of the next step
+                R* lc = lay0 + par * CS * mc2;
+                for (int t = tid; t < CS * mc2; t += blockDim.x) {
+                    const int c = t / mc2, e = t - c * mc2;
+                    const R v = cb[c * ccap + e];  // plane 0 is local plane 0 on rank 0
+                    for (int r = 0; r < C; ++r) peer<C>(lc, r)[t] = v;
+                }
+            }
+            // warp partials -> rank partials (fixed order) -> every rank's slot
+#pragma unroll
+            for (int f = 0; f < NI + NPM; ++f) {
+                if (f < F) {
+                    const double v = warp_sum(epart[f]);
+                    if (lane == 0) redw[warp * FDn + f] = v;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NI; ++j) {
+                const double v = warp_sum(tpart[j]);
+                if (lane == 0) redw[warp * FDn + F + j] = v;
+            }
             __syncthreads();
-            { R* t = fa; fa = fb; fb = t; }
-            { R* t = ca; ca = cb; cb = t; }
+            if (warp == 0) {
+                for (int k = lane; k < FDn; k += 32) {
+                    double v = 0;
+                    for (int w = 0; w < W; ++w) v += redw[w * FDn + k];
+                    for (int r = 0; r < C; ++r) {
+                        if (k < F) peer<C>(rede, r)[(par * C + rank) * F + k] = v;
+                        else peer<C>(redt, r)[(par * C + rank) * NI + (k - F)] = v;
+                    }
+                }
+            }
+            cluster_barrier<C>();
+            {
+                R* t = fa;
+                fa = fb;
+                fb = t;
+            }
+            {
+                R* t = ca;
+                ca = cb;
+                cb = t;
+            }
         }
 
         // ---------------------------------------------------------- store
         if (warp == 0 && a.nsteps > 0) {
+            const int pl = (int)((a.nsteps - 1) & 1);
             for (int f = lane; f < F; f += 32) {
                 double e = 0;
-                for (int w = 0; w < W; ++w) e += red[w * FM + f];
+                for (int r = 0; r < C; ++r) e += rede[(pl * C + r) * F + f];
                 q.efflux[f] = e;
             }
-            for (int j = 0; j < NI; ++j) {
+            for (int j = lane; j < NI; j += 32) {
                 double t = 0;
-                for (int c = lane; c < nch; c += 32) t += fluxd[c * NI + j];
-                t = warp_sum(t);
-                if (lane == 0) q.total[j] = t;
+                for (int r = 0; r < C; ++r) t += redt[(pl * C + r) * NI + j];
+                q.total[j] = t;
             }
             __syncwarp();
             if (lane == 0) {
@@ -584,8 +807,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
                         q.nsr[i] = m.nsr[i];
                         q.jsr[i] = q.jsr_new[i];
                     }
-                // stream state at the next unconsumed draw
-                cbrng::State gd = g0;
+                cbrng::State gd = g0;  // stream state at the next unconsumed draw
                 rng_jump(a.pow2, gd, 2ULL * (unsigned long long)D);
                 for (int i = 0; i < 6; ++i) q.rng[i] = gd.s[i];
                 q.draws += (unsigned long long)D;
@@ -593,142 +815,281 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) k_resident(const __grid_consta
         }
         __syncthreads();
         {
-            int4* dst = (int4*)((R*)a.fields + st.node_base * F);
-            const int4* src = (const int4*)fa;
-            const int n16 = (int)((size_t)F * np * sizeof(R) / 16);
-            for (int k = tid; k < n16; k += blockDim.x) dst[k] = src[k];
-            const unsigned int* qs = (const unsigned int*)&q;
-            unsigned int* qd = (unsigned int*)(a.sc + s);
-            for (int k = tid; k < (int)(sizeof(cb_site_scalars) / 4); k += blockDim.x) qd[k] = qs[k];
-            R* cg = (R*)a.curgrid + st.node_base * NI;
-            for (int c = tid; c < nch; c += blockDim.x) {
-                a.ch_state[st.ch_off + c] = chs[c];
-                if (cho[c])
-                    for (int j = 0; j < NI; ++j) cg[j * np + chn[c]] = flux[c * NI + j];
+            R* g = (R*)a.fields + st.node_base * F;
+            for (int f = 0; f < F; ++f)
+                for (int z = 0; z < nz; ++z) {
+                    R* dst = g + (long long)f * np + (long long)nx * (lo + (long long)ny * z);
+                    const R* src = fa + f * cap + lstride * z + nx * (lo - slo);
+                    for (int k = tid; k < nx * (hi - lo); k += blockDim.x) dst[k] = src[k];
+                }
+            if (rank == 0) {
+                const unsigned int* qs = (const unsigned int*)&q;
+                unsigned int* qd = (unsigned int*)(a.sc + s);
+                for (int k = tid; k < (int)(sizeof(cb_site_scalars) / 4); k += blockDim.x) qd[k] = qs[k];
+                for (int c = tid; c < nch; c += blockDim.x) a.ch_state[st.ch_off + c] = chs[c];
             }
+            R* cg_ = (R*)a.curgrid + st.node_base * NI;
+            for (int c = tid; c < nch; c += blockDim.x)
+                if (chn[c] >= 0 && ((cho[c] >> 30) & 1))
+                    for (int j = 0; j < NI; ++j) cg_[(size_t)j * np + (cho[c] & ((1 << 30) - 1))] = flux[c * NI + j];
             if (rd3d) {
                 R* cd = (R*)a.cyto + (size_t)s * CS * nc;
-                for (int k = tid; k < CS * nc; k += blockDim.x) cd[k] = ca[k];
-                if (a.nsteps > 0) {
+                for (int c = 0; c < CS; ++c)
+                    for (int k = tid; k < (phi - plo) * mc2; k += blockDim.x)
+                        cd[(size_t)c * nc + (size_t)plo * mc2 + k] = ca[c * ccap + (plo - splo) * mc2 + k];
+                if (rank == 0 && a.nsteps > 0) {
+                    // deposit of the final Update, for the next launch
+                    const int pl = (int)((a.nsteps - 1) & 1);
                     const int* ptr = a.dep_ptr + (size_t)s * (mc2 + 1);
-                    for (int n = tid; n < mc2; n += blockDim.x)
+                    for (int cn = tid; cn < mc2; cn += blockDim.x)
                         for (int c = 0; c < CS; ++c) {
-                            int f = c < NI ? c : m.c_dyad_pair[c - NI];
-                            if (f >= 0 && c >= NI) f += NI;
+                            const int f = c < NI ? c : (m.c_dyad_pair[c - NI] >= 0 ? NI + m.c_dyad_pair[c - NI] : -1);
+                            const int sl = f >= 0 ? dslot(f) : -1;
                             double dep = 0;
-                            if (f >= 0)
-                                for (int kk = ptr[n]; kk < ptr[n + 1]; ++kk) dep += terms[a.dep_term[st.term_off + kk] * FM + f];
-                            a.cin[((size_t)s * CS + c) * mc2 + n] = dep;
+                            if (sl >= 0)
+                                for (int q2 = ptr[cn]; q2 < ptr[cn + 1]; ++q2)
+                                    dep += (double)terms[((size_t)pl * a.max_terms + a.dep_term[st.term_off + q2]) * FD + sl];
+                            a.cin[((size_t)s * CS + c) * mc2 + cn] = dep;
                         }
                 }
             }
         }
-        __syncthreads();
+        cluster_barrier<C>();
     }
 }
 
 size_t align16(size_t v) { return (v + 15) / 16 * 16; }
 
-// smem carve for the largest site; returns false if it exceeds the block limit
-bool plan(const cb_dev& d, rs_args& a, int FM) {
+// shared-memory carve for the sites `idx` with cluster size C
+bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<int>& idx, int C, rs_args& a) {
     const cb_model& m = d.m;
     const size_t rs = d.precision == 0 ? 8 : 4;
-    const int np = d.max_nodes;
-    size_t off = align16((size_t)m.F * np * rs);
-    a.np = np;
-    a.off_fb = (int)off;
-    off = align16(off + (size_t)m.F * np * rs);
-    const int CS = m.n_ions + m.c_n_pairs;
     const bool rd3d = m.cyto_type == CB_CYTO_RD3D;
+    // channel and efflux-term capacities are the batch maxima, so the plan of a
+    // class fits whenever the plan of its largest site does
+    int cap = 0, ccap = 0;
+    const int maxch = std::max(d.max_ch, 1), maxt = std::max(d.max_terms, 1);
+    for (int s : idx) {
+        const cb_site& st = sites[s];
+        if (st.ny < 3 * C) return false;  // every rank needs three rows (y-edge efflux)
+        for (int r = 0; r < C; ++r) {
+            int lo = (int)((long long)r * st.ny / C), hi = (int)((long long)(r + 1) * st.ny / C);
+            int slo = lo > 0 ? lo - 1 : 0, shi = hi < st.ny ? hi + 1 : st.ny;
+            cap = std::max(cap, (shi - slo) * st.nx * st.nz);
+        }
+    }
+    cap = (cap + 3) / 4 * 4;
+    const int CS = m.n_ions + m.c_n_pairs;
+    const int mc = m.mc, mc2 = mc * mc;
+    if (rd3d) {
+        if (mc - 1 < C) return false;
+        for (int r = 0; r < C; ++r) {
+            int plo = (int)((long long)r * (mc - 1) / C), phi = (int)((long long)(r + 1) * (mc - 1) / C);
+            int splo = plo > 0 ? plo - 1 : 0;
+            ccap = std::max(ccap, (phi + 1 - splo) * mc2);
+        }
+        ccap = (ccap + 3) / 4 * 4;
+    }
+    int FD = 0;
+    for (int f = 0; f < m.F; ++f)
+        if (f < m.n_ions || m.dyad_c_pair[f - m.n_ions] >= 0) ++FD;
+    const int F = m.F, NI = m.n_ions;
+    size_t off = align16((size_t)F * cap * rs);
+    a.off_fb = (int)off;
+    off = align16(off + (size_t)F * cap * rs);
     a.off_ca = (int)off;
-    if (rd3d) off = align16(off + (size_t)CS * d.nc * rs);
+    off = align16(off + (size_t)CS * ccap * rs);
     a.off_cb = (int)off;
-    if (rd3d) off = align16(off + (size_t)CS * d.nc * rs);
-    a.off_terms = (int)off;
-    if (rd3d) off = align16(off + (size_t)d.max_terms * FM * 8);
-    a.off_cin = (int)off;
-    if (rd3d) off = align16(off + (size_t)CS * m.mc * m.mc * 8);
+    off = align16(off + (size_t)CS * ccap * rs);
     a.off_mask = (int)off;
-    off = align16(off + (size_t)(np + 31) / 32 * 4);
-    const int mch = std::max(d.max_ch, 1);
+    off = align16(off + (size_t)(cap + 31) / 32 * 4);
     a.off_chn = (int)off;
-    off = align16(off + (size_t)mch * 4);
+    off = align16(off + (size_t)maxch * 4);
     a.off_chs = (int)off;
-    off = align16(off + (size_t)mch * 4);
+    off = align16(off + (size_t)maxch * 4);
     a.off_cho = (int)off;
-    off = align16(off + (size_t)mch * 4);
+    off = align16(off + (size_t)maxch * 4);
     a.off_flux = (int)off;
-    off = align16(off + (size_t)mch * m.n_ions * rs);
+    off = align16(off + (size_t)maxch * NI * rs);
     a.off_fluxd = (int)off;
-    off = align16(off + (size_t)mch * m.n_ions * 8);
+    off = align16(off + (size_t)maxch * NI * 8);
     a.off_mi = (int)off;
-    off = align16(off + (size_t)mch * m.n_ions * 8);
+    off = align16(off + (size_t)2 * maxch * NI * 8);
     a.off_ring = (int)off;
     off = align16(off + (size_t)RING * 8);
-    a.off_red = (int)off;
-    off = align16(off + (size_t)(MAX_THREADS / 32) * FM * 8);
+    a.off_redw = (int)off;
+    off = align16(off + (size_t)MAX_WARPS * (F + NI) * 8);
+    a.off_rede = (int)off;
+    off = align16(off + (size_t)2 * C * F * 8);
+    a.off_redt = (int)off;
+    off = align16(off + (size_t)2 * C * NI * 8);
+    a.off_lay0 = (int)off;
+    if (rd3d) off = align16(off + (size_t)2 * CS * mc2 * rs);
+    a.off_terms = (int)off;
+    if (rd3d) off = align16(off + (size_t)2 * maxt * FD * rs);
     a.off_sc = (int)off;
     off = align16(off + sizeof(cb_site_scalars));
     a.smem_bytes = (int)off;
-    a.max_ch = d.max_ch;
-    a.max_terms = d.max_terms;
-    return off <= 227 * 1024 - 1024;
+    a.cap_cleft = cap;
+    a.cap_cyto = ccap;
+    a.max_ch = maxch;
+    a.max_terms = maxt;
+    a.FD = FD;
+    return off <= (size_t)(227 * 1024 - 1024);
 }
 
-int pick_fm(int F) { return F <= 4 ? 4 : F <= 8 ? 8 : 16; }
+int pick_threads(const std::vector<cb_site>& sites, const std::vector<int>& idx, int C) {
+    long long mx = 0;
+    for (int s : idx) mx = std::max(mx, (long long)sites[s].nx * sites[s].ny * sites[s].nz / C);
+    long long t = ((mx / 8 + 31) / 32 + 1) * 32;
+    return (int)std::max(128LL, std::min((long long)MAX_THREADS, t));
+}
 
-template <typename R, int FM>
-cudaError_t launch(cb_dev& d, rs_args& a, int threads, cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(k_resident<R, FM>, cudaFuncAttributeMaxDynamicSharedMemorySize, a.smem_bytes);
+// dry: only query how many clusters of this shape can be resident (n_sites receives it)
+template <typename R, int NI, int NPM, int C>
+cudaError_t launch_one(const rs_args& a, int threads, cudaStream_t st, int n_sites, int* dry = nullptr) {
+    auto kern = k_resident<R, NI, NPM, C>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, a.smem_bytes);
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resident<R, FM>, threads, a.smem_bytes);
-    int grid = std::max(1, std::min(d.S, sms * std::max(per_sm, 1)));
-    k_resident<R, FM><<<grid, threads, a.smem_bytes, st>>>(a);
-    return cudaGetLastError();
+    if (C > 8) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = a.smem_bytes;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(C);
+    int clusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg);
+    if (e != cudaSuccess) return e;
+    if (dry) {
+        *dry = clusters;
+        return cudaSuccess;
+    }
+    if (clusters < 1) return cudaErrorInvalidConfiguration;
+    clusters = std::min(clusters, n_sites);
+    cfg.gridDim = dim3(clusters * C);
+    return cudaLaunchKernelEx(&cfg, kern, a);
 }
 
-int pick_threads(const cb_dev& d) {
-    // one worker thread per ~8 interior columns, between 4 and 32 warps
-    long long cols = 0;
-    (void)cols;
-    int nodes = d.max_nodes;
-    int t = ((nodes / 8 + 31) / 32 + 1) * 32;
-    return std::max(128, std::min(MAX_THREADS, t));
+template <typename R, int NI, int NPM>
+cudaError_t launch_c(const rs_args& a, int C, int threads, cudaStream_t st, int n, int* dry) {
+    switch (C) {
+    case 1: return launch_one<R, NI, NPM, 1>(a, threads, st, n, dry);
+    case 2: return launch_one<R, NI, NPM, 2>(a, threads, st, n, dry);
+    case 4: return launch_one<R, NI, NPM, 4>(a, threads, st, n, dry);
+    case 8: return launch_one<R, NI, NPM, 8>(a, threads, st, n, dry);
+    case 16: return launch_one<R, NI, NPM, 16>(a, threads, st, n, dry);
+    default: return cudaErrorInvalidConfiguration;
+    }
+}
+
+template <typename R>
+cudaError_t launch_t(const rs_args& a, int NI, int NP, int C, int threads, cudaStream_t st, int n, int* dry = nullptr) {
+    if (NI == 1 && NP <= 2) return launch_c<R, 1, 2>(a, C, threads, st, n, dry);
+    if (NI == 1 && NP <= 4) return launch_c<R, 1, 4>(a, C, threads, st, n, dry);
+    if (NI == 2 && NP <= 4) return launch_c<R, 2, 4>(a, C, threads, st, n, dry);
+    return cudaErrorInvalidConfiguration;
+}
+
+bool species_supported(const cb_model& m) { return (m.n_ions == 1 && m.n_pairs <= 4) || (m.n_ions == 2 && m.n_pairs <= 4); }
+
+// Size classes: each site goes to the smallest cluster size that holds it;
+// one launch per class, largest sites first within a class.
+bool classify(const cb_dev& d, const std::vector<cb_site>& sites, std::vector<std::vector<int>>& classes, std::vector<int>& cs) {
+    static const int sizes[5] = {1, 2, 4, 8, 16};
+    std::vector<std::vector<int>> by(5);
+    for (int s = 0; s < d.S; ++s) {
+        int k = 0;
+        while (k < 5 && sizes[k] < d.min_cluster) ++k;
+        for (; k < 5; ++k) {
+            rs_args a{};
+            std::vector<int> one{s};
+            if (plan(d, sites, one, sizes[k], a)) break;
+        }
+        if (k == 5) return false;
+        by[k].push_back(s);
+    }
+    classes.clear();
+    cs.clear();
+    for (int k = 0; k < 5; ++k)
+        if (!by[k].empty()) {
+            std::stable_sort(by[k].begin(), by[k].end(), [&](int x, int y) {
+                return (long long)sites[x].nx * sites[x].ny * sites[x].nz > (long long)sites[y].nx * sites[y].ny * sites[y].nz;
+            });
+            classes.push_back(by[k]);
+            cs.push_back(sizes[k]);
+        }
+    return true;
 }
 
 }  // namespace
 
-bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem) {
-    rs_args a{};
-    int FM = pick_fm(d.m.F);
-    // one ring refill must cover two draws per RyR (RING >= WINDOW + 2*max_ch)
-    bool ok = plan(d, a, FM) && 2 * d.max_ch <= WINDOW;
-    if (threads) *threads = pick_threads(d);
-    if (smem) *smem = (size_t)a.smem_bytes;
-    return ok;
+bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* why) {
+    auto no = [&](const std::string& w) {
+        if (why) *why = w;
+        return false;
+    };
+    if (!species_supported(d.m)) return no("species layout not specialised (1-2 ions, at most 4 ion-buffer pairs)");
+    if (2 * d.max_ch > WINDOW) return no("more than 256 RyRs in a site");
+    std::vector<cb_site> sites(d.S);
+    if (cudaMemcpy(sites.data(), d.sites, sizeof(cb_site) * d.S, cudaMemcpyDeviceToHost) != cudaSuccess) return no("cudaMemcpy");
+    std::vector<std::vector<int>> classes;
+    std::vector<int> cs;
+    if (!classify(d, sites, classes, cs)) return no("a site does not fit the shared memory of a 16-block cluster");
+    // every class must be schedulable (a 16-block cluster needs 16 SMs of one GPC)
+    for (size_t k = 0; k < classes.size(); ++k) {
+        rs_args a{};
+        if (!plan(d, sites, classes[k], cs[k], a)) return no("the shared-memory plan of a cluster class does not fit");
+        a.m = d.m;
+        int clusters = 0;
+        const int thr = pick_threads(sites, classes[k], cs[k]);
+        cudaError_t e = d.precision == 0 ? launch_t<double>(a, d.m.n_ions, d.m.n_pairs, cs[k], thr, 0, 0, &clusters)
+                                         : launch_t<float>(a, d.m.n_ions, d.m.n_pairs, cs[k], thr, 0, 0, &clusters);
+        if (e != cudaSuccess || clusters < 1) {
+            cudaGetLastError();
+            return no("clusters of " + std::to_string(cs[k]) + " blocks with " + std::to_string(a.smem_bytes) +
+                      " B of shared memory each cannot be resident (" + std::string(cudaGetErrorString(e)) + ", " +
+                      std::to_string(clusters) + " clusters)");
+        }
+        if (k == 0) {
+            if (threads) *threads = thr;
+            if (smem) *smem = (size_t)a.smem_bytes;
+        }
+        if (why) {
+            *why += (k ? ", " : "resident: ") + std::to_string(classes[k].size()) + " sites on clusters of " +
+                    std::to_string(cs[k]) + " (" + std::to_string(a.smem_bytes / 1024) + " KiB, " + std::to_string(thr) +
+                    " threads, " + std::to_string(clusters) + " resident)";
+        }
+    }
+    return true;
 }
 
 cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long* launches) {
     if (n <= 0) return cudaSuccess;
-    cb_dev& rsd = d;
-    if (!rsd.rs_order) {
-        // work queue order: largest cleft + cytosol first
-        std::vector<cb_site> sites(d.S);
-        cudaError_t e = cudaMemcpy(sites.data(), d.sites, sizeof(cb_site) * d.S, cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) return e;
-        std::vector<int> order(d.S);
-        for (int s = 0; s < d.S; ++s) order[s] = s;
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            return (long long)sites[x].nx * sites[x].ny * sites[x].nz > (long long)sites[y].nx * sites[y].ny * sites[y].nz;
-        });
-        if ((e = cudaMalloc(&rsd.rs_order, sizeof(int) * d.S)) != cudaSuccess) return e;
-        if ((e = cudaMemcpy(rsd.rs_order, order.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&rsd.rs_counter, sizeof(int))) != cudaSuccess) return e;
-        // MRG32k3a: A^(2^k) for k < 64, both components
-        std::vector<unsigned long long> p2(64 * 18);
+    std::vector<cb_site> sites(d.S);
+    cudaError_t e = cudaMemcpy(sites.data(), d.sites, sizeof(cb_site) * d.S, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return e;
+    std::vector<std::vector<int>> classes;
+    std::vector<int> cs;
+    if (!classify(d, sites, classes, cs)) return cudaErrorInvalidConfiguration;
+    if (classes.size() > 8) return cudaErrorInvalidConfiguration;
+    if (!d.rs_order) {
+        std::vector<int> order;
+        for (auto& c : classes) order.insert(order.end(), c.begin(), c.end());
+        if ((e = cudaMalloc(&d.rs_order, sizeof(int) * d.S)) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(d.rs_order, order.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&d.rs_counter, sizeof(int) * 8)) != cudaSuccess) return e;
+        // MRG32k3a: A^(2^k) for k < 64 (both components), then the refill jump A^(2*31*LANE_DRAWS)
+        std::vector<unsigned long long> p2(65 * 18);
         cbrng::Mat3 a1 = cbrng::step_matrix1(), a2 = cbrng::step_matrix2();
         for (int k = 0; k < 64; ++k) {
             for (int i = 0; i < 9; ++i) {
@@ -738,50 +1099,62 @@ cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long*
             a1 = cbrng::matmul(a1, a1, cbrng::M1);
             a2 = cbrng::matmul(a2, a2, cbrng::M2);
         }
-        if ((e = cudaMalloc(&rsd.rs_pow2, sizeof(unsigned long long) * p2.size())) != cudaSuccess) return e;
-        if ((e = cudaMemcpy(rsd.rs_pow2, p2.data(), sizeof(unsigned long long) * p2.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        cbrng::Mat3 j1{{{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}}, j2 = j1;
+        unsigned long long steps = 2ULL * 31 * LANE_DRAWS;
+        for (int k = 0; steps; ++k, steps >>= 1)
+            if (steps & 1ULL) {
+                cbrng::Mat3 b1, b2;
+                for (int i = 0; i < 9; ++i) {
+                    b1.a[i / 3][i % 3] = p2[18 * k + i];
+                    b2.a[i / 3][i % 3] = p2[18 * k + 9 + i];
+                }
+                j1 = cbrng::matmul(b1, j1, cbrng::M1);
+                j2 = cbrng::matmul(b2, j2, cbrng::M2);
+            }
+        for (int i = 0; i < 9; ++i) {
+            p2[18 * JUMP_ROW + i] = j1.a[i / 3][i % 3];
+            p2[18 * JUMP_ROW + 9 + i] = j2.a[i / 3][i % 3];
+        }
+        if ((e = cudaMalloc(&d.rs_pow2, sizeof(unsigned long long) * p2.size())) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(d.rs_pow2, p2.data(), sizeof(unsigned long long) * p2.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return e;
     }
-    rs_args a{};
-    const int FM = pick_fm(d.m.F);
-    if (!plan(d, a, FM)) return cudaErrorInvalidConfiguration;
-    a.m = d.m;
-    a.sites = d.sites;
-    a.order = rsd.rs_order;
-    a.S = d.S;
-    a.counter = rsd.rs_counter;
-    a.fields = d.fields[d.cur];
-    a.curgrid = d.curgrid;
-    a.ch_node = d.ch_node;
-    a.ch_owner = d.ch_owner;
-    a.ch_state = d.ch_state;
-    a.mouth = d.mouth;
-    a.NS = d.NS;
-    a.sc = d.sc;
-    a.cyto = d.cyto[d.ccur];
-    a.cin = d.cin;
-    a.rim_cnode = d.rim_cnode;
-    a.dep_ptr = d.dep_ptr;
-    a.dep_term = d.dep_term;
-    a.nc = d.nc;
-    a.pow2 = rsd.rs_pow2;
-    a.spx0 = d.spx[0];
-    a.spc0 = d.spc[0];
-    a.spx1 = d.spx[1];
-    a.spc1 = d.spc[1];
-    a.nsteps = n;
-    cudaError_t e = cudaMemsetAsync(rsd.rs_counter, 0, sizeof(int), st);
-    if (e != cudaSuccess) return e;
-    const int threads = pick_threads(d);
-    if (d.precision == 0) {
-        if (FM == 4) e = launch<double, 4>(d, a, threads, st);
-        else if (FM == 8) e = launch<double, 8>(d, a, threads, st);
-        else e = launch<double, 16>(d, a, threads, st);
-    } else {
-        if (FM == 4) e = launch<float, 4>(d, a, threads, st);
-        else if (FM == 8) e = launch<float, 8>(d, a, threads, st);
-        else e = launch<float, 16>(d, a, threads, st);
+    if ((e = cudaMemsetAsync(d.rs_counter, 0, sizeof(int) * 8, st)) != cudaSuccess) return e;
+    int offset = 0;
+    for (size_t k = 0; k < classes.size(); ++k) {
+        rs_args a{};
+        if (!plan(d, sites, classes[k], cs[k], a)) return cudaErrorInvalidConfiguration;
+        a.m = d.m;
+        a.sites = d.sites;
+        a.order = d.rs_order + offset;
+        a.S = (int)classes[k].size();
+        a.counter = d.rs_counter + k;
+        a.fields = d.fields[d.cur];
+        a.curgrid = d.curgrid;
+        a.ch_node = d.ch_node;
+        a.ch_owner = d.ch_owner;
+        a.ch_state = d.ch_state;
+        a.mouth = d.mouth;
+        a.NS = d.NS;
+        a.sc = d.sc;
+        a.cyto = d.cyto[d.ccur];
+        a.cin = d.cin;
+        a.rim_cnode = d.rim_cnode;
+        a.dep_ptr = d.dep_ptr;
+        a.dep_term = d.dep_term;
+        a.nc = d.nc;
+        a.pow2 = d.rs_pow2;
+        a.spx0 = d.spx[0];
+        a.spc0 = d.spc[0];
+        a.spx1 = d.spx[1];
+        a.spc1 = d.spc[1];
+        a.nsteps = n;
+        const int threads = pick_threads(sites, classes[k], cs[k]);
+        e = d.precision == 0 ? launch_t<double>(a, d.m.n_ions, d.m.n_pairs, cs[k], threads, st, a.S)
+                             : launch_t<float>(a, d.m.n_ions, d.m.n_pairs, cs[k], threads, st, a.S);
+        if (e != cudaSuccess) return e;
+        if (launches) *launches += 1;
+        offset += a.S;
     }
-    if (launches) *launches += 1;
-    return e;
+    return cudaSuccess;
 }

@@ -159,6 +159,9 @@ casim_status casim_b200_check_finite(casim_h h, int32_t* bad_site);
 casim_status casim_b200_get_all_mouth(casim_h h, int32_t species, double* out);  /* sum of channels */
 casim_status casim_b200_get_all_states(casim_h h, int32_t* out);
 
+/* How the resident path splits the batch into thread-block-cluster classes,
+ * or why the handle runs on the plain path. */
+casim_status casim_b200_path_note(casim_h h, char* buf, size_t n);
 /* Device timing of the last casim_b200_step call in milliseconds (CUDA events
  * recorded on the handle's stream around the launch sequence). */
 casim_status casim_b200_last_step_ms(casim_h h, double* out);

@@ -122,6 +122,23 @@ def _compare_batch(sim, orc, tol, scale_rel=False, check_states=True):
 def test_fp64_uneven_batch_matches_oracle(cuda_device, dim, cytosol, path):
     params, sites = configs.small_mixed(n_sites=5, seed=7 + dim, dim=dim, cytosol=cytosol)
     sim = _make(params, sites, "fp64", path)
+    _check_uneven(sim, params, sites, cytosol, path)
+
+
+@pytest.mark.parametrize("cluster", [2, 4])
+@pytest.mark.parametrize("dim,cytosol", [(2, "Pool"), (3, "Pool"), (3, "RD3D")])
+def test_fp64_sites_split_over_block_clusters(cuda_device, dim, cytosol, cluster):
+    """The resident path split over a thread-block cluster (rows and cytosol planes
+    per block, DSMEM exchange) gives the same results as the oracle."""
+    params, sites = configs.small_mixed(n_sites=5, seed=17 + dim, dim=dim, cytosol=cytosol, side=(14, 26))
+    if cytosol == "RD3D":
+        params["Cytosol"]["Nodes"] = 11
+    params["B200"] = {"MinClusterSize": cluster}
+    sim = _make(params, sites, "fp64", "resident")
+    _check_uneven(sim, params, sites, cytosol, "resident")
+
+
+def _check_uneven(sim, params, sites, cytosol, path):
     _resident_ok(sim, path)
     orc = oracle.OracleSim(params, sites)
     sim.start(sites["first_channel"])
