@@ -4,6 +4,7 @@
 """
 import os
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 import sys
 import sysconfig
 
@@ -11,8 +12,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcasim_b200.so")
-SOURCES = ["capi.cu", "plain.cu", "resident.cu", "noalloc.cu", "parse.cpp"]
-HEADERS = ["model.h", "engine.h", "physics.cuh", "mrg32k3a.cuh", "parse.h"]
+SOURCES = ["resident_f64_z3.cu", "resident_f32_z3.cu", "resident_f64_z1.cu", "resident_f32_z1.cu", "capi.cu", "plain.cu",
+           "resident.cu", "noalloc.cu", "parse.cpp"]
+HEADERS = ["model.h", "engine.h", "physics.cuh", "mrg32k3a.cuh", "parse.h", "resident_kernel.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -44,9 +46,14 @@ def build(force=False, verbose=False, extra=()):
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     common = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + json_include(), "-I" + os.path.join(ROOT, "include")]
-    objs = []
-    for src in SOURCES:
+    hdr_t = max(os.path.getmtime(os.path.join(CSRC, h)) for h in HEADERS)
+    hdr_t = max(hdr_t, os.path.getmtime(os.path.join(ROOT, "include", "casim_b200.h")), os.path.getmtime(__file__))
+
+    def one(src):
         obj = os.path.join(objdir, src + ".o")
+        if (not force and os.path.exists(obj) and os.path.getmtime(obj) > max(hdr_t, os.path.getmtime(os.path.join(CSRC, src)))
+                and not extra and not verbose):
+            return obj, ""
         cmd = [nvcc()] + ARCH + common + list(extra) + ["-c", os.path.join(CSRC, src), "-o", obj]
         if src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"] if verbose else []
@@ -55,9 +62,15 @@ def build(force=False, verbose=False, extra=()):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, r.stdout, r.stderr))
-        if verbose:
-            sys.stderr.write(r.stderr)
-        objs.append(obj)
+        return obj, r.stderr
+
+    jobs = max(1, min(len(SOURCES), os.cpu_count() or 1))
+    with ThreadPoolExecutor(jobs) as ex:
+        results = list(ex.map(one, SOURCES))
+    objs = [o for o, _ in results]
+    if verbose:
+        for _, err in results:
+            sys.stderr.write(err)
     cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

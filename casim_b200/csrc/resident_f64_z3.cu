@@ -1,0 +1,7 @@
+// Resident-path kernels for double fields and 3 cleft layer(s): one translation
+// unit per (precision, layers) so the specialisations compile in parallel.
+#include "resident_kernel.cuh"
+
+cudaError_t cb_res_f64_z3(const cbres::rs_args& a, int NI, int NP, int C, int threads, cudaStream_t st, int n, int* dry) {
+    return cbres::dispatch<double, 3>(a, NI, NP, C, threads, st, n, dry);
+}

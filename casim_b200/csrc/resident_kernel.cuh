@@ -1,0 +1,1019 @@
+// Resident path kernel: each site lives in the shared memory of a thread-block
+// cluster (1..16 blocks, one per SM) for all K time steps of a launch, so HBM
+// is touched once per site per launch. Host logic: resident.cu.
+//
+// Layout of a site over the C blocks (ranks) of its cluster:
+//   cleft   rows y in [lo_r, hi_r) per rank (lo_r = r*ny/C), stored with one halo
+//           row on each side, all x and z, every stored species, ping-pong;
+//   RD3D    cytosol planes k in [plo_r, phi_r) of the updated range [0, mc-1),
+//           stored with one halo plane on each side, ping-pong.
+// Per step (the reference loop body CaSim/ParallelHybridSolver.cpp:532-540
+// followed by Update(), :270-286):
+//   phase A  warp 0: RyR gating (CaSim/DyadChannels.cpp:97-130);
+//            warp 1: reductions of the previous Update, jSR coupling, cytosol
+//            pool ODE (CaSim/CytosolPool.cpp:217-288), jSR ODE (CaSim/SRPool.cpp:70-89);
+//            both run redundantly and bit-identically on every rank;
+//            warps 2..: cleft stencil of the rank's rows (CaSim/DyadRD2DCPU.cpp:394-490,
+//            CaSim/DyadRDCPU.cpp:404-506), a lane marching down a strip of rows
+//            with the previous, current and next row in registers, and the
+//            RD3D cytosol planes, marching along z.
+//   phase B  Dirichlet rim, mouth gather, RyR currents, efflux
+//            (CaSim/DyadRD2DCPU.cpp:243-392) of the rank's rows; halo rows and
+//            planes, mouth values, partial sums and RD3D coupling values are
+//            stored into the peers' shared memory (DSMEM) in slots double-
+//            buffered by step parity.
+//   one cluster barrier (release/acquire) per step.
+//
+// RyR gating consumes the site's MRG32k3a stream in exactly the reference's
+// order without its serial loop: warp 0 keeps a ring of pre-generated draws
+// (32 lanes x 16 contiguous draws per refill, lanes jumped ahead by matrix
+// powers) and resolves 32 channels per ballot, re-evaluating after each
+// transition, which consumes one extra draw.
+#pragma once
+#include <cooperative_groups.h>
+
+#include "engine.h"
+#include "mrg32k3a.cuh"
+#include "physics.cuh"
+
+namespace cbres {
+
+namespace cg = cooperative_groups;
+
+constexpr int RING = 1024;               // pre-generated draws per site
+constexpr int LANE_DRAWS = 16;           // contiguous draws per lane per refill
+constexpr int WINDOW = 32 * LANE_DRAWS;  // draws per refill
+constexpr int MAX_THREADS = 512;
+constexpr int MAX_WARPS = MAX_THREADS / 32;
+constexpr int JUMP_ROW = 64;             // pow table row holding A^(2*31*LANE_DRAWS)
+
+// Threads per block a kernel is compiled for. A stencil lane keeps three rows
+// of CSM species x NZ layers in registers; FP64 3D layouts with many species
+// get 255 registers per thread (256 threads) instead of 128 (512 threads).
+__host__ __device__ constexpr int max_threads(int rbytes, int csm, int nz) { return 3 * nz * csm * rbytes / 4 > 60 ? 256 : 512; }
+// pair capacity of the kernel specialisation that serves NI ions and NP pairs
+__host__ __device__ constexpr int npm_of(int NI, int NP) { return (NI == 1 && NP <= 2) ? 2 : 4; }
+
+// Stencil constants in the field precision R, so that they are kernel-parameter
+// operands of the arithmetic (each value is the (R) cast of the model's double,
+// or of the product noted).
+template <typename R>
+struct rs_const {
+    R D_ion[CB_MAX_IONS], K1[CB_MAX_IONS], K2[CB_MAX_IONS];
+    R A1[CB_MAX_IONS], A2[CB_MAX_IONS];  // (R)(N1*K1), (R)(N2*K2)
+    R D_pair[CB_MAX_PAIRS], kon[CB_MAX_PAIRS], koff[CB_MAX_PAIRS];
+    R ctp[CB_MAX_PAIRS];                 // total of the pair's buffer
+    int same[CB_MAX_PAIRS];              // bit p2: pair p2 binds the same buffer
+    R idx2, idy2, idz2, dt, ih2;
+    // RD3D cytosol species c: ions, then cytosol pairs at NI + p
+    R cD[CB_MAX_CSPECIES], ckon[CB_MAX_CSPECIES], ckoff[CB_MAX_CSPECIES], cctp[CB_MAX_CSPECIES];
+    int csame[CB_MAX_CSPECIES];          // bit c2: species c2 is a pair of the same buffer
+    int cdep[CB_MAX_CSPECIES];           // deposit slot feeding species c, or -1
+    R Kup2[CB_MAX_IONS], bg2[CB_MAX_IONS], Jmax[CB_MAX_IONS];  // by SERCA index: (R)(Kup^2), (R)(bg^2)
+};
+
+struct rs_args {
+    cb_model m;
+    rs_const<float> kf;
+    rs_const<double> kd;
+    const cb_site* sites;
+    const int* order;  // sites of this launch, largest first
+    int S;             // sites in order[]
+    int* counter;
+    void* fields;
+    void* curgrid;
+    const int* ch_node;
+    const int* ch_owner;
+    int* ch_state;
+    double* mouth;
+    int NS;
+    cb_site_scalars* sc;
+    void* cyto;
+    double* cin;
+    const int* rim_cnode;
+    const int* dep_ptr;
+    const int* dep_term;
+    int nc;
+    const unsigned long long* pow2;  // [65][2][9]: A^(2^k) for k < 64, then the refill jump
+    const double* spx0;
+    const double* spc0;
+    const double* spx1;
+    const double* spc1;
+    long long nsteps;
+    // shared-memory carve (bytes, identical for every block of the launch)
+    int cap_cleft;  // stored cleft nodes per species per rank
+    int cap_cyto;   // stored cytosol nodes per species per rank
+    int max_ch, max_terms, FD;
+    int off_fb, off_ca, off_cb, off_chidx, off_chn, off_chs, off_cho, off_ftab, off_fluxd, off_mi, off_ring,
+        off_redw, off_rede, off_redt, off_lay0, off_terms, off_sc, smem_bytes;
+};
+
+// ---- MRG32k3a arithmetic by folding: m1 = 2^32 - 209, m2 = 2^32 - 22853 ----
+template <unsigned long long M>
+__device__ __forceinline__ unsigned long long fold_mod(unsigned long long x) {
+    constexpr unsigned long long c = (1ULL << 32) - M;
+    unsigned long long t = (x >> 32) * c + (x & 0xffffffffULL);
+    t = (t >> 32) * c + (t & 0xffffffffULL);
+    return t >= M ? t - M : t;
+}
+
+__device__ __forceinline__ double u01_fast(cbrng::State& g) {
+    unsigned long long a = fold_mod<cbrng::M1>(cbrng::A12 * g.s[1]);
+    unsigned long long b = fold_mod<cbrng::M1>(cbrng::A13N * g.s[0]);
+    const unsigned long long p1 = a >= b ? a - b : a + cbrng::M1 - b;
+    g.s[0] = g.s[1];
+    g.s[1] = g.s[2];
+    g.s[2] = (unsigned int)p1;
+    a = fold_mod<cbrng::M2>(cbrng::A21 * g.s[5]);
+    b = fold_mod<cbrng::M2>(cbrng::A23N * g.s[3]);
+    const unsigned long long p2 = a >= b ? a - b : a + cbrng::M2 - b;
+    g.s[3] = g.s[4];
+    g.s[4] = g.s[5];
+    g.s[5] = (unsigned int)p2;
+    const double norm = 1.0 / (4294967087.0 + 1.0);
+    const double d1 = (double)p1, d2 = (double)p2;
+    return (p1 > p2) ? __dmul_rn(d1 - d2, norm) : __dmul_rn(__dadd_rn(d1 - d2, 4294967087.0), norm);
+}
+
+// RandU01 with incPrec (CaSim/rngstream.cpp:271-283), no FMA contraction
+__device__ __forceinline__ double u01d_fast(cbrng::State& g) {
+    double u = u01_fast(g);
+    const double v = u01_fast(g);
+    u = __dadd_rn(u, __dmul_rn(v, 5.9604644775390625e-8));
+    return (u < 1.0) ? u : (u - 1.0);
+}
+
+template <unsigned long long M>
+__device__ __forceinline__ void mat_apply(const unsigned long long* A, unsigned int* v) {
+    unsigned long long r[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        unsigned long long acc = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            acc += fold_mod<M>(A[3 * i + k] * (unsigned long long)v[k]);
+            if (acc >= M) acc -= M;
+        }
+        r[i] = acc;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = (unsigned int)r[i];
+}
+
+__device__ __forceinline__ void jump_row(const unsigned long long* pow2, cbrng::State& g, int k) {
+    mat_apply<cbrng::M1>(pow2 + 18 * k, g.s);
+    mat_apply<cbrng::M2>(pow2 + 18 * k + 9, g.s + 3);
+}
+
+// advance by `steps` recurrence steps (binary powering with the 2^k table)
+__device__ __forceinline__ void rng_jump(const unsigned long long* pow2, cbrng::State& g, unsigned long long steps) {
+    for (int k = 0; steps; ++k, steps >>= 1)
+        if (steps & 1ULL) jump_row(pow2, g, k);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int C>
+__device__ __forceinline__ void cluster_barrier() {
+    if constexpr (C == 1) __syncthreads();
+    else cg::this_cluster().sync();
+}
+
+// pointer to `p` (this block's shared memory) in the shared memory of rank r
+template <int C, typename T>
+__device__ __forceinline__ T* peer(T* p, int r) {
+    if constexpr (C == 1) return p;
+    else return cg::this_cluster().map_shared_rank(p, r);
+}
+
+__host__ __device__ __forceinline__ int row_lo(int r, int ny, int C) { return (int)(((long long)r * ny) / C); }
+
+// deposit slot of dyad species f (its index among species with a cytosol counterpart), or -1
+__device__ __forceinline__ int dslot(const cb_model& m, int NI, int f) {
+    int k = 0;
+    for (int g = 0; g < f; ++g)
+        if (g < NI || m.dyad_c_pair[g - NI] >= 0) ++k;
+    return (f < NI || m.dyad_c_pair[f - NI] >= 0) ? k : -1;
+}
+
+template <typename R, int NI, int NPM, int NZ, int C>
+__global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_resident(const __grid_constant__ rs_args a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_site;
+    // RNG of warp 0, kept in shared memory so it holds no registers during the stencils:
+    // lane l's stream at draw s_we + l*LANE_DRAWS; s_D draws consumed
+    __shared__ unsigned int s_rng[32 * 6];
+    __shared__ long long s_D, s_we;
+    constexpr int CSM = NI + NPM;  // cytosol species capacity
+    const cb_model& m = a.m;
+    const int NP = m.n_pairs, F = NI + NP;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, W = blockDim.x >> 5;
+    int rank = 0;
+    if constexpr (C > 1) rank = (int)cg::this_cluster().block_rank();
+    const bool rd3d = m.cyto_type == CB_CYTO_RD3D;
+    const int mc = m.mc, mc2 = mc * mc, nc = a.nc, CS = m.n_ions + m.c_n_pairs;
+    const int FD = a.FD;
+
+    R* fa = (R*)smem;
+    R* fb = (R*)(smem + a.off_fb);
+    R* ca = (R*)(smem + a.off_ca);
+    R* cb = (R*)(smem + a.off_cb);
+    unsigned short* chidx = (unsigned short*)(smem + a.off_chidx);  // 1 + owning RyR at a node, 0 if none
+    int* chn = (int*)(smem + a.off_chn);   // local node of own RyRs, -1 otherwise
+    int* chs = (int*)(smem + a.off_chs);   // state of every RyR of the site
+    int* cho = (int*)(smem + a.off_cho);   // site node (x + nx*(y + ny*z)) | owner flag in bit 30
+    R* ftab = (R*)(smem + a.off_ftab);     // [(1 + max_ch)][NI]: RyR currents, slot 0 is zero
+    double* fluxd = (double*)(smem + a.off_fluxd);
+    double* mi = (double*)(smem + a.off_mi);      // [2][max_ch][NI]
+    double* ring = (double*)(smem + a.off_ring);
+    double* redw = (double*)(smem + a.off_redw);  // [MAX_WARPS][F + NI]
+    double* rede = (double*)(smem + a.off_rede);  // [2][C][F]
+    double* redt = (double*)(smem + a.off_redt);  // [2][C][NI]
+    R* lay0 = (R*)(smem + a.off_lay0);            // [2][CS][mc2]
+    R* terms = (R*)(smem + a.off_terms);          // [2][max_terms][FD]
+    cb_site_scalars& q = *(cb_site_scalars*)(smem + a.off_sc);
+
+    const rs_const<R>& K = *[&]() {
+        if constexpr (sizeof(R) == 4) return &a.kf;
+        else return &a.kd;
+    }();
+    const double dt = m.dt;
+    const int FDn = F + NI;
+
+    for (;;) {
+        if (rank == 0 && tid == 0) {
+            const int v = atomicAdd(a.counter, 1);
+            for (int r = 0; r < C; ++r) *peer<C>(&s_site, r) = v;
+        }
+        cluster_barrier<C>();
+        const int qsite = s_site;
+        if (qsite >= a.S) break;
+        const int s = a.order[qsite];
+        const cb_site st = a.sites[s];
+        const int nx = st.nx, ny = st.ny, nz = st.nz, nxy = nx * ny, np = st.npad;
+        const int nch = st.n_ch;
+        const int zmax = NZ == 1 ? 1 : nz - 1;
+        const int lo = row_lo(rank, ny, C), hi = row_lo(rank + 1, ny, C);
+        const int slo = lo > 0 ? lo - 1 : 0, shi = hi < ny ? hi + 1 : ny;
+        const int nr = shi - slo;
+        const int lstride = nx * nr;  // z stride in local storage
+        const int nloc = lstride * nz;
+        const int nplanes = mc - 1;
+        const int plo = rd3d ? (int)(((long long)rank * nplanes) / C) : 0;
+        const int phi = rd3d ? (int)(((long long)(rank + 1) * nplanes) / C) : 0;
+        const int splo = plo > 0 ? plo - 1 : 0, sphi = phi + 1;
+        const int cloc = (sphi - splo) * mc2;
+        const int cap = a.cap_cleft, ccap = a.cap_cyto;
+
+        // ---------------------------------------------------------- load
+        {
+            const R* g = (const R*)a.fields + st.node_base * F;
+            for (int f = 0; f < F; ++f)
+                for (int z = 0; z < nz; ++z) {
+                    const R* src = g + (long long)f * np + (long long)nx * (slo + (long long)ny * z);
+                    for (int k = tid; k < lstride; k += blockDim.x) {
+                        const R v = src[k];
+                        fa[f * cap + lstride * z + k] = v;
+                        fb[f * cap + lstride * z + k] = v;
+                    }
+                }
+            for (int k = tid; k < nloc; k += blockDim.x) chidx[k] = 0;
+            const unsigned int* qs = (const unsigned int*)(a.sc + s);
+            unsigned int* qd = (unsigned int*)&q;
+            for (int k = tid; k < (int)(sizeof(cb_site_scalars) / 4); k += blockDim.x) qd[k] = qs[k];
+            for (int k = tid; k < NI; k += blockDim.x) ftab[k] = (R)0;
+            if (rd3d) {
+                const R* cs = (const R*)a.cyto + (size_t)s * CS * nc;
+                for (int c = 0; c < CS; ++c)
+                    for (int k = tid; k < cloc; k += blockDim.x) {
+                        const R v = cs[(size_t)c * nc + (size_t)splo * mc2 + k];
+                        ca[c * ccap + k] = v;
+                        cb[c * ccap + k] = v;
+                    }
+                // cytosol layer 0 at entry: the rim values of the first step (parity-1 slot)
+                for (int c = 0; c < CS; ++c)
+                    for (int k = tid; k < mc2; k += blockDim.x) lay0[(CS + c) * mc2 + k] = cs[(size_t)c * nc + k];
+            }
+        }
+        __syncthreads();
+        for (int c = tid; c < nch; c += blockDim.x) {
+            const int gnode = a.ch_node[st.ch_off + c];
+            const int x = gnode % nx, y = (gnode / nx) % ny, z = gnode / nxy;
+            chs[c] = a.ch_state[st.ch_off + c];
+            const bool owner = a.ch_owner[st.ch_off + c] != 0;
+            cho[c] = gnode | (owner ? (1 << 30) : 0);
+            const bool own = y >= lo && y < hi;
+            const int ln = own ? x + nx * ((y - slo) + nr * z) : -1;
+            chn[c] = ln;
+            const double* mo = a.mouth + (size_t)(st.ch_off + c) * a.NS;
+            for (int j = 0; j < NI; ++j) mi[(a.max_ch + c) * NI + j] = mo[j];  // parity-1 slot
+            if (own) {
+                if (owner) chidx[ln] = (unsigned short)(1 + c);
+                for (int j = 0; j < NI; ++j) {
+                    // current of the last Update: state * g * (jSR - Ca at the node)
+                    const double fl = chs[c] * (m.g[j] * (q.jsr_new[j] - (double)fa[j * cap + ln]));
+                    ftab[(1 + c) * NI + j] = (R)fl;
+                    fluxd[c * NI + j] = fl;
+                }
+            }
+        }
+        // RNG (warp 0): lane l holds the stream at draw D + l*LANE_DRAWS of the next window
+        if (warp == 0) {
+            cbrng::State gl;
+            for (int i = 0; i < 6; ++i) gl.s[i] = q.rng[i];
+            rng_jump(a.pow2, gl, 2ULL * LANE_DRAWS * lane);
+            for (int i = 0; i < 6; ++i) s_rng[lane * 6 + i] = gl.s[i];
+            if (lane == 0) s_D = s_we = 0;
+        }
+        cluster_barrier<C>();
+
+        // ---------------------------------------------------------- steps
+        for (long long it = 0; it < a.nsteps; ++it) {
+            const int par = (int)(it & 1), prv = par ^ 1;
+            const bool last = it == a.nsteps - 1;
+            if (warp == 0) {
+                // ---- RyR gating: draw D+i tests channel i until a transition takes one more draw
+                long long D = s_D;
+                const long long we = s_we;
+                if (we - D < 2LL * nch) {  // ring refill: at least two draws per channel available
+                    cbrng::State gl;
+                    for (int i = 0; i < 6; ++i) gl.s[i] = s_rng[lane * 6 + i];
+                    const long long base = we + (long long)lane * LANE_DRAWS;
+                    for (int i = 0; i < LANE_DRAWS; ++i) ring[(base + i) & (RING - 1)] = u01d_fast(gl);
+                    jump_row(a.pow2, gl, JUMP_ROW);  // to this lane's chunk of the next window
+                    for (int i = 0; i < 6; ++i) s_rng[lane * 6 + i] = gl.s[i];
+                    __syncwarp();
+                    if (lane == 0) s_we = we + WINDOW;
+                }
+                __syncwarp();
+                const double* mprev = mi + prv * a.max_ch * NI;
+                for (int base = 0; base < nch; base += 32) {
+                    const int c = base + lane;
+                    const int cnt = min(32, nch - base);
+                    const bool act = lane < cnt;
+                    double p = 0;
+                    int stt = 0;
+                    if (act) {
+                        stt = chs[c];
+                        const double cam = mprev[c * NI + m.ca_idx];
+                        const double mgm = m.mg_idx >= 0 ? mprev[c * NI + m.mg_idx] : 0.0;
+                        p = cb_rate(m, a.spx0, a.spc0, a.spx1, a.spc1, stt, cam, mgm) * dt;
+                    }
+                    int start = 0;
+                    while (start < cnt) {
+                        const bool rem = act && lane >= start;
+                        const double u = rem ? ring[(D + (lane - start)) & (RING - 1)] : 2.0;
+                        const unsigned int t = __ballot_sync(0xffffffffu, rem && (u < p));
+                        if (t == 0u) {
+                            D += cnt - start;
+                            break;
+                        }
+                        const int f = __ffs(t) - 1;
+                        if (lane == f) chs[c] = 1 - stt;
+                        D += (f - start) + 2;
+                        start = f + 1;
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) s_D = D;
+            } else if (warp == 1) {
+                // ---- pools: reductions of the previous Update (rank order on every rank)
+                if (it > 0) {
+                    for (int f = lane; f < F; f += 32) {
+                        double e = 0;
+                        for (int r = 0; r < C; ++r) e += rede[(prv * C + r) * F + f];
+                        q.efflux[f] = e;
+                    }
+                    for (int j = lane; j < NI; j += 32) {
+                        double t = 0;
+                        for (int r = 0; r < C; ++r) t += redt[(prv * C + r) * NI + j];
+                        q.total[j] = t;
+                    }
+                    __syncwarp();
+                    if (lane == 0 && !m.jsr_const)
+                        for (int i = 0; i < NI; ++i) {
+                            q.IjSR[i] = q.total[i] * m.V_elem;
+                            q.nsr[i] = m.nsr[i];
+                            q.jsr[i] = q.jsr_new[i];
+                        }
+                    __syncwarp();
+                }
+                if (lane == 0) {
+                    if (!rd3d) {
+                        // cytosol pool ODE (CaSim/CytosolPool.cpp:217-288)
+                        double evo_i[CB_MAX_IONS], evo_p[CB_MAX_CPAIRS];
+                        int ipd = 0, is = 0;
+                        for (int j = 0; j < NI; ++j) {
+                            double react = 0;
+                            for (int p = 0; p < m.c_n_pairs; ++p) {
+                                if (m.c_pair_ion[p] != j) continue;
+                                const double R1 = m.c_koff[p] * q.c_pairs[p] - m.c_kon[p] * q.c_ions[j] * q.c_free[m.c_pair_buf[p]];
+                                evo_p[p] = -R1;
+                                react += R1;
+                                if (m.c_in_dyad[p]) evo_p[p] += q.efflux[NI + ipd++];
+                            }
+                            evo_i[j] = react + q.efflux[j];
+                            if (m.c_serca[j]) {
+                                const double i2 = q.c_ions[j] * q.c_ions[j];
+                                const double K2 = m.c_Kup[is] * m.c_Kup[is];
+                                const double b2 = m.c_bg[is] * m.c_bg[is];
+                                evo_i[j] -= m.c_Jmax[is] * (i2 / (i2 + K2) - b2 / (b2 + K2));
+                                ++is;
+                            }
+                        }
+                        for (int j = 0; j < NI; ++j) {
+                            evo_i[j] -= m.c_onetau_ion[j] * (q.c_ions[j] - m.c_bg[j]);
+                            q.c_ions[j] += evo_i[j] * dt;
+                        }
+                        ipd = 0;
+                        for (int p = 0; p < m.c_n_pairs; ++p) {
+                            evo_p[p] -= m.c_onetau_pair[p] * (q.c_pairs[p] - m.c_init[p]);
+                            q.c_pairs[p] += evo_p[p] * dt;
+                            if (m.c_in_dyad[p]) q.c_bnd[ipd++] = q.c_pairs[p];
+                        }
+                        for (int b = 0; b < m.c_n_buf; ++b) q.c_free[b] = m.c_Ctot[b];
+                        for (int p = 0; p < m.c_n_pairs; ++p) q.c_free[m.c_pair_buf[p]] -= q.c_pairs[p];
+                    }
+                    // jSR ODE (CaSim/SRPool.cpp:70-89) with the site's own beta
+                    if (!m.jsr_const) {
+                        double beta = 1;
+                        for (int j = 0; j < NI; ++j)
+                            beta += m.nCQ[j] * m.K_CQ[j] * m.CQ / ((m.K_CQ[j] + q.jsr[j]) * (m.K_CQ[j] + q.jsr[j]));
+                        for (int i = 0; i < NI; ++i) {
+                            const double Iref = 1 / m.tau_refill[i] * (q.nsr[i] - q.jsr[i]);
+                            q.jsr_new[i] = q.jsr[i] + dt / beta * (Iref - q.IjSR[i] / m.V_jsr);
+                        }
+                        if (m.ca_idx >= 0) q.release += q.IjSR[m.ca_idx] * dt;
+                    }
+                }
+                __syncwarp();
+            } else {
+                // ---- worker warps: cleft stencil, strips of rows with a lane per x;
+                // constants are kernel-parameter operands (K), not registers
+                const int wk = warp - 2, NW = W - 2;
+                const int ylo = max(lo, 1), yhi = min(hi, ny - 1);
+                const int nrows = yhi - ylo;
+                const int XB = (nx - 2 + 31) >> 5;
+                const int RS = max(2, (nrows * XB + NW - 1) / NW);
+                const int nchunk = (nrows + RS - 1) / RS;
+                for (int sI = wk; sI < XB * nchunk; sI += NW) {
+                    const int ch = sI / XB;
+                    const int x = 1 + ((sI - ch * XB) << 5) + lane;
+                    if (x > nx - 2) continue;
+                    const int y0 = ylo + ch * RS, y1 = min(y0 + RS, yhi);
+                    // previous / current / next row of every species and layer
+                    R vP[CSM][NZ], vC[CSM][NZ], vN[CSM][NZ];
+#pragma unroll
+                    for (int f = 0; f < CSM; ++f)
+#pragma unroll
+                        for (int z = 0; z < NZ; ++z) vP[f][z] = vC[f][z] = vN[f][z] = (R)0;
+                    {
+                        const int n0 = x + nx * (y0 - slo);
+#pragma unroll
+                        for (int f = 0; f < CSM; ++f)
+#pragma unroll
+                            for (int z = 0; z < NZ; ++z)
+                                if (f < F) {
+                                    vP[f][z] = fa[f * cap + n0 - nx + lstride * z];
+                                    vC[f][z] = fa[f * cap + n0 + lstride * z];
+                                }
+                    }
+                    for (int y = y0; y < y1; ++y) {
+                        const int nrow = x + nx * (y - slo);
+#pragma unroll
+                        for (int f = 0; f < CSM; ++f)
+#pragma unroll
+                            for (int z = 0; z < NZ; ++z)
+                                if (f < F) vN[f][z] = fa[f * cap + nrow + nx + lstride * z];
+#pragma unroll
+                        for (int z = 0; z < NZ; ++z) {
+                            const int n = nrow + lstride * z;
+                            const int zl = z == 0 ? (NZ > 1 ? 1 : 0) : z - 1;
+                            const int zr = z == NZ - 1 ? (NZ > 1 ? NZ - 2 : 0) : z + 1;
+                            R ei[NI], ep[NPM];
+#pragma unroll
+                            for (int j = 0; j < NI; ++j) {
+                                const R cc = vC[j][z];
+                                R lap = (fa[j * cap + n + 1] - 2 * cc + fa[j * cap + n - 1]) * K.idx2 + (vN[j][z] - 2 * cc + vP[j][z]) * K.idy2;
+                                if constexpr (NZ > 1) lap = lap + (vC[j][zr] - 2 * cc + vC[j][zl]) * K.idz2;
+                                ei[j] = K.D_ion[j] * lap;
+                            }
+#pragma unroll
+                            for (int p = 0; p < NPM; ++p) {
+                                ep[p] = 0;
+                                if (p < NP && K.D_pair[p] != (R)0) {
+                                    const R cc = vC[NI + p][z];
+                                    const R* v = fa + (NI + p) * cap;
+                                    R lap = (v[n + 1] - 2 * cc + v[n - 1]) * K.idx2 + (vN[NI + p][z] - 2 * cc + vP[NI + p][z]) * K.idy2;
+                                    if constexpr (NZ > 1) lap = lap + (vC[NI + p][zr] - 2 * cc + vC[NI + p][zl]) * K.idz2;
+                                    ep[p] = K.D_pair[p] * lap;
+                                }
+                            }
+                            // reactions: R1 = koff*B - kon*ion*free, free = total minus the
+                            // buffer's pairs in pair order (CaSim/DyadRD2DCPU.cpp:415-456)
+                            R Rj[NI];
+#pragma unroll
+                            for (int j = 0; j < NI; ++j) Rj[j] = 0;
+#pragma unroll
+                            for (int p = 0; p < NPM; ++p) {
+                                if (p < NP) {
+                                    R fr = K.ctp[p];
+#pragma unroll
+                                    for (int p2 = 0; p2 < NPM; ++p2)
+                                        if ((K.same[p] >> p2) & 1) fr -= vC[NI + p2][z];
+                                    R ion = vC[0][z];
+#pragma unroll
+                                    for (int j = 1; j < NI; ++j)
+                                        if (m.pair_ion[p] == j) ion = vC[j][z];
+                                    const R r1 = K.koff[p] * vC[NI + p][z] - K.kon[p] * ion * fr;
+                                    ep[p] += -r1;
+#pragma unroll
+                                    for (int j = 0; j < NI; ++j)
+                                        if (m.pair_ion[p] == j) Rj[j] += r1;
+                                }
+                            }
+                            const int ci = chidx[n];
+#pragma unroll
+                            for (int j = 0; j < NI; ++j) {
+                                R e = ei[j] + Rj[j];
+                                e += ftab[ci * NI + j];
+                                if (m.has_sl[j] && (NZ == 1 || z == NZ - 1)) {
+                                    const R cc = vC[j][z];
+                                    const R s1 = K.K1[j] + cc;
+                                    const R s2 = K.K2[j] + cc;
+                                    e *= (R)1 / ((R)1 + K.A1[j] / (s1 * s1) + K.A2[j] / (s2 * s2));
+                                }
+                                fb[j * cap + n] = vC[j][z] + e * K.dt;
+                            }
+#pragma unroll
+                            for (int p = 0; p < NPM; ++p)
+                                if (p < NP) fb[(NI + p) * cap + n] = vC[NI + p][z] + ep[p] * K.dt;
+                        }
+#pragma unroll
+                        for (int f = 0; f < CSM; ++f)
+#pragma unroll
+                            for (int z = 0; z < NZ; ++z) {
+                                vP[f][z] = vC[f][z];
+                                vC[f][z] = vN[f][z];
+                            }
+                    }
+                }
+                if (rd3d) {
+                    // RD3D cytosol of this rank: a thread per (i, j) column marching along z
+                    // (no reference analog; see the oracle)
+                    const int* ptr = a.dep_ptr + (size_t)s * (mc2 + 1);
+                    const int wt = tid - 64, NWT = blockDim.x - 64;
+                    const int ni = mc - 2;
+                    // tasks: columns x chunks of PL planes, PC chosen to balance the threads
+                    const int ncol = ni * ni, npr = phi - plo;
+                    int PC = 1;
+                    long long best = 1LL << 62;
+                    for (int pc = 1; pc <= npr; ++pc) {
+                        const long long cost = (long long)((ncol * pc + NWT - 1) / NWT) * ((npr + pc - 1) / pc + 1);
+                        if (cost < best) {
+                            best = cost;
+                            PC = pc;
+                        }
+                    }
+                    const int PL = npr > 0 ? (npr + PC - 1) / PC : 1;
+                    for (int t = wt; t < ncol * PC; t += NWT) {
+                        const int pc = t / ncol, col = t - pc * ncol;
+                        const int k0 = plo + pc * PL, k1 = min(k0 + PL, phi);
+                        if (k0 >= k1) continue;
+                        const int jj = 1 + col / ni, ii = 1 + (col - (col / ni) * ni);
+                        const int cn = ii + mc * jj;
+                        R uP[CSM], uC[CSM], uN[CSM];
+#pragma unroll
+                        for (int c = 0; c < CSM; ++c) {
+                            uP[c] = uC[c] = uN[c] = (R)0;
+                            if (c < CS) {
+                                uC[c] = ca[c * ccap + cn + mc2 * (k0 - splo)];
+                                if (k0 > 0) uP[c] = ca[c * ccap + cn + mc2 * (k0 - 1 - splo)];
+                            }
+                        }
+                        for (int k = k0; k < k1; ++k) {
+                            const int ln = cn + mc2 * (k - splo);
+#pragma unroll
+                            for (int c = 0; c < CSM; ++c)
+                                if (c < CS) {
+                                    uN[c] = ca[c * ccap + ln + mc2];
+                                    if (k == 0) uP[c] = uN[c];  // no-flux face: mirror
+                                }
+                            R evo[CSM];
+#pragma unroll
+                            for (int c = 0; c < CSM; ++c) {
+                                evo[c] = 0;
+                                if (c < CS) {
+                                    const R* v = ca + c * ccap;
+                                    const R cc = uC[c];
+                                    evo[c] = K.cD[c] * ((v[ln + 1] - 2 * cc + v[ln - 1]) * K.ih2 + (v[ln + mc] - 2 * cc + v[ln - mc]) * K.ih2 +
+                                                        (uN[c] - 2 * cc + uP[c]) * K.ih2);
+                                }
+                            }
+                            int is = 0;
+#pragma unroll
+                            for (int j2 = 0; j2 < NI; ++j2) {
+                                const R ion = uC[j2];
+                                R react = 0;
+#pragma unroll
+                                for (int c = NI; c < CSM; ++c)
+                                    if (c < CS && m.c_pair_ion[c - NI] == j2) {
+                                        R fr = K.cctp[c];
+#pragma unroll
+                                        for (int c2 = NI; c2 < CSM; ++c2)
+                                            if ((K.csame[c] >> c2) & 1) fr -= uC[c2];
+                                        const R R1 = K.ckoff[c] * uC[c] - K.ckon[c] * ion * fr;
+                                        evo[c] += -R1;
+                                        react += R1;
+                                    }
+                                evo[j2] += react;
+                                if (m.c_serca[j2]) {
+                                    const R i2 = ion * ion;
+                                    const R K2 = K.Kup2[is];
+                                    const R b2 = K.bg2[is];
+                                    evo[j2] -= K.Jmax[is] * (i2 / (i2 + K2) - b2 / (b2 + K2));
+                                    ++is;
+                                }
+                            }
+#pragma unroll
+                            for (int c = 0; c < CSM; ++c)
+                                if (c < CS) {
+                                    R e = evo[c];
+                                    if (k == 0) {
+                                        // deposit of the previous Update, in the oracle's term order
+                                        double dep = 0;
+                                        if (it == 0) {
+                                            dep = a.cin[((size_t)s * CS + c) * mc2 + cn];
+                                        } else if (K.cdep[c] >= 0) {
+                                            for (int q2 = ptr[cn]; q2 < ptr[cn + 1]; ++q2)
+                                                dep += (double)terms[((size_t)prv * a.max_terms + a.dep_term[st.term_off + q2]) * FD + K.cdep[c]];
+                                        }
+                                        e += (R)dep;
+                                    }
+                                    cb[c * ccap + ln] = uC[c] + e * K.dt;
+                                }
+#pragma unroll
+                            for (int c = 0; c < CSM; ++c) {
+                                uP[c] = uC[c];
+                                uC[c] = uN[c];
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+
+            // ---------------------------------------------------- phase B: Update
+            const R* lprev = lay0 + prv * CS * mc2;  // cytosol layer 0 at the start of this step
+            auto rim_value = [&](int f, int x, int y) -> R {
+                if (!rd3d) return f < NI ? (R)q.c_ions[f] : (R)q.c_bnd[f - NI];
+                const int cn = a.rim_cnode[st.rim_off + cb_rim_index(x, y, nx, ny)];
+                if (f < NI) return lprev[f * mc2 + cn];
+                const int cq = m.dyad_c_pair[f - NI];
+                return cq >= 0 ? lprev[(NI + cq) * mc2 + cn] : (R)m.pair_init[f - NI];
+            };
+            // Dirichlet rim of this rank's rows (CaSim/DyadRD2DCPU.cpp:274-303)
+            {
+                const int nxe = 2 * (hi - lo);                                     // x = 0 / nx-1 columns
+                const int nye = (lo == 0 ? nx - 2 : 0) + (hi == ny ? nx - 2 : 0);  // inner nodes of rows 0 / ny-1
+                const int per_z = nxe + nye;
+                for (int t = tid; t < per_z * nz; t += blockDim.x) {
+                    const int z = t / per_z, k = t - z * per_z;
+                    int x, y;
+                    if (k < nxe) {
+                        y = lo + (k >> 1);
+                        x = (k & 1) ? nx - 1 : 0;
+                    } else {
+                        int kk = k - nxe;
+                        if (lo == 0 && kk < nx - 2) {
+                            y = 0;
+                        } else {
+                            if (lo == 0) kk -= nx - 2;
+                            y = ny - 1;
+                        }
+                        x = 1 + kk;
+                    }
+                    const int n = x + nx * ((y - slo) + nr * z);
+                    for (int f = 0; f < F; ++f) fb[f * cap + n] = rim_value(f, x, y);
+                }
+            }
+            // mouth gather and RyR currents of own channels (CaSim/DyadRD2DCPU.cpp:243-264, 361-380)
+            double tpart[NI];
+#pragma unroll
+            for (int j = 0; j < NI; ++j) tpart[j] = 0;
+            double* mcur = mi + par * a.max_ch * NI;
+            for (int c = tid; c < nch; c += blockDim.x) {
+                const int n = chn[c];
+                if (n < 0) continue;
+                const int gnode = cho[c] & ((1 << 30) - 1);
+                const int x = gnode % nx, y = (gnode / nx) % ny;
+                const bool rim = x == 0 || y == 0 || x == nx - 1 || y == ny - 1;
+                const R* src = rim ? fa : fb;  // the mouth is gathered before the rim is reset
+                const int stc = chs[c];
+#pragma unroll
+                for (int j = 0; j < NI; ++j) {
+                    const double mv = (double)src[j * cap + n];
+                    #pragma unroll 1
+                    for (int r = 0; r < C; ++r) peer<C>(mcur, r)[c * NI + j] = mv;
+                    const double cv = rim ? (double)rim_value(j, x, y) : mv;
+                    const double fl = stc * (m.g[j] * (q.jsr_new[j] - cv));
+                    ftab[(1 + c) * NI + j] = (R)fl;
+                    fluxd[c * NI + j] = fl;
+                    tpart[j] += fl;
+                }
+                if (last) {
+                    double* mo = a.mouth + (size_t)(st.ch_off + c) * a.NS;
+                    double fr[CB_MAX_BUF];
+                    for (int b = 0; b < m.n_buf; ++b) fr[b] = m.Ctot[b];
+                    for (int f = 0; f < F; ++f) {
+                        const double v = (double)src[f * cap + n];
+                        mo[f] = v;
+                        if (f >= NI) fr[m.pair_buf[f - NI]] -= v;
+                    }
+                    for (int b = 0; b < m.n_buf; ++b) mo[F + b] = fr[b];
+                }
+            }
+            // efflux of this rank's rim terms (CaSim/DyadRD2DCPU.cpp:305-350); u0 is the rim value
+            double epart[CSM];
+#pragma unroll
+            for (int f = 0; f < CSM; ++f) epart[f] = 0;
+            {
+                const int ylo = max(lo, 1), yhi = min(hi, ny - 1);
+                const int nxr = max(yhi - ylo, 0);
+                const int nxt = 2 * nxr;                                   // x-edge terms per z
+                const int nyt = (lo == 0 ? nx : 0) + (hi == ny ? nx : 0);  // y-edge terms per z
+                const int per_z = nxt + nyt;
+                R* t0 = peer<C>(terms + (size_t)par * a.max_terms * FD, 0);
+                for (int t = tid; t < per_z * zmax; t += blockDim.x) {
+                    const int z = t / per_z, k = t - z * per_z;
+                    int x0, y0, dxs, dys, gterm;
+                    double sf;
+                    if (k < nxt) {
+                        const int e = k / nxr, y = ylo + (k - e * nxr);
+                        x0 = e ? nx - 1 : 0;
+                        y0 = y;
+                        dxs = e ? -1 : 1;
+                        dys = 0;
+                        sf = m.sx;
+                        gterm = (e * (ny - 2) + (y - 1)) * zmax + z;
+                    } else {
+                        int kk = k - nxt;
+                        int e;
+                        if (lo == 0 && kk < nx) {
+                            e = 0;
+                        } else {
+                            if (lo == 0) kk -= nx;
+                            e = 1;
+                        }
+                        x0 = kk;
+                        y0 = e ? ny - 1 : 0;
+                        dxs = 0;
+                        dys = e ? -1 : 1;
+                        sf = m.sy;
+                        gterm = (2 * (ny - 2) + e * nx + kk) * zmax + z;
+                    }
+                    const int n1 = (x0 + dxs) + nx * ((y0 + dys - slo) + nr * z);
+                    const int n2 = (x0 + 2 * dxs) + nx * ((y0 + 2 * dys - slo) + nr * z);
+#pragma unroll
+                    for (int f = 0; f < CSM; ++f) {
+                        if (f < F) {
+                            const double u0 = (double)rim_value(f, x0, y0);
+                            const double D = f < NI ? m.D_ion[f] : m.D_pair[f - NI];
+                            const double gr = 2 * (double)fb[f * cap + n1] - 1.5 * u0 - 0.5 * (double)fb[f * cap + n2];
+                            if (!rd3d) {
+                                epart[f] += D * m.grad_mult * sf * gr;
+                            } else {
+                                const double v = D * sf * gr * m.inv_hc3;
+                                epart[f] += v;
+                                const int sl = dslot(m, NI, f);
+                                if (sl >= 0) t0[(size_t)gterm * FD + sl] = (R)v;
+                            }
+                        }
+                    }
+                }
+            }
+            if constexpr (C > 1) {
+                // halo rows into the neighbours' write buffers; rim columns carry the
+                // rim value because the rim stores above may not be visible yet
+                for (int side = 0; side < 2; ++side) {
+                    const int nb = side == 0 ? rank - 1 : rank + 1;
+                    if (nb < 0 || nb >= C) continue;
+                    const int y = side == 0 ? lo : hi - 1;
+                    const int nlo = row_lo(nb, ny, C), nhi = row_lo(nb + 1, ny, C);
+                    const int nslo = nlo > 0 ? nlo - 1 : 0;
+                    const int nnr = (nhi < ny ? nhi + 1 : ny) - nslo;
+                    R* dst = peer<C>(fb, nb);
+                    for (int k = tid; k < F * nx * nz; k += blockDim.x) {
+                        const int f = k / (nx * nz), rem = k - f * nx * nz;
+                        const int z = rem / nx, x = rem - z * nx;
+                        const R v = (x == 0 || x == nx - 1 || y == 0 || y == ny - 1) ? rim_value(f, x, y)
+                                                                                    : fb[f * cap + x + nx * ((y - slo) + nr * z)];
+                        dst[f * cap + x + nx * ((y - nslo) + nnr * z)] = v;
+                    }
+                }
+                if (rd3d && phi > plo) {
+                    // cytosol halo planes
+                    for (int side = 0; side < 2; ++side) {
+                        const int nb = side == 0 ? rank - 1 : rank + 1;
+                        if (nb < 0 || nb >= C) continue;
+                        const int k = side == 0 ? plo : phi - 1;
+                        const int nplo = (int)(((long long)nb * nplanes) / C);
+                        const int nsplo = nplo > 0 ? nplo - 1 : 0;
+                        R* dst = peer<C>(cb, nb);
+                        for (int t = tid; t < CS * mc2; t += blockDim.x) {
+                            const int c = t / mc2, e = t - c * mc2;
+                            dst[c * ccap + (k - nsplo) * mc2 + e] = cb[c * ccap + (k - splo) * mc2 + e];
+                        }
+                    }
+                }
+            }
+            if (rd3d && rank == 0) {
+                // cytosol layer 0 after this step: the rim values of the next step
+                R* lc = lay0 + par * CS * mc2;
+                for (int t = tid; t < CS * mc2; t += blockDim.x) {
+                    const int c = t / mc2, e = t - c * mc2;
+                    const R v = cb[c * ccap + e];  // plane 0 is local plane 0 on rank 0
+                    #pragma unroll 1
+                    for (int r = 0; r < C; ++r) peer<C>(lc, r)[t] = v;
+                }
+            }
+            // warp partials -> rank partials (fixed order) -> every rank's slot
+#pragma unroll
+            for (int f = 0; f < CSM; ++f) {
+                if (f < F) {
+                    const double v = warp_sum(epart[f]);
+                    if (lane == 0) redw[warp * FDn + f] = v;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NI; ++j) {
+                const double v = warp_sum(tpart[j]);
+                if (lane == 0) redw[warp * FDn + F + j] = v;
+            }
+            __syncthreads();
+            if (warp == 0) {
+                for (int k = lane; k < FDn; k += 32) {
+                    double v = 0;
+                    for (int w = 0; w < W; ++w) v += redw[w * FDn + k];
+                    #pragma unroll 1
+                    for (int r = 0; r < C; ++r) {
+                        if (k < F) peer<C>(rede, r)[(par * C + rank) * F + k] = v;
+                        else peer<C>(redt, r)[(par * C + rank) * NI + (k - F)] = v;
+                    }
+                }
+            }
+            cluster_barrier<C>();
+            {
+                R* t = fa;
+                fa = fb;
+                fb = t;
+            }
+            {
+                R* t = ca;
+                ca = cb;
+                cb = t;
+            }
+        }
+
+        // ---------------------------------------------------------- store
+        if (warp == 0 && a.nsteps > 0) {
+            const int pl = (int)((a.nsteps - 1) & 1);
+            for (int f = lane; f < F; f += 32) {
+                double e = 0;
+                for (int r = 0; r < C; ++r) e += rede[(pl * C + r) * F + f];
+                q.efflux[f] = e;
+            }
+            for (int j = lane; j < NI; j += 32) {
+                double t = 0;
+                for (int r = 0; r < C; ++r) t += redt[(pl * C + r) * NI + j];
+                q.total[j] = t;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                if (!m.jsr_const)
+                    for (int i = 0; i < NI; ++i) {
+                        q.IjSR[i] = q.total[i] * m.V_elem;
+                        q.nsr[i] = m.nsr[i];
+                        q.jsr[i] = q.jsr_new[i];
+                    }
+                cbrng::State gd;  // stream state at the next unconsumed draw
+                for (int i = 0; i < 6; ++i) gd.s[i] = q.rng[i];
+                const long long D = s_D;
+                rng_jump(a.pow2, gd, 2ULL * (unsigned long long)D);
+                for (int i = 0; i < 6; ++i) q.rng[i] = gd.s[i];
+                q.draws += (unsigned long long)D;
+            }
+        }
+        __syncthreads();
+        {
+            R* g = (R*)a.fields + st.node_base * F;
+            for (int f = 0; f < F; ++f)
+                for (int z = 0; z < nz; ++z) {
+                    R* dst = g + (long long)f * np + (long long)nx * (lo + (long long)ny * z);
+                    const R* src = fa + f * cap + lstride * z + nx * (lo - slo);
+                    for (int k = tid; k < nx * (hi - lo); k += blockDim.x) dst[k] = src[k];
+                }
+            if (rank == 0) {
+                const unsigned int* qs = (const unsigned int*)&q;
+                unsigned int* qd = (unsigned int*)(a.sc + s);
+                for (int k = tid; k < (int)(sizeof(cb_site_scalars) / 4); k += blockDim.x) qd[k] = qs[k];
+                for (int c = tid; c < nch; c += blockDim.x) a.ch_state[st.ch_off + c] = chs[c];
+            }
+            R* cg_ = (R*)a.curgrid + st.node_base * NI;
+            for (int c = tid; c < nch; c += blockDim.x)
+                if (chn[c] >= 0 && ((cho[c] >> 30) & 1))
+                    for (int j = 0; j < NI; ++j) cg_[(size_t)j * np + (cho[c] & ((1 << 30) - 1))] = ftab[(1 + c) * NI + j];
+            if (rd3d) {
+                R* cd = (R*)a.cyto + (size_t)s * CS * nc;
+                for (int c = 0; c < CS; ++c)
+                    for (int k = tid; k < (phi - plo) * mc2; k += blockDim.x)
+                        cd[(size_t)c * nc + (size_t)plo * mc2 + k] = ca[c * ccap + (plo - splo) * mc2 + k];
+                if (rank == 0 && a.nsteps > 0) {
+                    // deposit of the final Update, for the next launch
+                    const int pl = (int)((a.nsteps - 1) & 1);
+                    const int* ptr = a.dep_ptr + (size_t)s * (mc2 + 1);
+                    for (int cn = tid; cn < mc2; cn += blockDim.x)
+                        for (int c = 0; c < CS; ++c) {
+                            const int f = c < NI ? c : (m.c_dyad_pair[c - NI] >= 0 ? NI + m.c_dyad_pair[c - NI] : -1);
+                            const int sl = f >= 0 ? dslot(m, NI, f) : -1;
+                            double dep = 0;
+                            if (sl >= 0)
+                                for (int q2 = ptr[cn]; q2 < ptr[cn + 1]; ++q2)
+                                    dep += (double)terms[((size_t)pl * a.max_terms + a.dep_term[st.term_off + q2]) * FD + sl];
+                            a.cin[((size_t)s * CS + c) * mc2 + cn] = dep;
+                        }
+                }
+            }
+        }
+        cluster_barrier<C>();
+    }
+}
+
+// dry: only report how many clusters of this shape can be resident
+template <typename R, int NI, int NPM, int NZ, int C>
+cudaError_t launch_one(const rs_args& a, int threads, cudaStream_t st, int n_sites, int* dry) {
+    auto kern = k_resident<R, NI, NPM, NZ, C>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, a.smem_bytes);
+    if (e != cudaSuccess) return e;
+    if (C > 8) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = a.smem_bytes;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(C);
+    int clusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg);
+    if (e != cudaSuccess) return e;
+    if (dry) {
+        *dry = clusters;
+        return cudaSuccess;
+    }
+    if (clusters < 1) return cudaErrorInvalidConfiguration;
+    clusters = clusters < n_sites ? clusters : n_sites;
+    cfg.gridDim = dim3(clusters * C);
+    return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+template <typename R, int NI, int NPM, int NZ>
+cudaError_t launch_c(const rs_args& a, int C, int threads, cudaStream_t st, int n, int* dry) {
+    switch (C) {
+    case 1: return launch_one<R, NI, NPM, NZ, 1>(a, threads, st, n, dry);
+    case 2: return launch_one<R, NI, NPM, NZ, 2>(a, threads, st, n, dry);
+    case 4: return launch_one<R, NI, NPM, NZ, 4>(a, threads, st, n, dry);
+    case 8: return launch_one<R, NI, NPM, NZ, 8>(a, threads, st, n, dry);
+    case 16: return launch_one<R, NI, NPM, NZ, 16>(a, threads, st, n, dry);
+    default: return cudaErrorInvalidConfiguration;
+    }
+}
+
+// NP: the larger of the cleft's ion-buffer pairs and (RD3D) the cytosol's
+template <typename R, int NZ>
+cudaError_t dispatch(const rs_args& a, int NI, int NP, int C, int threads, cudaStream_t st, int n, int* dry) {
+    if (threads > max_threads(sizeof(R), NI + npm_of(NI, NP), NZ)) return cudaErrorInvalidConfiguration;
+    if (NI == 1 && NP <= 2) return launch_c<R, 1, 2, NZ>(a, C, threads, st, n, dry);
+    if (NI == 1 && NP <= 4) return launch_c<R, 1, 4, NZ>(a, C, threads, st, n, dry);
+    if (NI == 2 && NP <= 4) return launch_c<R, 2, 4, NZ>(a, C, threads, st, n, dry);
+    return cudaErrorInvalidConfiguration;
+}
+
+}  // namespace cbres
+
+// per (precision, layers) launchers, each compiled in its own translation unit
+cudaError_t cb_res_f32_z1(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*);
+cudaError_t cb_res_f32_z3(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*);
+cudaError_t cb_res_f64_z1(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*);
+cudaError_t cb_res_f64_z3(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*);
