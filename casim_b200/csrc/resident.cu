@@ -74,8 +74,9 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
     const bool rd3d = m.cyto_type == CB_CYTO_RD3D;
     // channel and efflux-term capacities are the batch maxima, so the plan of a
     // class fits whenever the plan of its largest site does
-    int cap = 0, ccap = 0;
+    int cap = 0, ccap = 0, maxrim = 1;
     const int maxch = std::max(d.max_ch, 1), maxt = std::max(d.max_terms, 1);
+    for (const cb_site& st : sites) maxrim = std::max(maxrim, cb_rim_count(st.nx, st.ny));
     for (int s : idx) {
         const cb_site& st = sites[s];
         if (st.ny < 3 * C) return false;  // every rank needs three rows (y-edge efflux)
@@ -116,10 +117,10 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
     off = align16(off + (size_t)maxch * 4);
     a.off_cho = (int)off;
     off = align16(off + (size_t)maxch * 4);
+    a.off_chr = (int)off;
+    off = align16(off + (size_t)maxch * 4);
     a.off_ftab = (int)off;
     off = align16(off + (size_t)(maxch + 1) * NI * rs);
-    a.off_fluxd = (int)off;
-    off = align16(off + (size_t)maxch * NI * 8);
     a.off_mi = (int)off;
     off = align16(off + (size_t)2 * maxch * NI * 8);
     a.off_ring = (int)off;
@@ -130,10 +131,14 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
     off = align16(off + (size_t)2 * C * F * 8);
     a.off_redt = (int)off;
     off = align16(off + (size_t)2 * C * NI * 8);
-    a.off_lay0 = (int)off;
-    if (rd3d) off = align16(off + (size_t)2 * CS * mc2 * rs);
     a.off_terms = (int)off;
     if (rd3d) off = align16(off + (size_t)2 * maxt * FD * rs);
+    a.off_crim = (int)off;
+    if (rd3d) off = align16(off + (size_t)maxrim * 2);
+    a.off_dptr = (int)off;
+    if (rd3d) off = align16(off + (size_t)(mc2 + 1) * 2);
+    a.off_dterm = (int)off;
+    if (rd3d) off = align16(off + (size_t)maxt * 2);
     a.off_sc = (int)off;
     off = align16(off + sizeof(cb_site_scalars));
     a.smem_bytes = (int)off;
@@ -141,7 +146,9 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
     a.cap_cyto = ccap;
     a.max_ch = maxch;
     a.max_terms = maxt;
+    a.max_rim = maxrim;
     a.FD = FD;
+    if (rd3d && (maxt > 65535 || mc2 + 1 > 65535)) return false;  // u16 deposit tables
     return off <= (size_t)(227 * 1024 - 1024);
 }
 

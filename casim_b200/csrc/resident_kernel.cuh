@@ -103,9 +103,9 @@ struct rs_args {
     // shared-memory carve (bytes, identical for every block of the launch)
     int cap_cleft;  // stored cleft nodes per species per rank
     int cap_cyto;   // stored cytosol nodes per species per rank
-    int max_ch, max_terms, FD;
-    int off_fb, off_ca, off_cb, off_chidx, off_chn, off_chs, off_cho, off_ftab, off_fluxd, off_mi, off_ring,
-        off_redw, off_rede, off_redt, off_lay0, off_terms, off_sc, smem_bytes;
+    int max_ch, max_terms, max_rim, FD;
+    int off_fb, off_ca, off_cb, off_chidx, off_chn, off_chs, off_cho, off_chr, off_ftab, off_mi, off_ring, off_redw,
+        off_rede, off_redt, off_terms, off_crim, off_dptr, off_dterm, off_sc, smem_bytes;
 };
 
 // ---- MRG32k3a arithmetic by folding: m1 = 2^32 - 209, m2 = 2^32 - 22853 ----
@@ -226,15 +226,17 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     int* chn = (int*)(smem + a.off_chn);   // local node of own RyRs, -1 otherwise
     int* chs = (int*)(smem + a.off_chs);   // state of every RyR of the site
     int* cho = (int*)(smem + a.off_cho);   // site node (x + nx*(y + ny*z)) | owner flag in bit 30
+    int* chr = (int*)(smem + a.off_chr);   // rim index of own RyRs on the rim, -1 otherwise
     R* ftab = (R*)(smem + a.off_ftab);     // [(1 + max_ch)][NI]: RyR currents, slot 0 is zero
-    double* fluxd = (double*)(smem + a.off_fluxd);
     double* mi = (double*)(smem + a.off_mi);      // [2][max_ch][NI]
     double* ring = (double*)(smem + a.off_ring);
     double* redw = (double*)(smem + a.off_redw);  // [MAX_WARPS][F + NI]
     double* rede = (double*)(smem + a.off_rede);  // [2][C][F]
     double* redt = (double*)(smem + a.off_redt);  // [2][C][NI]
-    R* lay0 = (R*)(smem + a.off_lay0);            // [2][CS][mc2]
-    R* terms = (R*)(smem + a.off_terms);          // [2][max_terms][FD]
+    R* terms = (R*)(smem + a.off_terms);          // [2][max_terms][FD] RD3D efflux terms (rank 0)
+    unsigned short* crim = (unsigned short*)(smem + a.off_crim);    // RD3D: rim index -> layer-0 cytosol node
+    unsigned short* dptr = (unsigned short*)(smem + a.off_dptr);    // RD3D: deposit list offsets per layer-0 node
+    unsigned short* dterm = (unsigned short*)(smem + a.off_dterm);  // RD3D: efflux terms, oracle order
     cb_site_scalars& q = *(cb_site_scalars*)(smem + a.off_sc);
 
     const rs_const<R>& K = *[&]() {
@@ -294,9 +296,11 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                         ca[c * ccap + k] = v;
                         cb[c * ccap + k] = v;
                     }
-                // cytosol layer 0 at entry: the rim values of the first step (parity-1 slot)
-                for (int c = 0; c < CS; ++c)
-                    for (int k = tid; k < mc2; k += blockDim.x) lay0[(CS + c) * mc2 + k] = cs[(size_t)c * nc + k];
+                const int nrim = cb_rim_count(nx, ny);
+                for (int k = tid; k < nrim; k += blockDim.x) crim[k] = (unsigned short)a.rim_cnode[st.rim_off + k];
+                const int* gp = a.dep_ptr + (size_t)s * (mc2 + 1);
+                for (int k = tid; k <= mc2; k += blockDim.x) dptr[k] = (unsigned short)gp[k];
+                for (int k = tid; k < gp[mc2]; k += blockDim.x) dterm[k] = (unsigned short)a.dep_term[st.term_off + k];
             }
         }
         __syncthreads();
@@ -309,6 +313,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             const bool own = y >= lo && y < hi;
             const int ln = own ? x + nx * ((y - slo) + nr * z) : -1;
             chn[c] = ln;
+            chr[c] = (x == 0 || y == 0 || x == nx - 1 || y == ny - 1) ? cb_rim_index(x, y, nx, ny) : -1;
             const double* mo = a.mouth + (size_t)(st.ch_off + c) * a.NS;
             for (int j = 0; j < NI; ++j) mi[(a.max_ch + c) * NI + j] = mo[j];  // parity-1 slot
             if (own) {
@@ -317,7 +322,6 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     // current of the last Update: state * g * (jSR - Ca at the node)
                     const double fl = chs[c] * (m.g[j] * (q.jsr_new[j] - (double)fa[j * cap + ln]));
                     ftab[(1 + c) * NI + j] = (R)fl;
-                    fluxd[c * NI + j] = fl;
                 }
             }
         }
@@ -329,6 +333,39 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             for (int i = 0; i < 6; ++i) s_rng[lane * 6 + i] = gl.s[i];
             if (lane == 0) s_D = s_we = 0;
         }
+        // stencil partition of this rank: strips of RS rows x 32 columns over the
+        // worker warps, RS minimising the rounds x (rows per strip + 1 row of setup)
+        const int ylo = max(lo, 1), yhi = min(hi, ny - 1);
+        const int nrows = max(yhi - ylo, 0);
+        const int XB = (nx - 2 + 31) >> 5;
+        const int NW = W - 2;
+        int RS = max(nrows, 1);
+        {
+            long long best = 1LL << 62;
+            for (int rs = 1; rs <= nrows; ++rs) {
+                const int strips = XB * ((nrows + rs - 1) / rs);
+                const long long cost = (long long)((strips + NW - 1) / NW) * (rs + 1);
+                if (cost < best) {
+                    best = cost;
+                    RS = rs;
+                }
+            }
+        }
+        const int nchunk = (nrows + RS - 1) / RS;
+        // RD3D partition: (i, j) columns x chunks of PL planes over the worker threads
+        const int ni = mc - 2, ncol = ni * ni, npr = phi - plo, NWT = blockDim.x - 64;
+        int PC = 1;
+        if (rd3d) {
+            long long best = 1LL << 62;
+            for (int pc = 1; pc <= npr; ++pc) {
+                const long long cost = (long long)((ncol * pc + NWT - 1) / NWT) * ((npr + pc - 1) / pc + 1);
+                if (cost < best) {
+                    best = cost;
+                    PC = pc;
+                }
+            }
+        }
+        const int PL = npr > 0 ? (npr + PC - 1) / PC : 1;
         cluster_barrier<C>();
 
         // ---------------------------------------------------------- steps
@@ -454,12 +491,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             } else {
                 // ---- worker warps: cleft stencil, strips of rows with a lane per x;
                 // constants are kernel-parameter operands (K), not registers
-                const int wk = warp - 2, NW = W - 2;
-                const int ylo = max(lo, 1), yhi = min(hi, ny - 1);
-                const int nrows = yhi - ylo;
-                const int XB = (nx - 2 + 31) >> 5;
-                const int RS = max(2, (nrows * XB + NW - 1) / NW);
-                const int nchunk = (nrows + RS - 1) / RS;
+                const int wk = warp - 2;
                 for (int sI = wk; sI < XB * nchunk; sI += NW) {
                     const int ch = sI / XB;
                     const int x = 1 + ((sI - ch * XB) << 5) + lane;
@@ -565,21 +597,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 if (rd3d) {
                     // RD3D cytosol of this rank: a thread per (i, j) column marching along z
                     // (no reference analog; see the oracle)
-                    const int* ptr = a.dep_ptr + (size_t)s * (mc2 + 1);
-                    const int wt = tid - 64, NWT = blockDim.x - 64;
-                    const int ni = mc - 2;
-                    // tasks: columns x chunks of PL planes, PC chosen to balance the threads
-                    const int ncol = ni * ni, npr = phi - plo;
-                    int PC = 1;
-                    long long best = 1LL << 62;
-                    for (int pc = 1; pc <= npr; ++pc) {
-                        const long long cost = (long long)((ncol * pc + NWT - 1) / NWT) * ((npr + pc - 1) / pc + 1);
-                        if (cost < best) {
-                            best = cost;
-                            PC = pc;
-                        }
-                    }
-                    const int PL = npr > 0 ? (npr + PC - 1) / PC : 1;
+                    const int wt = tid - 64;
                     for (int t = wt; t < ncol * PC; t += NWT) {
                         const int pc = t / ncol, col = t - pc * ncol;
                         const int k0 = plo + pc * PL, k1 = min(k0 + PL, phi);
@@ -649,8 +667,8 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                                         if (it == 0) {
                                             dep = a.cin[((size_t)s * CS + c) * mc2 + cn];
                                         } else if (K.cdep[c] >= 0) {
-                                            for (int q2 = ptr[cn]; q2 < ptr[cn + 1]; ++q2)
-                                                dep += (double)terms[((size_t)prv * a.max_terms + a.dep_term[st.term_off + q2]) * FD + K.cdep[c]];
+                                            for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2)
+                                                dep += (double)terms[(prv * a.max_terms + dterm[q2]) * FD + K.cdep[c]];
                                         }
                                         e += (R)dep;
                                     }
@@ -668,61 +686,126 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             __syncthreads();
 
             // ---------------------------------------------------- phase B: Update
-            const R* lprev = lay0 + prv * CS * mc2;  // cytosol layer 0 at the start of this step
-            auto rim_value = [&](int f, int x, int y) -> R {
+            // rim values: the cytosol at the start of this step (RD3D: layer 0 of
+            // rank 0's current buffer, whose plane 0 is its local plane 0)
+            const R* c0 = peer<C>(ca, 0);
+            auto rim_value = [&](int f, int ri) -> R {
                 if (!rd3d) return f < NI ? (R)q.c_ions[f] : (R)q.c_bnd[f - NI];
-                const int cn = a.rim_cnode[st.rim_off + cb_rim_index(x, y, nx, ny)];
-                if (f < NI) return lprev[f * mc2 + cn];
+                const int cn = crim[ri];
+                if (f < NI) return c0[f * ccap + cn];
                 const int cq = m.dyad_c_pair[f - NI];
-                return cq >= 0 ? lprev[(NI + cq) * mc2 + cn] : (R)m.pair_init[f - NI];
+                return cq >= 0 ? c0[(NI + cq) * ccap + cn] : (R)m.pair_init[f - NI];
             };
-            // Dirichlet rim of this rank's rows (CaSim/DyadRD2DCPU.cpp:274-303)
+            // lines of this rank's rim, a warp per line, lanes along it:
+            //   l < 4*nz         Dirichlet rim (CaSim/DyadRD2DCPU.cpp:274-303), edge e = l & 3, layer l >> 2:
+            //                    e 0/1 columns x = 0 / nx-1 over y in [lo, hi); e 2/3 rows y = 0 / ny-1
+            //                    over x in [1, nx-2] where this rank holds them
+            //   l - 4*nz < 4*zmax  efflux terms (CaSim/DyadRD2DCPU.cpp:305-350) in the same edge order:
+            //                    e 0/1 over y in [ylo, yhi); e 2/3 over x in [0, nx-1]
+            double epart[CSM];
+#pragma unroll
+            for (int f = 0; f < CSM; ++f) epart[f] = 0;
+            bool did_e = false;
             {
-                const int nxe = 2 * (hi - lo);                                     // x = 0 / nx-1 columns
-                const int nye = (lo == 0 ? nx - 2 : 0) + (hi == ny ? nx - 2 : 0);  // inner nodes of rows 0 / ny-1
-                const int per_z = nxe + nye;
-                for (int t = tid; t < per_z * nz; t += blockDim.x) {
-                    const int z = t / per_z, k = t - z * per_z;
-                    int x, y;
-                    if (k < nxe) {
-                        y = lo + (k >> 1);
-                        x = (k & 1) ? nx - 1 : 0;
-                    } else {
-                        int kk = k - nxe;
-                        if (lo == 0 && kk < nx - 2) {
-                            y = 0;
+                R* t0 = peer<C>(terms + (size_t)par * a.max_terms * FD, 0);
+                for (int l = warp; l < 4 * (nz + zmax); l += W) {
+                    const bool eff = l >= 4 * nz;
+                    const int le = eff ? l - 4 * nz : l;
+                    const int z = le >> 2, e = le & 3;
+                    if (!eff) {
+                        int len, x0, y0, dxs, ri0;
+                        if (e < 2) {
+                            len = hi - lo;
+                            x0 = e ? nx - 1 : 0;
+                            y0 = lo;
+                            dxs = 0;
+                            ri0 = (e ? ny : 0) + lo;
                         } else {
-                            if (lo == 0) kk -= nx - 2;
-                            y = ny - 1;
+                            len = (e == 2 ? lo == 0 : hi == ny) ? nx - 2 : 0;
+                            x0 = 1;
+                            y0 = e == 2 ? 0 : ny - 1;
+                            dxs = 1;
+                            ri0 = 2 * ny + (e == 2 ? 0 : nx - 2);
                         }
-                        x = 1 + kk;
+                        for (int i = lane; i < len; i += 32) {
+                            const int x = x0 + dxs * i, y = y0 + (1 - dxs) * i;
+                            const int n = x + nx * ((y - slo) + nr * z);
+#pragma unroll
+                            for (int f = 0; f < CSM; ++f)
+                                if (f < F) fb[f * cap + n] = rim_value(f, ri0 + i);
+                        }
+                    } else {
+                        did_e = true;
+                        int len, x0, y0, dxs, dys, gt0, gts;
+                        double sf;
+                        if (e < 2) {
+                            len = nrows;
+                            x0 = e ? nx - 1 : 0;
+                            y0 = ylo;
+                            dxs = e ? -1 : 1;
+                            dys = 0;
+                            sf = m.sx;
+                            gt0 = (e * (ny - 2) + (ylo - 1)) * zmax + z;
+                        } else {
+                            len = (e == 2 ? lo == 0 : hi == ny) ? nx : 0;
+                            x0 = 0;
+                            y0 = e == 2 ? 0 : ny - 1;
+                            dxs = 0;
+                            dys = e == 2 ? 1 : -1;
+                            sf = m.sy;
+                            gt0 = (2 * (ny - 2) + (e - 2) * nx) * zmax + z;
+                        }
+                        for (int i = lane; i < len; i += 32) {
+                            // the edge node walks along the line: y for x-edges, x for y-edges
+                            const int xe = e < 2 ? x0 : i, ye = e < 2 ? y0 + i : y0;
+                            const int ri = e < 2 ? (e ? ny : 0) + ye
+                                                 : (xe == 0 ? ye == 0 ? 0 : ny - 1
+                                                            : xe == nx - 1 ? ny + ye : 2 * ny + (e == 2 ? 0 : nx - 2) + xe - 1);
+                            const int n1 = (xe + dxs) + nx * ((ye + dys - slo) + nr * z);
+                            const int n2 = (xe + 2 * dxs) + nx * ((ye + 2 * dys - slo) + nr * z);
+                            const int gterm = gt0 + i * zmax;
+#pragma unroll
+                            for (int f = 0; f < CSM; ++f) {
+                                if (f < F) {
+                                    const double u0 = (double)rim_value(f, ri);
+                                    const double D = f < NI ? m.D_ion[f] : m.D_pair[f - NI];
+                                    const double gr = 2 * (double)fb[f * cap + n1] - 1.5 * u0 - 0.5 * (double)fb[f * cap + n2];
+                                    if (!rd3d) {
+                                        epart[f] += D * m.grad_mult * sf * gr;
+                                    } else {
+                                        const double v = D * sf * gr * m.inv_hc3;
+                                        epart[f] += v;
+                                        const int sl = dslot(m, NI, f);
+                                        if (sl >= 0) t0[gterm * FD + sl] = (R)v;
+                                    }
+                                }
+                            }
+                        }
                     }
-                    const int n = x + nx * ((y - slo) + nr * z);
-                    for (int f = 0; f < F; ++f) fb[f * cap + n] = rim_value(f, x, y);
                 }
             }
-            // mouth gather and RyR currents of own channels (CaSim/DyadRD2DCPU.cpp:243-264, 361-380)
+            // mouth gather and RyR currents of own channels (CaSim/DyadRD2DCPU.cpp:243-264, 361-380),
+            // channels from the last thread down so they meet the warps with fewer rim lines
             double tpart[NI];
 #pragma unroll
             for (int j = 0; j < NI; ++j) tpart[j] = 0;
+            const int ct = blockDim.x - 1 - tid;
+            const bool did_t = (W - 1 - warp) * 32 < nch;
             double* mcur = mi + par * a.max_ch * NI;
-            for (int c = tid; c < nch; c += blockDim.x) {
+            for (int c = ct; c < nch; c += blockDim.x) {
                 const int n = chn[c];
                 if (n < 0) continue;
-                const int gnode = cho[c] & ((1 << 30) - 1);
-                const int x = gnode % nx, y = (gnode / nx) % ny;
-                const bool rim = x == 0 || y == 0 || x == nx - 1 || y == ny - 1;
-                const R* src = rim ? fa : fb;  // the mouth is gathered before the rim is reset
+                const int ri = chr[c];
+                const R* src = ri >= 0 ? fa : fb;  // the mouth is gathered before the rim is reset
                 const int stc = chs[c];
 #pragma unroll
                 for (int j = 0; j < NI; ++j) {
                     const double mv = (double)src[j * cap + n];
-                    #pragma unroll 1
+#pragma unroll 1
                     for (int r = 0; r < C; ++r) peer<C>(mcur, r)[c * NI + j] = mv;
-                    const double cv = rim ? (double)rim_value(j, x, y) : mv;
+                    const double cv = ri >= 0 ? (double)rim_value(j, ri) : mv;
                     const double fl = stc * (m.g[j] * (q.jsr_new[j] - cv));
                     ftab[(1 + c) * NI + j] = (R)fl;
-                    fluxd[c * NI + j] = fl;
                     tpart[j] += fl;
                 }
                 if (last) {
@@ -737,68 +820,34 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     for (int b = 0; b < m.n_buf; ++b) mo[F + b] = fr[b];
                 }
             }
-            // efflux of this rank's rim terms (CaSim/DyadRD2DCPU.cpp:305-350); u0 is the rim value
-            double epart[CSM];
+            // warp partials (warps without terms or channels contribute exact zeros)
 #pragma unroll
-            for (int f = 0; f < CSM; ++f) epart[f] = 0;
-            {
-                const int ylo = max(lo, 1), yhi = min(hi, ny - 1);
-                const int nxr = max(yhi - ylo, 0);
-                const int nxt = 2 * nxr;                                   // x-edge terms per z
-                const int nyt = (lo == 0 ? nx : 0) + (hi == ny ? nx : 0);  // y-edge terms per z
-                const int per_z = nxt + nyt;
-                R* t0 = peer<C>(terms + (size_t)par * a.max_terms * FD, 0);
-                for (int t = tid; t < per_z * zmax; t += blockDim.x) {
-                    const int z = t / per_z, k = t - z * per_z;
-                    int x0, y0, dxs, dys, gterm;
-                    double sf;
-                    if (k < nxt) {
-                        const int e = k / nxr, y = ylo + (k - e * nxr);
-                        x0 = e ? nx - 1 : 0;
-                        y0 = y;
-                        dxs = e ? -1 : 1;
-                        dys = 0;
-                        sf = m.sx;
-                        gterm = (e * (ny - 2) + (y - 1)) * zmax + z;
-                    } else {
-                        int kk = k - nxt;
-                        int e;
-                        if (lo == 0 && kk < nx) {
-                            e = 0;
-                        } else {
-                            if (lo == 0) kk -= nx;
-                            e = 1;
-                        }
-                        x0 = kk;
-                        y0 = e ? ny - 1 : 0;
-                        dxs = 0;
-                        dys = e ? -1 : 1;
-                        sf = m.sy;
-                        gterm = (2 * (ny - 2) + e * nx + kk) * zmax + z;
-                    }
-                    const int n1 = (x0 + dxs) + nx * ((y0 + dys - slo) + nr * z);
-                    const int n2 = (x0 + 2 * dxs) + nx * ((y0 + 2 * dys - slo) + nr * z);
+            for (int f = 0; f < CSM; ++f) {
+                if (f < F) {
+                    const double v = did_e ? warp_sum(epart[f]) : 0.0;
+                    if (lane == 0) redw[warp * FDn + f] = v;
+                }
+            }
 #pragma unroll
-                    for (int f = 0; f < CSM; ++f) {
-                        if (f < F) {
-                            const double u0 = (double)rim_value(f, x0, y0);
-                            const double D = f < NI ? m.D_ion[f] : m.D_pair[f - NI];
-                            const double gr = 2 * (double)fb[f * cap + n1] - 1.5 * u0 - 0.5 * (double)fb[f * cap + n2];
-                            if (!rd3d) {
-                                epart[f] += D * m.grad_mult * sf * gr;
-                            } else {
-                                const double v = D * sf * gr * m.inv_hc3;
-                                epart[f] += v;
-                                const int sl = dslot(m, NI, f);
-                                if (sl >= 0) t0[(size_t)gterm * FD + sl] = (R)v;
-                            }
-                        }
+            for (int j = 0; j < NI; ++j) {
+                const double v = did_t ? warp_sum(tpart[j]) : 0.0;
+                if (lane == 0) redw[warp * FDn + F + j] = v;
+            }
+            __syncthreads();
+            // rank partials (fixed warp order) into every rank's slot
+            if (warp == 0) {
+                for (int k = lane; k < FDn; k += 32) {
+                    double v = 0;
+                    for (int w = 0; w < W; ++w) v += redw[w * FDn + k];
+#pragma unroll 1
+                    for (int r = 0; r < C; ++r) {
+                        if (k < F) peer<C>(rede, r)[(par * C + rank) * F + k] = v;
+                        else peer<C>(redt, r)[(par * C + rank) * NI + (k - F)] = v;
                     }
                 }
             }
             if constexpr (C > 1) {
-                // halo rows into the neighbours' write buffers; rim columns carry the
-                // rim value because the rim stores above may not be visible yet
+                // halo rows into the neighbours' write buffers, a warp per (species, layer) row
                 for (int side = 0; side < 2; ++side) {
                     const int nb = side == 0 ? rank - 1 : rank + 1;
                     if (nb < 0 || nb >= C) continue;
@@ -807,12 +856,11 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     const int nslo = nlo > 0 ? nlo - 1 : 0;
                     const int nnr = (nhi < ny ? nhi + 1 : ny) - nslo;
                     R* dst = peer<C>(fb, nb);
-                    for (int k = tid; k < F * nx * nz; k += blockDim.x) {
-                        const int f = k / (nx * nz), rem = k - f * nx * nz;
-                        const int z = rem / nx, x = rem - z * nx;
-                        const R v = (x == 0 || x == nx - 1 || y == 0 || y == ny - 1) ? rim_value(f, x, y)
-                                                                                    : fb[f * cap + x + nx * ((y - slo) + nr * z)];
-                        dst[f * cap + x + nx * ((y - nslo) + nnr * z)] = v;
+                    for (int l = warp; l < F * NZ; l += W) {
+                        const int f = l / NZ, z = l - f * NZ;
+                        const R* src = fb + f * cap + nx * ((y - slo) + nr * z);
+                        R* d = dst + f * cap + nx * ((y - nslo) + nnr * z);
+                        for (int x = lane; x < nx; x += 32) d[x] = src[x];
                     }
                 }
                 if (rd3d && phi > plo) {
@@ -824,45 +872,9 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                         const int nplo = (int)(((long long)nb * nplanes) / C);
                         const int nsplo = nplo > 0 ? nplo - 1 : 0;
                         R* dst = peer<C>(cb, nb);
-                        for (int t = tid; t < CS * mc2; t += blockDim.x) {
-                            const int c = t / mc2, e = t - c * mc2;
-                            dst[c * ccap + (k - nsplo) * mc2 + e] = cb[c * ccap + (k - splo) * mc2 + e];
-                        }
-                    }
-                }
-            }
-            if (rd3d && rank == 0) {
-                // cytosol layer 0 after this step: the rim values of the next step
-                R* lc = lay0 + par * CS * mc2;
-                for (int t = tid; t < CS * mc2; t += blockDim.x) {
-                    const int c = t / mc2, e = t - c * mc2;
-                    const R v = cb[c * ccap + e];  // plane 0 is local plane 0 on rank 0
-                    #pragma unroll 1
-                    for (int r = 0; r < C; ++r) peer<C>(lc, r)[t] = v;
-                }
-            }
-            // warp partials -> rank partials (fixed order) -> every rank's slot
-#pragma unroll
-            for (int f = 0; f < CSM; ++f) {
-                if (f < F) {
-                    const double v = warp_sum(epart[f]);
-                    if (lane == 0) redw[warp * FDn + f] = v;
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < NI; ++j) {
-                const double v = warp_sum(tpart[j]);
-                if (lane == 0) redw[warp * FDn + F + j] = v;
-            }
-            __syncthreads();
-            if (warp == 0) {
-                for (int k = lane; k < FDn; k += 32) {
-                    double v = 0;
-                    for (int w = 0; w < W; ++w) v += redw[w * FDn + k];
-                    #pragma unroll 1
-                    for (int r = 0; r < C; ++r) {
-                        if (k < F) peer<C>(rede, r)[(par * C + rank) * F + k] = v;
-                        else peer<C>(redt, r)[(par * C + rank) * NI + (k - F)] = v;
+                        for (int c = 0; c < CS; ++c)
+                            for (int e = tid; e < mc2; e += blockDim.x)
+                                dst[c * ccap + (k - nsplo) * mc2 + e] = cb[c * ccap + (k - splo) * mc2 + e];
                     }
                 }
             }
@@ -935,15 +947,13 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 if (rank == 0 && a.nsteps > 0) {
                     // deposit of the final Update, for the next launch
                     const int pl = (int)((a.nsteps - 1) & 1);
-                    const int* ptr = a.dep_ptr + (size_t)s * (mc2 + 1);
                     for (int cn = tid; cn < mc2; cn += blockDim.x)
                         for (int c = 0; c < CS; ++c) {
-                            const int f = c < NI ? c : (m.c_dyad_pair[c - NI] >= 0 ? NI + m.c_dyad_pair[c - NI] : -1);
-                            const int sl = f >= 0 ? dslot(m, NI, f) : -1;
+                            const int sl = K.cdep[c];
                             double dep = 0;
                             if (sl >= 0)
-                                for (int q2 = ptr[cn]; q2 < ptr[cn + 1]; ++q2)
-                                    dep += (double)terms[((size_t)pl * a.max_terms + a.dep_term[st.term_off + q2]) * FD + sl];
+                                for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2)
+                                    dep += (double)terms[(pl * a.max_terms + dterm[q2]) * FD + sl];
                             a.cin[((size_t)s * CS + c) * mc2 + cn] = dep;
                         }
                 }
