@@ -26,7 +26,10 @@ void fill_const(const cb_model& m, rs_const<R>& k) {
         k.A1[j] = (R)(m.N1[j] * m.K1[j]);
         k.A2[j] = (R)(m.N2[j] * m.K2[j]);
         k.Kup2[j] = (R)(m.c_Kup[j] * m.c_Kup[j]);
-        k.bg2[j] = (R)(m.c_bg[j] * m.c_bg[j]);
+        {
+            const double b2 = m.c_bg[j] * m.c_bg[j], K2 = m.c_Kup[j] * m.c_Kup[j];
+            k.serca0[j] = (R)(b2 / (b2 + K2));
+        }
         k.Jmax[j] = (R)m.c_Jmax[j];
     }
     for (int p = 0; p < m.n_pairs; ++p) {

@@ -69,8 +69,16 @@ struct rs_const {
     R cD[CB_MAX_CSPECIES], ckon[CB_MAX_CSPECIES], ckoff[CB_MAX_CSPECIES], cctp[CB_MAX_CSPECIES];
     int csame[CB_MAX_CSPECIES];          // bit c2: species c2 is a pair of the same buffer
     int cdep[CB_MAX_CSPECIES];           // deposit slot feeding species c, or -1
-    R Kup2[CB_MAX_IONS], bg2[CB_MAX_IONS], Jmax[CB_MAX_IONS];  // by SERCA index: (R)(Kup^2), (R)(bg^2)
+    R Kup2[CB_MAX_IONS], Jmax[CB_MAX_IONS];  // by SERCA index: (R)(Kup^2)
+    R serca0[CB_MAX_IONS];                   // (R)(bg^2 / (bg^2 + Kup^2)): SERCA uptake at rest
 };
+
+// a field-precision constant of the launch, read straight from the kernel parameter
+#define RSK(x) (sizeof(R) == 4 ? (R)a.kf.x : (R)a.kd.x)
+
+// FP32: a * (1/b) with the approximate reciprocal (2 ulp); FP64: IEEE division
+__device__ __forceinline__ float div_fast(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double div_fast(double a, double b) { return a / b; }
 
 struct rs_args {
     cb_model m;
@@ -239,10 +247,6 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     unsigned short* dterm = (unsigned short*)(smem + a.off_dterm);  // RD3D: efflux terms, oracle order
     cb_site_scalars& q = *(cb_site_scalars*)(smem + a.off_sc);
 
-    const rs_const<R>& K = *[&]() {
-        if constexpr (sizeof(R) == 4) return &a.kf;
-        else return &a.kd;
-    }();
     const double dt = m.dt;
     const int FDn = F + NI;
 
@@ -530,19 +534,19 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
 #pragma unroll
                             for (int j = 0; j < NI; ++j) {
                                 const R cc = vC[j][z];
-                                R lap = (fa[j * cap + n + 1] - 2 * cc + fa[j * cap + n - 1]) * K.idx2 + (vN[j][z] - 2 * cc + vP[j][z]) * K.idy2;
-                                if constexpr (NZ > 1) lap = lap + (vC[j][zr] - 2 * cc + vC[j][zl]) * K.idz2;
-                                ei[j] = K.D_ion[j] * lap;
+                                R lap = (fa[j * cap + n + 1] - 2 * cc + fa[j * cap + n - 1]) * RSK(idx2) + (vN[j][z] - 2 * cc + vP[j][z]) * RSK(idy2);
+                                if constexpr (NZ > 1) lap = lap + (vC[j][zr] - 2 * cc + vC[j][zl]) * RSK(idz2);
+                                ei[j] = RSK(D_ion[j]) * lap;
                             }
 #pragma unroll
                             for (int p = 0; p < NPM; ++p) {
                                 ep[p] = 0;
-                                if (p < NP && K.D_pair[p] != (R)0) {
+                                if (p < NP && RSK(D_pair[p]) != (R)0) {
                                     const R cc = vC[NI + p][z];
                                     const R* v = fa + (NI + p) * cap;
-                                    R lap = (v[n + 1] - 2 * cc + v[n - 1]) * K.idx2 + (vN[NI + p][z] - 2 * cc + vP[NI + p][z]) * K.idy2;
-                                    if constexpr (NZ > 1) lap = lap + (vC[NI + p][zr] - 2 * cc + vC[NI + p][zl]) * K.idz2;
-                                    ep[p] = K.D_pair[p] * lap;
+                                    R lap = (v[n + 1] - 2 * cc + v[n - 1]) * RSK(idx2) + (vN[NI + p][z] - 2 * cc + vP[NI + p][z]) * RSK(idy2);
+                                    if constexpr (NZ > 1) lap = lap + (vC[NI + p][zr] - 2 * cc + vC[NI + p][zl]) * RSK(idz2);
+                                    ep[p] = RSK(D_pair[p]) * lap;
                                 }
                             }
                             // reactions: R1 = koff*B - kon*ion*free, free = total minus the
@@ -553,15 +557,15 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
 #pragma unroll
                             for (int p = 0; p < NPM; ++p) {
                                 if (p < NP) {
-                                    R fr = K.ctp[p];
+                                    R fr = RSK(ctp[p]);
 #pragma unroll
                                     for (int p2 = 0; p2 < NPM; ++p2)
-                                        if ((K.same[p] >> p2) & 1) fr -= vC[NI + p2][z];
+                                        if ((a.kf.same[p] >> p2) & 1) fr -= vC[NI + p2][z];
                                     R ion = vC[0][z];
 #pragma unroll
                                     for (int j = 1; j < NI; ++j)
                                         if (m.pair_ion[p] == j) ion = vC[j][z];
-                                    const R r1 = K.koff[p] * vC[NI + p][z] - K.kon[p] * ion * fr;
+                                    const R r1 = RSK(koff[p]) * vC[NI + p][z] - RSK(kon[p]) * ion * fr;
                                     ep[p] += -r1;
 #pragma unroll
                                     for (int j = 0; j < NI; ++j)
@@ -575,15 +579,15 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                                 e += ftab[ci * NI + j];
                                 if (m.has_sl[j] && (NZ == 1 || z == NZ - 1)) {
                                     const R cc = vC[j][z];
-                                    const R s1 = K.K1[j] + cc;
-                                    const R s2 = K.K2[j] + cc;
-                                    e *= (R)1 / ((R)1 + K.A1[j] / (s1 * s1) + K.A2[j] / (s2 * s2));
+                                    const R s1 = RSK(K1[j]) + cc;
+                                    const R s2 = RSK(K2[j]) + cc;
+                                    e *= div_fast((R)1, (R)1 + div_fast(RSK(A1[j]), s1 * s1) + div_fast(RSK(A2[j]), s2 * s2));
                                 }
-                                fb[j * cap + n] = vC[j][z] + e * K.dt;
+                                fb[j * cap + n] = vC[j][z] + e * RSK(dt);
                             }
 #pragma unroll
                             for (int p = 0; p < NPM; ++p)
-                                if (p < NP) fb[(NI + p) * cap + n] = vC[NI + p][z] + ep[p] * K.dt;
+                                if (p < NP) fb[(NI + p) * cap + n] = vC[NI + p][z] + ep[p] * RSK(dt);
                         }
 #pragma unroll
                         for (int f = 0; f < CSM; ++f)
@@ -628,8 +632,8 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                                 if (c < CS) {
                                     const R* v = ca + c * ccap;
                                     const R cc = uC[c];
-                                    evo[c] = K.cD[c] * ((v[ln + 1] - 2 * cc + v[ln - 1]) * K.ih2 + (v[ln + mc] - 2 * cc + v[ln - mc]) * K.ih2 +
-                                                        (uN[c] - 2 * cc + uP[c]) * K.ih2);
+                                    evo[c] = RSK(cD[c]) * ((v[ln + 1] - 2 * cc + v[ln - 1]) * RSK(ih2) + (v[ln + mc] - 2 * cc + v[ln - mc]) * RSK(ih2) +
+                                                        (uN[c] - 2 * cc + uP[c]) * RSK(ih2));
                                 }
                             }
                             int is = 0;
@@ -640,20 +644,18 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
 #pragma unroll
                                 for (int c = NI; c < CSM; ++c)
                                     if (c < CS && m.c_pair_ion[c - NI] == j2) {
-                                        R fr = K.cctp[c];
+                                        R fr = RSK(cctp[c]);
 #pragma unroll
                                         for (int c2 = NI; c2 < CSM; ++c2)
-                                            if ((K.csame[c] >> c2) & 1) fr -= uC[c2];
-                                        const R R1 = K.ckoff[c] * uC[c] - K.ckon[c] * ion * fr;
+                                            if ((a.kf.csame[c] >> c2) & 1) fr -= uC[c2];
+                                        const R R1 = RSK(ckoff[c]) * uC[c] - RSK(ckon[c]) * ion * fr;
                                         evo[c] += -R1;
                                         react += R1;
                                     }
                                 evo[j2] += react;
                                 if (m.c_serca[j2]) {
                                     const R i2 = ion * ion;
-                                    const R K2 = K.Kup2[is];
-                                    const R b2 = K.bg2[is];
-                                    evo[j2] -= K.Jmax[is] * (i2 / (i2 + K2) - b2 / (b2 + K2));
+                                    evo[j2] -= RSK(Jmax[is]) * (div_fast(i2, i2 + RSK(Kup2[is])) - RSK(serca0[is]));
                                     ++is;
                                 }
                             }
@@ -666,13 +668,13 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                                         double dep = 0;
                                         if (it == 0) {
                                             dep = a.cin[((size_t)s * CS + c) * mc2 + cn];
-                                        } else if (K.cdep[c] >= 0) {
+                                        } else if (a.kf.cdep[c] >= 0) {
                                             for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2)
-                                                dep += (double)terms[(prv * a.max_terms + dterm[q2]) * FD + K.cdep[c]];
+                                                dep += (double)terms[(prv * a.max_terms + dterm[q2]) * FD + a.kf.cdep[c]];
                                         }
                                         e += (R)dep;
                                     }
-                                    cb[c * ccap + ln] = uC[c] + e * K.dt;
+                                    cb[c * ccap + ln] = uC[c] + e * RSK(dt);
                                 }
 #pragma unroll
                             for (int c = 0; c < CSM; ++c) {
@@ -949,7 +951,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     const int pl = (int)((a.nsteps - 1) & 1);
                     for (int cn = tid; cn < mc2; cn += blockDim.x)
                         for (int c = 0; c < CS; ++c) {
-                            const int sl = K.cdep[c];
+                            const int sl = a.kf.cdep[c];
                             double dep = 0;
                             if (sl >= 0)
                                 for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2)
