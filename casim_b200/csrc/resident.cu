@@ -15,6 +15,9 @@ namespace {
 
 size_t align16(size_t v) { return (v + 15) / 16 * 16; }
 
+// pair slots the kernel must hold: the cleft's ion-buffer pairs and (RD3D) the cytosol's
+int pairs_of(const cb_model& m) { return std::max(m.n_pairs, m.cyto_type == CB_CYTO_RD3D ? m.c_n_pairs : 0); }
+
 template <typename R>
 void fill_const(const cb_model& m, rs_const<R>& k) {
     k = rs_const<R>{};
@@ -52,8 +55,8 @@ void fill_const(const cb_model& m, rs_const<R>& k) {
             if (g < NI || m.dyad_c_pair[g - NI] >= 0) ++n;
         return (f < NI || m.dyad_c_pair[f - NI] >= 0) ? n : -1;
     };
+    for (int c = 0; c < CB_MAX_CSPECIES; ++c) k.cdep[c] = -1;
     for (int c = 0; c < NI + m.c_n_pairs && c < CB_MAX_CSPECIES; ++c) {
-        k.cdep[c] = -1;
         if (c < NI) {
             k.cD[c] = (R)m.D_ion[c];
             k.cdep[c] = slot(c);
@@ -105,13 +108,15 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
     for (int f = 0; f < m.F; ++f)
         if (f < m.n_ions || m.dyad_c_pair[f - m.n_ions] >= 0) ++FD;
     const int F = m.F, NI = m.n_ions;
-    size_t off = align16((size_t)F * cap * rs);
+    // species slots of the kernel specialisation (the stencils step all of them)
+    const int FP = NI + npm_of(NI, pairs_of(m)), CSP = rd3d ? FP : 0;
+    size_t off = align16((size_t)FP * cap * rs);
     a.off_fb = (int)off;
-    off = align16(off + (size_t)F * cap * rs);
+    off = align16(off + (size_t)FP * cap * rs);
     a.off_ca = (int)off;
-    off = align16(off + (size_t)CS * ccap * rs);
+    off = align16(off + (size_t)CSP * ccap * rs);
     a.off_cb = (int)off;
-    off = align16(off + (size_t)CS * ccap * rs);
+    off = align16(off + (size_t)CSP * ccap * rs);
     a.off_chidx = (int)off;
     off = align16(off + (size_t)cap * 2);
     a.off_chn = (int)off;
@@ -171,7 +176,6 @@ int layers_of(const cb_model& m, const std::vector<cb_site>& sites) {
     return nz;
 }
 
-int pairs_of(const cb_model& m) { return std::max(m.n_pairs, m.cyto_type == CB_CYTO_RD3D ? m.c_n_pairs : 0); }
 
 int thread_cap(const cb_dev& d, int nz) {
     return max_threads(d.precision == 0 ? 8 : 4, d.m.n_ions + npm_of(d.m.n_ions, pairs_of(d.m)), nz);

@@ -80,6 +80,11 @@ struct rs_const {
 __device__ __forceinline__ float div_fast(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ double div_fast(double a, double b) { return a / b; }
 
+template <bool B>
+struct bconst {
+    static constexpr bool value = B;
+};
+
 struct rs_args {
     cb_model m;
     rs_const<float> kf;
@@ -216,7 +221,8 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     // lane l's stream at draw s_we + l*LANE_DRAWS; s_D draws consumed
     __shared__ unsigned int s_rng[32 * 6];
     __shared__ long long s_D, s_we;
-    constexpr int CSM = NI + NPM;  // cytosol species capacity
+    constexpr int CSM = NI + NPM;  // cytosol species slots
+    constexpr int FP = NI + NPM;   // cleft species slots
     const cb_model& m = a.m;
     const int NP = m.n_pairs, F = NI + NP;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, W = blockDim.x >> 5;
@@ -278,11 +284,11 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
         // ---------------------------------------------------------- load
         {
             const R* g = (const R*)a.fields + st.node_base * F;
-            for (int f = 0; f < F; ++f)
+            for (int f = 0; f < FP; ++f)
                 for (int z = 0; z < nz; ++z) {
                     const R* src = g + (long long)f * np + (long long)nx * (slo + (long long)ny * z);
                     for (int k = tid; k < lstride; k += blockDim.x) {
-                        const R v = src[k];
+                        const R v = f < F ? src[k] : (R)0;  // unused species slots hold zeros
                         fa[f * cap + lstride * z + k] = v;
                         fb[f * cap + lstride * z + k] = v;
                     }
@@ -294,9 +300,9 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             for (int k = tid; k < NI; k += blockDim.x) ftab[k] = (R)0;
             if (rd3d) {
                 const R* cs = (const R*)a.cyto + (size_t)s * CS * nc;
-                for (int c = 0; c < CS; ++c)
+                for (int c = 0; c < CSM; ++c)
                     for (int k = tid; k < cloc; k += blockDim.x) {
-                        const R v = cs[(size_t)c * nc + (size_t)splo * mc2 + k];
+                        const R v = c < CS ? cs[(size_t)c * nc + (size_t)splo * mc2 + k] : (R)0;
                         ca[c * ccap + k] = v;
                         cb[c * ccap + k] = v;
                     }
@@ -493,8 +499,10 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 }
                 __syncwarp();
             } else {
-                // ---- worker warps: cleft stencil, strips of rows with a lane per x;
-                // constants are kernel-parameter operands (K), not registers
+                // ---- worker warps: cleft stencil, strips of rows with a lane per x.
+                // All FP = NI + NPM species slots are stepped (unused slots hold zeros and
+                // have zero coefficients), so the loops carry no species-count tests;
+                // constants are kernel-parameter operands.
                 const int wk = warp - 2;
                 for (int sI = wk; sI < XB * nchunk; sI += NW) {
                     const int ch = sI / XB;
@@ -502,51 +510,36 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     if (x > nx - 2) continue;
                     const int y0 = ylo + ch * RS, y1 = min(y0 + RS, yhi);
                     // previous / current / next row of every species and layer
-                    R vP[CSM][NZ], vC[CSM][NZ], vN[CSM][NZ];
+                    R vP[FP][NZ], vC[FP][NZ], vN[FP][NZ];
+                    int nrow = x + nx * (y0 - slo);
 #pragma unroll
-                    for (int f = 0; f < CSM; ++f)
+                    for (int f = 0; f < FP; ++f)
 #pragma unroll
-                        for (int z = 0; z < NZ; ++z) vP[f][z] = vC[f][z] = vN[f][z] = (R)0;
-                    {
-                        const int n0 = x + nx * (y0 - slo);
+                        for (int z = 0; z < NZ; ++z) {
+                            vP[f][z] = fa[f * cap + nrow - nx + lstride * z];
+                            vC[f][z] = fa[f * cap + nrow + lstride * z];
+                        }
+                    for (int y = y0; y < y1; ++y, nrow += nx) {
 #pragma unroll
-                        for (int f = 0; f < CSM; ++f)
+                        for (int f = 0; f < FP; ++f)
 #pragma unroll
-                            for (int z = 0; z < NZ; ++z)
-                                if (f < F) {
-                                    vP[f][z] = fa[f * cap + n0 - nx + lstride * z];
-                                    vC[f][z] = fa[f * cap + n0 + lstride * z];
-                                }
-                    }
-                    for (int y = y0; y < y1; ++y) {
-                        const int nrow = x + nx * (y - slo);
-#pragma unroll
-                        for (int f = 0; f < CSM; ++f)
-#pragma unroll
-                            for (int z = 0; z < NZ; ++z)
-                                if (f < F) vN[f][z] = fa[f * cap + nrow + nx + lstride * z];
+                            for (int z = 0; z < NZ; ++z) vN[f][z] = fa[f * cap + nrow + nx + lstride * z];
 #pragma unroll
                         for (int z = 0; z < NZ; ++z) {
                             const int n = nrow + lstride * z;
                             const int zl = z == 0 ? (NZ > 1 ? 1 : 0) : z - 1;
                             const int zr = z == NZ - 1 ? (NZ > 1 ? NZ - 2 : 0) : z + 1;
-                            R ei[NI], ep[NPM];
+                            R ev[FP];
 #pragma unroll
-                            for (int j = 0; j < NI; ++j) {
-                                const R cc = vC[j][z];
-                                R lap = (fa[j * cap + n + 1] - 2 * cc + fa[j * cap + n - 1]) * RSK(idx2) + (vN[j][z] - 2 * cc + vP[j][z]) * RSK(idy2);
-                                if constexpr (NZ > 1) lap = lap + (vC[j][zr] - 2 * cc + vC[j][zl]) * RSK(idz2);
-                                ei[j] = RSK(D_ion[j]) * lap;
-                            }
-#pragma unroll
-                            for (int p = 0; p < NPM; ++p) {
-                                ep[p] = 0;
-                                if (p < NP && RSK(D_pair[p]) != (R)0) {
-                                    const R cc = vC[NI + p][z];
-                                    const R* v = fa + (NI + p) * cap;
-                                    R lap = (v[n + 1] - 2 * cc + v[n - 1]) * RSK(idx2) + (vN[NI + p][z] - 2 * cc + vP[NI + p][z]) * RSK(idy2);
-                                    if constexpr (NZ > 1) lap = lap + (vC[NI + p][zr] - 2 * cc + vC[NI + p][zl]) * RSK(idz2);
-                                    ep[p] = RSK(D_pair[p]) * lap;
+                            for (int f = 0; f < FP; ++f) {
+                                ev[f] = 0;
+                                const R D = f < NI ? RSK(D_ion[f]) : RSK(D_pair[f - NI]);
+                                if (f < NI || D != (R)0) {
+                                    const R cc = vC[f][z];
+                                    R lap = (fa[f * cap + n + 1] - 2 * cc + fa[f * cap + n - 1]) * RSK(idx2) +
+                                            (vN[f][z] - 2 * cc + vP[f][z]) * RSK(idy2);
+                                    if constexpr (NZ > 1) lap = lap + (vC[f][zr] - 2 * cc + vC[f][zl]) * RSK(idz2);
+                                    ev[f] = D * lap;
                                 }
                             }
                             // reactions: R1 = koff*B - kon*ion*free, free = total minus the
@@ -556,17 +549,23 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                             for (int j = 0; j < NI; ++j) Rj[j] = 0;
 #pragma unroll
                             for (int p = 0; p < NPM; ++p) {
-                                if (p < NP) {
-                                    R fr = RSK(ctp[p]);
+                                R fr = RSK(ctp[p]);
+                                R ion = vC[0][z];
+                                if constexpr (NI == 1) {
+                                    fr -= vC[1 + p][z];  // one ion: every buffer has one pair
+                                } else {
 #pragma unroll
                                     for (int p2 = 0; p2 < NPM; ++p2)
                                         if ((a.kf.same[p] >> p2) & 1) fr -= vC[NI + p2][z];
-                                    R ion = vC[0][z];
 #pragma unroll
                                     for (int j = 1; j < NI; ++j)
                                         if (m.pair_ion[p] == j) ion = vC[j][z];
-                                    const R r1 = RSK(koff[p]) * vC[NI + p][z] - RSK(kon[p]) * ion * fr;
-                                    ep[p] += -r1;
+                                }
+                                const R r1 = RSK(koff[p]) * vC[NI + p][z] - RSK(kon[p]) * ion * fr;
+                                ev[NI + p] += -r1;
+                                if constexpr (NI == 1) {
+                                    Rj[0] += r1;
+                                } else {
 #pragma unroll
                                     for (int j = 0; j < NI; ++j)
                                         if (m.pair_ion[p] == j) Rj[j] += r1;
@@ -575,9 +574,9 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                             const int ci = chidx[n];
 #pragma unroll
                             for (int j = 0; j < NI; ++j) {
-                                R e = ei[j] + Rj[j];
+                                R e = ev[j] + Rj[j];
                                 e += ftab[ci * NI + j];
-                                if (m.has_sl[j] && (NZ == 1 || z == NZ - 1)) {
+                                if ((NZ == 1 || z == NZ - 1) && m.has_sl[j]) {
                                     const R cc = vC[j][z];
                                     const R s1 = RSK(K1[j]) + cc;
                                     const R s2 = RSK(K2[j]) + cc;
@@ -586,11 +585,10 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                                 fb[j * cap + n] = vC[j][z] + e * RSK(dt);
                             }
 #pragma unroll
-                            for (int p = 0; p < NPM; ++p)
-                                if (p < NP) fb[(NI + p) * cap + n] = vC[NI + p][z] + ep[p] * RSK(dt);
+                            for (int p = 0; p < NPM; ++p) fb[(NI + p) * cap + n] = vC[NI + p][z] + ev[NI + p] * RSK(dt);
                         }
 #pragma unroll
-                        for (int f = 0; f < CSM; ++f)
+                        for (int f = 0; f < FP; ++f)
 #pragma unroll
                             for (int z = 0; z < NZ; ++z) {
                                 vP[f][z] = vC[f][z];
@@ -599,8 +597,9 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     }
                 }
                 if (rd3d) {
-                    // RD3D cytosol of this rank: a thread per (i, j) column marching along z
-                    // (no reference analog; see the oracle)
+                    // RD3D cytosol of this rank (no reference analog; see the oracle):
+                    // a thread per (i, j) column marching along z through a chunk of
+                    // planes; all CSM species slots are stepped (unused slots are zero)
                     const int wt = tid - 64;
                     for (int t = wt; t < ncol * PC; t += NWT) {
                         const int pc = t / ncol, col = t - pc * ncol;
@@ -611,30 +610,26 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                         R uP[CSM], uC[CSM], uN[CSM];
 #pragma unroll
                         for (int c = 0; c < CSM; ++c) {
-                            uP[c] = uC[c] = uN[c] = (R)0;
-                            if (c < CS) {
-                                uC[c] = ca[c * ccap + cn + mc2 * (k0 - splo)];
-                                if (k0 > 0) uP[c] = ca[c * ccap + cn + mc2 * (k0 - 1 - splo)];
-                            }
+                            uC[c] = ca[c * ccap + cn + mc2 * (k0 - splo)];
+                            uP[c] = k0 > 0 ? ca[c * ccap + cn + mc2 * (k0 - 1 - splo)] : (R)0;
                         }
-                        for (int k = k0; k < k1; ++k) {
+                        // one plane; P0: plane 0, whose lower face mirrors and which
+                        // receives the efflux deposit of the previous Update
+                        auto plane = [&](int k, auto p0) {
+                            constexpr bool P0 = decltype(p0)::value;
                             const int ln = cn + mc2 * (k - splo);
 #pragma unroll
-                            for (int c = 0; c < CSM; ++c)
-                                if (c < CS) {
-                                    uN[c] = ca[c * ccap + ln + mc2];
-                                    if (k == 0) uP[c] = uN[c];  // no-flux face: mirror
-                                }
+                            for (int c = 0; c < CSM; ++c) {
+                                uN[c] = ca[c * ccap + ln + mc2];
+                                if constexpr (P0) uP[c] = uN[c];  // no-flux face: mirror
+                            }
                             R evo[CSM];
 #pragma unroll
                             for (int c = 0; c < CSM; ++c) {
-                                evo[c] = 0;
-                                if (c < CS) {
-                                    const R* v = ca + c * ccap;
-                                    const R cc = uC[c];
-                                    evo[c] = RSK(cD[c]) * ((v[ln + 1] - 2 * cc + v[ln - 1]) * RSK(ih2) + (v[ln + mc] - 2 * cc + v[ln - mc]) * RSK(ih2) +
-                                                        (uN[c] - 2 * cc + uP[c]) * RSK(ih2));
-                                }
+                                const R* v = ca + c * ccap;
+                                const R cc = uC[c];
+                                evo[c] = RSK(cD[c]) * ((v[ln + 1] - 2 * cc + v[ln - 1]) * RSK(ih2) + (v[ln + mc] - 2 * cc + v[ln - mc]) * RSK(ih2) +
+                                                       (uN[c] - 2 * cc + uP[c]) * RSK(ih2));
                             }
                             int is = 0;
 #pragma unroll
@@ -642,16 +637,21 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                                 const R ion = uC[j2];
                                 R react = 0;
 #pragma unroll
-                                for (int c = NI; c < CSM; ++c)
-                                    if (c < CS && m.c_pair_ion[c - NI] == j2) {
+                                for (int c = NI; c < CSM; ++c) {
+                                    if (NI == 1 || m.c_pair_ion[c - NI] == j2) {
                                         R fr = RSK(cctp[c]);
+                                        if constexpr (NI == 1) {
+                                            fr -= uC[c];
+                                        } else {
 #pragma unroll
-                                        for (int c2 = NI; c2 < CSM; ++c2)
-                                            if ((a.kf.csame[c] >> c2) & 1) fr -= uC[c2];
+                                            for (int c2 = NI; c2 < CSM; ++c2)
+                                                if ((a.kf.csame[c] >> c2) & 1) fr -= uC[c2];
+                                        }
                                         const R R1 = RSK(ckoff[c]) * uC[c] - RSK(ckon[c]) * ion * fr;
                                         evo[c] += -R1;
                                         react += R1;
                                     }
+                                }
                                 evo[j2] += react;
                                 if (m.c_serca[j2]) {
                                     const R i2 = ion * ion;
@@ -660,28 +660,30 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                                 }
                             }
 #pragma unroll
-                            for (int c = 0; c < CSM; ++c)
-                                if (c < CS) {
-                                    R e = evo[c];
-                                    if (k == 0) {
-                                        // deposit of the previous Update, in the oracle's term order
-                                        double dep = 0;
-                                        if (it == 0) {
-                                            dep = a.cin[((size_t)s * CS + c) * mc2 + cn];
-                                        } else if (a.kf.cdep[c] >= 0) {
-                                            for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2)
-                                                dep += (double)terms[(prv * a.max_terms + dterm[q2]) * FD + a.kf.cdep[c]];
-                                        }
-                                        e += (R)dep;
+                            for (int c = 0; c < CSM; ++c) {
+                                R e = evo[c];
+                                if constexpr (P0) {
+                                    // deposit of the previous Update, in the oracle's term order
+                                    double dep = 0;
+                                    if (it == 0) {
+                                        if (c < CS) dep = a.cin[((size_t)s * CS + c) * mc2 + cn];
+                                    } else if (a.kf.cdep[c] >= 0) {
+                                        for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2)
+                                            dep += (double)terms[(prv * a.max_terms + dterm[q2]) * FD + a.kf.cdep[c]];
                                     }
-                                    cb[c * ccap + ln] = uC[c] + e * RSK(dt);
+                                    e += (R)dep;
                                 }
+                                cb[c * ccap + ln] = uC[c] + e * RSK(dt);
+                            }
 #pragma unroll
                             for (int c = 0; c < CSM; ++c) {
                                 uP[c] = uC[c];
                                 uC[c] = uN[c];
                             }
-                        }
+                        };
+                        int k = k0;
+                        if (k == 0) plane(k++, bconst<true>{});
+                        for (; k < k1; ++k) plane(k, bconst<false>{});
                     }
                 }
             }
