@@ -39,6 +39,10 @@ EXPORTS = (
     "casim_b200_get_all_mouth", "casim_b200_get_all_states", "casim_b200_last_step_ms",
     "casim_b200_last_step_launches", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
     "casim_b200_rng_draws_static", "casim_b200_path_note",
+    "casim_b200_sg_create", "casim_b200_sg_destroy", "casim_b200_sg_set_stream", "casim_b200_sg_num_params",
+    "casim_b200_sg_get_params", "casim_b200_sg_set_params", "casim_b200_sg_forward", "casim_b200_sg_gradients",
+    "casim_b200_sg_train_step", "casim_b200_sg_check", "casim_b200_sg_launches", "casim_b200_sg_last_error",
+    "casim_b200_sg_gemm",
 )
 
 
@@ -111,6 +115,20 @@ def lib():
         L.casim_b200_set_site_jsr.argtypes = [vp, dp]
         L.casim_b200_path_note.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         L.casim_b200_rng_draws_static.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.casim_b200_sg_create.argtypes = [i32, i32, i32, i32, ctypes.c_uint64, ctypes.POINTER(vp)]
+        L.casim_b200_sg_destroy.argtypes = [vp]
+        L.casim_b200_sg_set_stream.argtypes = [vp, vp]
+        L.casim_b200_sg_num_params.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.casim_b200_sg_get_params.argtypes = [vp, fp]
+        L.casim_b200_sg_set_params.argtypes = [vp, fp]
+        L.casim_b200_sg_forward.argtypes = [vp, vp, i32, vp]
+        L.casim_b200_sg_gradients.argtypes = [vp, vp, vp, i32, fp, fp]
+        L.casim_b200_sg_train_step.argtypes = [vp, vp, vp, i32, ctypes.c_float, fp]
+        L.casim_b200_sg_check.argtypes = [vp]
+        L.casim_b200_sg_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.casim_b200_sg_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+        L.casim_b200_sg_gemm.argtypes = [vp, vp, i32, i32, i32, vp]
         _lib = L
     return _lib
 

@@ -258,6 +258,7 @@ casim_status casim_b200_destroy(casim_h h) {
     if (h->d.rs_order) cudaFree(h->d.rs_order);
     if (h->d.rs_counter) cudaFree(h->d.rs_counter);
     if (h->d.rs_pow2) cudaFree(h->d.rs_pow2);
+    cb_resident_free(h->d);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);

@@ -47,6 +47,7 @@ struct cb_dev {
     int* rs_order = nullptr;
     int* rs_counter = nullptr;
     unsigned long long* rs_pow2 = nullptr;
+    struct cb_rs_plan* rs_plan = nullptr;  // host-side launch plan (resident.cu)
 };
 
 // plain path (plain.cu)
@@ -58,3 +59,4 @@ cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* la
 // resident path (resident.cu)
 bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* why);
 cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);
+void cb_resident_free(cb_dev& d);

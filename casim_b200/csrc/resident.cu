@@ -181,10 +181,12 @@ int thread_cap(const cb_dev& d, int nz) {
     return max_threads(d.precision == 0 ? 8 : 4, d.m.n_ions + npm_of(d.m.n_ions, pairs_of(d.m)), nz);
 }
 
-cudaError_t launch_t(const cb_dev& d, const rs_args& a, int nz, int C, int threads, cudaStream_t st, int n, int* dry = nullptr) {
+cudaError_t launch_t(const cb_dev& d, const rs_args& a, int nz, int C, int threads, cudaStream_t st, int n, int* dry = nullptr,
+                     int known = 0) {
     const int NI = d.m.n_ions, NP = pairs_of(d.m);
-    if (d.precision == 0) return nz == 1 ? cb_res_f64_z1(a, NI, NP, C, threads, st, n, dry) : cb_res_f64_z3(a, NI, NP, C, threads, st, n, dry);
-    return nz == 1 ? cb_res_f32_z1(a, NI, NP, C, threads, st, n, dry) : cb_res_f32_z3(a, NI, NP, C, threads, st, n, dry);
+    if (d.precision == 0)
+        return nz == 1 ? cb_res_f64_z1(a, NI, NP, C, threads, st, n, dry, known) : cb_res_f64_z3(a, NI, NP, C, threads, st, n, dry, known);
+    return nz == 1 ? cb_res_f32_z1(a, NI, NP, C, threads, st, n, dry, known) : cb_res_f32_z3(a, NI, NP, C, threads, st, n, dry, known);
 }
 
 bool species_supported(const cb_model& m) {
@@ -266,8 +268,22 @@ bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* 
     return true;
 }
 
-cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long* launches) {
-    if (n <= 0) return cudaSuccess;
+// launch plan of a batch, built on the first step and reused: one entry per
+// cluster-size class with its static arguments, block size and resident clusters
+struct cb_rs_plan {
+    int nz = 0;
+    std::vector<rs_args> args;
+    std::vector<int> cs, threads, clusters;
+};
+
+void cb_resident_free(cb_dev& d) {
+    delete d.rs_plan;
+    d.rs_plan = nullptr;
+}
+
+namespace {
+
+cudaError_t build_plan(cb_dev& d) {
     std::vector<cb_site> sites(d.S);
     cudaError_t e = cudaMemcpy(sites.data(), d.sites, sizeof(cb_site) * d.S, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return e;
@@ -277,48 +293,49 @@ cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long*
     if (classes.size() > 8) return cudaErrorInvalidConfiguration;
     const int nz = layers_of(d.m, sites);
     if (nz == 0) return cudaErrorInvalidConfiguration;
-    if (!d.rs_order) {
-        std::vector<int> order;
-        for (auto& c : classes) order.insert(order.end(), c.begin(), c.end());
-        if ((e = cudaMalloc(&d.rs_order, sizeof(int) * d.S)) != cudaSuccess) return e;
-        if ((e = cudaMemcpy(d.rs_order, order.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&d.rs_counter, sizeof(int) * 8)) != cudaSuccess) return e;
-        // MRG32k3a: A^(2^k) for k < 64 (both components), then the refill jump A^(2*31*LANE_DRAWS)
-        std::vector<unsigned long long> p2(65 * 18);
-        cbrng::Mat3 a1 = cbrng::step_matrix1(), a2 = cbrng::step_matrix2();
-        for (int k = 0; k < 64; ++k) {
-            for (int i = 0; i < 9; ++i) {
-                p2[18 * k + i] = a1.a[i / 3][i % 3];
-                p2[18 * k + 9 + i] = a2.a[i / 3][i % 3];
-            }
-            a1 = cbrng::matmul(a1, a1, cbrng::M1);
-            a2 = cbrng::matmul(a2, a2, cbrng::M2);
-        }
-        cbrng::Mat3 j1{{{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}}, j2 = j1;
-        unsigned long long steps = 2ULL * 31 * LANE_DRAWS;
-        for (int k = 0; steps; ++k, steps >>= 1)
-            if (steps & 1ULL) {
-                cbrng::Mat3 b1, b2;
-                for (int i = 0; i < 9; ++i) {
-                    b1.a[i / 3][i % 3] = p2[18 * k + i];
-                    b2.a[i / 3][i % 3] = p2[18 * k + 9 + i];
-                }
-                j1 = cbrng::matmul(b1, j1, cbrng::M1);
-                j2 = cbrng::matmul(b2, j2, cbrng::M2);
-            }
+    std::vector<int> order;
+    for (auto& c : classes) order.insert(order.end(), c.begin(), c.end());
+    if ((e = cudaMalloc(&d.rs_order, sizeof(int) * d.S)) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(d.rs_order, order.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&d.rs_counter, sizeof(int) * 8)) != cudaSuccess) return e;
+    // MRG32k3a: A^(2^k) for k < 64 (both components), then the refill jump A^(2*31*LANE_DRAWS)
+    std::vector<unsigned long long> p2(65 * 18);
+    cbrng::Mat3 a1 = cbrng::step_matrix1(), a2 = cbrng::step_matrix2();
+    for (int k = 0; k < 64; ++k) {
         for (int i = 0; i < 9; ++i) {
-            p2[18 * JUMP_ROW + i] = j1.a[i / 3][i % 3];
-            p2[18 * JUMP_ROW + 9 + i] = j2.a[i / 3][i % 3];
+            p2[18 * k + i] = a1.a[i / 3][i % 3];
+            p2[18 * k + 9 + i] = a2.a[i / 3][i % 3];
         }
-        if ((e = cudaMalloc(&d.rs_pow2, sizeof(unsigned long long) * p2.size())) != cudaSuccess) return e;
-        if ((e = cudaMemcpy(d.rs_pow2, p2.data(), sizeof(unsigned long long) * p2.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
-            return e;
+        a1 = cbrng::matmul(a1, a1, cbrng::M1);
+        a2 = cbrng::matmul(a2, a2, cbrng::M2);
     }
-    if ((e = cudaMemsetAsync(d.rs_counter, 0, sizeof(int) * 8, st)) != cudaSuccess) return e;
+    cbrng::Mat3 j1{{{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}}, j2 = j1;
+    unsigned long long steps = 2ULL * 31 * LANE_DRAWS;
+    for (int k = 0; steps; ++k, steps >>= 1)
+        if (steps & 1ULL) {
+            cbrng::Mat3 b1, b2;
+            for (int i = 0; i < 9; ++i) {
+                b1.a[i / 3][i % 3] = p2[18 * k + i];
+                b2.a[i / 3][i % 3] = p2[18 * k + 9 + i];
+            }
+            j1 = cbrng::matmul(b1, j1, cbrng::M1);
+            j2 = cbrng::matmul(b2, j2, cbrng::M2);
+        }
+    for (int i = 0; i < 9; ++i) {
+        p2[18 * JUMP_ROW + i] = j1.a[i / 3][i % 3];
+        p2[18 * JUMP_ROW + 9 + i] = j2.a[i / 3][i % 3];
+    }
+    if ((e = cudaMalloc(&d.rs_pow2, sizeof(unsigned long long) * p2.size())) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(d.rs_pow2, p2.data(), sizeof(unsigned long long) * p2.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    cb_rs_plan* P = new cb_rs_plan();
+    P->nz = nz;
     int offset = 0;
     for (size_t k = 0; k < classes.size(); ++k) {
         rs_args a{};
-        if (!plan(d, sites, classes[k], cs[k], a)) return cudaErrorInvalidConfiguration;
+        if (!plan(d, sites, classes[k], cs[k], a)) {
+            delete P;
+            return cudaErrorInvalidConfiguration;
+        }
         a.m = d.m;
         fill_const(d.m, a.kf);
         fill_const(d.m, a.kd);
@@ -326,7 +343,6 @@ cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long*
         a.order = d.rs_order + offset;
         a.S = (int)classes[k].size();
         a.counter = d.rs_counter + k;
-        a.fields = d.fields[d.cur];
         a.curgrid = d.curgrid;
         a.ch_node = d.ch_node;
         a.ch_owner = d.ch_owner;
@@ -334,7 +350,6 @@ cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long*
         a.mouth = d.mouth;
         a.NS = d.NS;
         a.sc = d.sc;
-        a.cyto = d.cyto[d.ccur];
         a.cin = d.cin;
         a.rim_cnode = d.rim_cnode;
         a.dep_ptr = d.dep_ptr;
@@ -345,12 +360,39 @@ cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long*
         a.spc0 = d.spc[0];
         a.spx1 = d.spx[1];
         a.spc1 = d.spc[1];
-        a.nsteps = n;
         const int threads = pick_threads(sites, classes[k], cs[k], thread_cap(d, nz));
-        e = launch_t(d, a, nz, cs[k], threads, st, a.S);
+        int clusters = 0;
+        e = launch_t(d, a, nz, cs[k], threads, 0, a.S, &clusters);
+        if (e != cudaSuccess || clusters < 1) {
+            delete P;
+            return e != cudaSuccess ? e : cudaErrorInvalidConfiguration;
+        }
+        P->args.push_back(a);
+        P->cs.push_back(cs[k]);
+        P->threads.push_back(threads);
+        P->clusters.push_back(clusters);
+        offset += a.S;
+    }
+    d.rs_plan = P;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long* launches) {
+    if (n <= 0) return cudaSuccess;
+    cudaError_t e;
+    if (!d.rs_plan && (e = build_plan(d)) != cudaSuccess) return e;
+    const cb_rs_plan& P = *d.rs_plan;
+    if ((e = cudaMemsetAsync(d.rs_counter, 0, sizeof(int) * 8, st)) != cudaSuccess) return e;
+    for (size_t k = 0; k < P.args.size(); ++k) {
+        rs_args a = P.args[k];
+        a.fields = d.fields[d.cur];
+        a.cyto = d.cyto[d.ccur];
+        a.nsteps = n;
+        e = launch_t(d, a, P.nz, P.cs[k], P.threads[k], st, a.S, nullptr, P.clusters[k]);
         if (e != cudaSuccess) return e;
         if (launches) *launches += 1;
-        offset += a.S;
     }
     return cudaSuccess;
 }

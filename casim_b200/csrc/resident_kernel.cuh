@@ -967,9 +967,10 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     }
 }
 
-// dry: only report how many clusters of this shape can be resident
+// dry: only report how many clusters of this shape can be resident;
+// known > 0: that count, from an earlier dry call
 template <typename R, int NI, int NPM, int NZ, int C>
-cudaError_t launch_one(const rs_args& a, int threads, cudaStream_t st, int n_sites, int* dry) {
+cudaError_t launch_one(const rs_args& a, int threads, cudaStream_t st, int n_sites, int* dry, int known) {
     auto kern = k_resident<R, NI, NPM, NZ, C>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, a.smem_bytes);
     if (e != cudaSuccess) return e;
@@ -989,9 +990,11 @@ cudaError_t launch_one(const rs_args& a, int threads, cudaStream_t st, int n_sit
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cfg.gridDim = dim3(C);
-    int clusters = 0;
-    e = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg);
-    if (e != cudaSuccess) return e;
+    int clusters = known;
+    if (clusters <= 0) {
+        e = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg);
+        if (e != cudaSuccess) return e;
+    }
     if (dry) {
         *dry = clusters;
         return cudaSuccess;
@@ -1003,31 +1006,31 @@ cudaError_t launch_one(const rs_args& a, int threads, cudaStream_t st, int n_sit
 }
 
 template <typename R, int NI, int NPM, int NZ>
-cudaError_t launch_c(const rs_args& a, int C, int threads, cudaStream_t st, int n, int* dry) {
+cudaError_t launch_c(const rs_args& a, int C, int threads, cudaStream_t st, int n, int* dry, int known) {
     switch (C) {
-    case 1: return launch_one<R, NI, NPM, NZ, 1>(a, threads, st, n, dry);
-    case 2: return launch_one<R, NI, NPM, NZ, 2>(a, threads, st, n, dry);
-    case 4: return launch_one<R, NI, NPM, NZ, 4>(a, threads, st, n, dry);
-    case 8: return launch_one<R, NI, NPM, NZ, 8>(a, threads, st, n, dry);
-    case 16: return launch_one<R, NI, NPM, NZ, 16>(a, threads, st, n, dry);
+    case 1: return launch_one<R, NI, NPM, NZ, 1>(a, threads, st, n, dry, known);
+    case 2: return launch_one<R, NI, NPM, NZ, 2>(a, threads, st, n, dry, known);
+    case 4: return launch_one<R, NI, NPM, NZ, 4>(a, threads, st, n, dry, known);
+    case 8: return launch_one<R, NI, NPM, NZ, 8>(a, threads, st, n, dry, known);
+    case 16: return launch_one<R, NI, NPM, NZ, 16>(a, threads, st, n, dry, known);
     default: return cudaErrorInvalidConfiguration;
     }
 }
 
 // NP: the larger of the cleft's ion-buffer pairs and (RD3D) the cytosol's
 template <typename R, int NZ>
-cudaError_t dispatch(const rs_args& a, int NI, int NP, int C, int threads, cudaStream_t st, int n, int* dry) {
+cudaError_t dispatch(const rs_args& a, int NI, int NP, int C, int threads, cudaStream_t st, int n, int* dry, int known) {
     if (threads > max_threads(sizeof(R), NI + npm_of(NI, NP), NZ)) return cudaErrorInvalidConfiguration;
-    if (NI == 1 && NP <= 2) return launch_c<R, 1, 2, NZ>(a, C, threads, st, n, dry);
-    if (NI == 1 && NP <= 4) return launch_c<R, 1, 4, NZ>(a, C, threads, st, n, dry);
-    if (NI == 2 && NP <= 4) return launch_c<R, 2, 4, NZ>(a, C, threads, st, n, dry);
+    if (NI == 1 && NP <= 2) return launch_c<R, 1, 2, NZ>(a, C, threads, st, n, dry, known);
+    if (NI == 1 && NP <= 4) return launch_c<R, 1, 4, NZ>(a, C, threads, st, n, dry, known);
+    if (NI == 2 && NP <= 4) return launch_c<R, 2, 4, NZ>(a, C, threads, st, n, dry, known);
     return cudaErrorInvalidConfiguration;
 }
 
 }  // namespace cbres
 
 // per (precision, layers) launchers, each compiled in its own translation unit
-cudaError_t cb_res_f32_z1(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*);
-cudaError_t cb_res_f32_z3(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*);
-cudaError_t cb_res_f64_z1(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*);
-cudaError_t cb_res_f64_z3(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*);
+cudaError_t cb_res_f32_z1(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*, int);
+cudaError_t cb_res_f32_z3(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*, int);
+cudaError_t cb_res_f64_z1(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*, int);
+cudaError_t cb_res_f64_z3(const cbres::rs_args&, int, int, int, int, cudaStream_t, int, int*, int);

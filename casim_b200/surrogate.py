@@ -1,0 +1,149 @@
+"""Surrogate of the quasi-steady Ca at the RyR mouths (host side).
+
+The network, its forward and backward passes and the Adam update run in
+libcasim_b200.so on the tensor cores (tcgen05, BF16 operands, FP32
+accumulation); this module binds the casim_b200_sg_* entry points of
+include/casim_b200.h and builds the training set from the plain RD solver of
+the same library: each snapshot is one site held at a fixed set of open RyRs
+(gating frozen) until the cleft Ca has relaxed, then read at every mouth.
+
+Features of a snapshot (config-1 layout, padded RyR slots are zero):
+    per RyR slot: open flag, x and y of the RyR scaled to [-1, 1] by the cleft
+    half-widths; then jSR Ca / 1000 uM; then each buffer total / its config value.
+Targets: log10(mouth Ca / 1 uM) per RyR slot (zero for empty slots).
+
+Device data are torch tensors (torch is the device-memory plumbing here).
+"""
+import ctypes
+
+import numpy as np
+
+from . import CasimError, lib
+
+WIDTH, DEPTH = 256, 4
+
+
+def _ck(st, h=None):
+    if st != 0:
+        msg = ""
+        if h:
+            buf = ctypes.create_string_buffer(1024)
+            lib().casim_b200_sg_last_error(h, buf, 1024)
+            msg = buf.value.decode()
+        raise CasimError(st, msg or "surrogate call failed")
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Surrogate:
+    """MLP n_in -> depth x width (GELU) -> n_out on the device."""
+
+    def __init__(self, n_in, n_out, width=WIDTH, depth=DEPTH, seed=1234):
+        self.n_in, self.n_out, self.width, self.depth = n_in, n_out, width, depth
+        self.h = ctypes.c_void_p()
+        _ck(lib().casim_b200_sg_create(n_in, n_out, width, depth, seed, ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().casim_b200_sg_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        _ck(lib().casim_b200_sg_set_stream(self.h, ctypes.c_void_p(stream_ptr)), self.h)
+
+    def num_params(self):
+        n = ctypes.c_int64()
+        _ck(lib().casim_b200_sg_num_params(self.h, ctypes.byref(n)), self.h)
+        return n.value
+
+    def layer_shapes(self):
+        """(dout, din) of each layer, padded as the library stores them."""
+        in_pad = (self.n_in + 63) // 64 * 64
+        out_pad = (self.n_out + 127) // 128 * 128
+        dims = [in_pad] + [self.width] * self.depth + [out_pad]
+        return [(dims[i + 1], dims[i]) for i in range(self.depth + 1)]
+
+    def get_params(self):
+        out = np.zeros(self.num_params(), np.float32)
+        _ck(lib().casim_b200_sg_get_params(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self.h)
+        return out
+
+    def set_params(self, flat):
+        flat = np.ascontiguousarray(flat, np.float32)
+        assert flat.size == self.num_params()
+        _ck(lib().casim_b200_sg_set_params(self.h, flat.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self.h)
+
+    def unflatten(self, flat):
+        """[(W [dout][din], b [dout]) per layer] views of a flat parameter vector."""
+        out, off = [], 0
+        for dout, din in self.layer_shapes():
+            w = flat[off:off + dout * din].reshape(dout, din)
+            off += dout * din
+            b = flat[off:off + dout]
+            off += dout
+            out.append((w, b))
+        return out
+
+    def forward(self, x):
+        """x: float32 CUDA tensor [batch, n_in], batch a multiple of 128."""
+        import torch
+        y = torch.empty((x.shape[0], self.n_out), dtype=torch.float32, device=x.device)
+        _ck(lib().casim_b200_sg_forward(self.h, _ptr(x), int(x.shape[0]), _ptr(y)), self.h)
+        return y
+
+    def gradients(self, x, t):
+        loss = ctypes.c_float()
+        g = np.zeros(self.num_params(), np.float32)
+        _ck(lib().casim_b200_sg_gradients(self.h, _ptr(x), _ptr(t), int(x.shape[0]), ctypes.byref(loss),
+                                          g.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self.h)
+        return float(loss.value), g
+
+    def train_step(self, x, t, lr):
+        loss = ctypes.c_float()
+        _ck(lib().casim_b200_sg_train_step(self.h, _ptr(x), _ptr(t), int(x.shape[0]), float(lr), ctypes.byref(loss)), self.h)
+        return float(loss.value)
+
+    def launches(self):
+        n = ctypes.c_int64()
+        _ck(lib().casim_b200_sg_launches(self.h, ctypes.byref(n)), self.h)
+        return n.value
+
+
+def gemm(a_bf16, b_bf16):
+    """C = A . B^T on the tensor cores; a [M, K], b [N, K] bfloat16 CUDA tensors."""
+    import torch
+    M, K = a_bf16.shape
+    N = b_bf16.shape[0]
+    c = torch.empty((M, N), dtype=torch.float32, device=a_bf16.device)
+    _ck(lib().casim_b200_sg_gemm(_ptr(a_bf16), _ptr(b_bf16), M, N, K, _ptr(c)))
+    return c
+
+
+def features(params, sites, open_mask, jsr, max_ch):
+    """Feature matrix [S, 3*max_ch + 1 + n_buf] of snapshot sites (see module doc)."""
+    S = len(sites["nx"])
+    off = np.concatenate([[0], np.cumsum(sites["n_ch"])])
+    d = params["Dyad"]
+    bufs = sorted(params["Buffers"].keys()) if "Buffers" in params else sorted(d.get("Buffers", {}).keys())
+    tot = [float(params["Buffers"][b]["Total Concentration"]) for b in bufs] if "Buffers" in params else []
+    X = np.zeros((S, 3 * max_ch + 1 + len(tot)), np.float32)
+    for s in range(S):
+        n = int(sites["n_ch"][s])
+        hx = 0.5 * (int(sites["nx"][s]) - 1) * float(d["dx"])
+        hy = 0.5 * (int(sites["ny"][s]) - 1) * float(d["dy"])
+        xs = sites["ch_x"][off[s]:off[s] + n]
+        ys = sites["ch_y"][off[s]:off[s] + n]
+        X[s, 0:3 * n:3] = open_mask[s, :n]
+        X[s, 1:3 * n:3] = (xs - hx) / hx
+        X[s, 2:3 * n:3] = (ys - hy) / hy
+        X[s, 3 * max_ch] = jsr[s] / 1000.0
+        X[s, 3 * max_ch + 1:] = 1.0  # buffer totals relative to the config values
+    return X

@@ -185,6 +185,41 @@ casim_status casim_b200_debug_rng(const uint32_t seed[6], int64_t n, double* out
  * memory. */
 casim_status casim_b200_rng_draws_static(const uint32_t seed[6], int64_t n, double* out);
 
+/* ---- Surrogate of the quasi-steady Ca at the RyR mouths (no counterpart in
+ * the reference; the plain RD step above generates its training snapshots and
+ * judges its error). An MLP n_in -> depth x width (GELU) -> n_out with BF16
+ * weights and activations and FP32 accumulation, every matrix product on the
+ * tensor cores (tcgen05.mma), FP32 master weights updated by Adam. x, t and y
+ * are DEVICE pointers to row-major FP32 [batch][n_in] / [batch][n_out];
+ * batch must be a multiple of 128. width is 64, 128, 192 or 256; n_in <= 256,
+ * n_out <= 256. */
+typedef struct casim_surrogate_s* casim_sg;
+casim_status casim_b200_sg_create(int n_in, int n_out, int width, int depth, uint64_t seed, casim_sg* out);
+casim_status casim_b200_sg_destroy(casim_sg h);
+casim_status casim_b200_sg_set_stream(casim_sg h, void* cuda_stream);
+/* Parameter count: per layer W [dout][din] then b [dout], with din and dout
+ * padded (n_in to a multiple of 64, n_out to a multiple of 128; padding is zero). */
+casim_status casim_b200_sg_num_params(casim_sg h, int64_t* n);
+/* FP32 parameters in the layout of casim_b200_sg_num_params (host memory). */
+casim_status casim_b200_sg_get_params(casim_sg h, float* host);
+casim_status casim_b200_sg_set_params(casim_sg h, const float* host);
+/* y = net(x). */
+casim_status casim_b200_sg_forward(casim_sg h, const float* x_dev, int batch, float* y_dev);
+/* Mean-square loss over the n_out outputs and the gradient of every parameter
+ * (host memory, parameter layout); no update. */
+casim_status casim_b200_sg_gradients(casim_sg h, const float* x_dev, const float* t_dev, int batch, float* loss, float* grads_host);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the mean-square loss; loss may be NULL. */
+casim_status casim_b200_sg_train_step(casim_sg h, const float* x_dev, const float* t_dev, int batch, float lr, float* loss);
+/* CASIM_ETIMEOUT if a tensor-core wait inside a kernel gave up. */
+casim_status casim_b200_sg_check(casim_sg h);
+/* Kernel launches issued by the handle so far. */
+casim_status casim_b200_sg_launches(casim_sg h, int64_t* out);
+casim_status casim_b200_sg_last_error(casim_sg h, char* buf, size_t n);
+/* One product C = A . B^T on the tensor cores: A [M][K] and B [N][K] BF16
+ * (bit patterns), C [M][N] FP32, all device memory; M a multiple of 128,
+ * N a multiple of 16 in [16, 256], K a multiple of 64. */
+casim_status casim_b200_sg_gemm(const void* a_dev, const void* b_dev, int M, int N, int K, float* c_dev);
+
 #ifdef __cplusplus
 }
 #endif
