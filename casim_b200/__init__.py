@@ -39,7 +39,7 @@ EXPORTS = (
     "casim_b200_get_all_mouth", "casim_b200_get_all_states", "casim_b200_last_step_ms",
     "casim_b200_last_step_launches", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
     "casim_b200_rng_draws_static", "casim_b200_path_note",
-    "casim_b200_sg_create", "casim_b200_sg_destroy", "casim_b200_sg_set_stream", "casim_b200_sg_num_params",
+    "casim_b200_set_all_states", "casim_b200_sg_create", "casim_b200_sg_destroy", "casim_b200_sg_set_stream", "casim_b200_sg_num_params",
     "casim_b200_sg_get_params", "casim_b200_sg_set_params", "casim_b200_sg_forward", "casim_b200_sg_gradients",
     "casim_b200_sg_train_step", "casim_b200_sg_check", "casim_b200_sg_launches", "casim_b200_sg_last_error",
     "casim_b200_sg_gemm",
@@ -109,6 +109,7 @@ def lib():
         L.casim_b200_check_finite.argtypes = [vp, ip]
         L.casim_b200_get_all_mouth.argtypes = [vp, i32, dp]
         L.casim_b200_get_all_states.argtypes = [vp, ip]
+        L.casim_b200_set_all_states.argtypes = [vp, ip]
         L.casim_b200_last_step_ms.argtypes = [vp, dp]
         L.casim_b200_last_step_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.casim_b200_debug_rng.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]
@@ -316,6 +317,11 @@ class ReleaseSiteBatch:
         out = np.zeros(int(self.n_ch.sum()), dtype=np.int32)
         self._ck(lib().casim_b200_get_all_states(self.h, _p(out, ctypes.c_int32)))
         return out
+
+    def set_all_states(self, states):
+        st = np.ascontiguousarray(states, dtype=np.int32).reshape(-1)
+        assert st.size == int(self.n_ch.sum())
+        self._ck(lib().casim_b200_set_all_states(self.h, _p(st, ctypes.c_int32)))
 
     def all_mouth(self, species):
         out = np.zeros(int(self.n_ch.sum()), dtype=np.float64)

@@ -511,6 +511,17 @@ casim_status casim_b200_get_states(casim_h h, int32_t site, int32_t* out) {
     END_GUARD(h)
 }
 
+casim_status casim_b200_set_all_states(casim_h h, const int32_t* states) {
+    GUARD(h)
+    if (!states) throw std::runtime_error("states is null");
+    for (long long c = 0; c < h->d.total_ch; ++c)
+        if (states[c] != 0 && states[c] != 1) throw std::runtime_error("RyR states must be 0 or 1");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    ck(cudaMemcpy(h->d.ch_state, states, sizeof(int) * (size_t)h->d.total_ch, cudaMemcpyHostToDevice), "cudaMemcpy");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
 casim_status casim_b200_get_all_states(casim_h h, int32_t* out) {
     GUARD(h)
     ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");

@@ -132,9 +132,8 @@ def features(params, sites, open_mask, jsr, max_ch):
     S = len(sites["nx"])
     off = np.concatenate([[0], np.cumsum(sites["n_ch"])])
     d = params["Dyad"]
-    bufs = sorted(params["Buffers"].keys()) if "Buffers" in params else sorted(d.get("Buffers", {}).keys())
-    tot = [float(params["Buffers"][b]["Total Concentration"]) for b in bufs] if "Buffers" in params else []
-    X = np.zeros((S, 3 * max_ch + 1 + len(tot)), np.float32)
+    n_buf = len(d.get("Buffers", {}))
+    X = np.zeros((S, 3 * max_ch + 1 + n_buf), np.float32)
     for s in range(S):
         n = int(sites["n_ch"][s])
         hx = 0.5 * (int(sites["nx"][s]) - 1) * float(d["dx"])
@@ -147,3 +146,81 @@ def features(params, sites, open_mask, jsr, max_ch):
         X[s, 3 * max_ch] = jsr[s] / 1000.0
         X[s, 3 * max_ch + 1:] = 1.0  # buffer totals relative to the config values
     return X
+
+
+# ---------------------------------------------------------------- snapshots
+RELAX_STEPS = 5000  # 0.25 ms at dt = 50 ns: the time a frozen open set is held before the mouths are read
+CA_REF_UM = 1.0     # targets are log10(mouth Ca / CA_REF_UM)
+
+
+def snapshot_batch(n_sites, seed=0, n_ryr=20, max_open=4, jsr_range=(500.0, 1500.0)):
+    """Config-1 sites (2D 64 x 64, 20 RyRs on the jittered 31 nm lattice) with a
+    random frozen open set of 1..max_open RyRs and a constant jSR Ca per site.
+    Returns (params, sites, open_mask [S, n_ryr], jsr [S])."""
+    from . import configs
+    frozen = {"kopen0": 0.0, "ncaopen": 2.5, "kopenmax": 1e15, "kclose0": 0.0, "ncaclose": 0.0}
+    p = configs.base_params(dim=2, nx=64, ny=64, gating=frozen)
+    p["jSR"]["Constant"] = True
+    p = configs._clean(p)
+    rng = np.random.default_rng(seed)
+    xs, ys, seeds = [], [], []
+    jsr = rng.uniform(jsr_range[0], jsr_range[1], size=n_sites)
+    mask = np.zeros((n_sites, n_ryr), np.float32)
+    for k in range(n_sites):
+        x, y = configs.lattice(n_ryr, 63 * 5.0, 63 * 5.0, rng)
+        xs += x
+        ys += y
+        seeds.append([int(v) for v in rng.integers(1, 4294944443, size=6)])
+        n_open = int(rng.integers(1, max_open + 1))
+        mask[k, rng.choice(n_ryr, size=n_open, replace=False)] = 1.0
+    sites = configs.sites_table([64] * n_sites, [64] * n_sites, [1] * n_sites, [n_ryr] * n_sites, xs, ys, seeds,
+                                jsr_init=jsr.reshape(-1, 1))
+    return p, sites, mask, jsr
+
+
+def rd_snapshots(n_sites, seed=0, relax_steps=RELAX_STEPS, precision="fp32", n_ryr=20, max_open=4):
+    """Features and targets of n_sites snapshots computed by the plain RD method
+    of this library: reset, open the frozen set, relax_steps RD steps, read the
+    Ca at every mouth. Returns (X [S, F], Y [S, n_ryr], seconds of RD device time)."""
+    from . import ReleaseSiteBatch
+    p, s, mask, jsr = snapshot_batch(n_sites, seed, n_ryr, max_open)
+    sim = ReleaseSiteBatch(p, s, precision=precision, path="auto")
+    sim.reset()
+    sim.set_all_states(mask.astype(np.int32).reshape(-1))
+    sim.update()
+    sim.step(relax_steps)
+    sim.synchronize()
+    secs = sim.last_step_ms() / 1e3
+    st = sim.all_states().reshape(n_sites, n_ryr)
+    assert np.array_equal(st, mask.astype(np.int32)), "gating was not frozen"
+    ca = sim.all_mouth(0).reshape(n_sites, n_ryr)
+    sim.close()
+    X = features(p, s, mask, jsr, n_ryr)
+    Y = np.log10(np.maximum(ca, 1e-6) / CA_REF_UM).astype(np.float32)
+    return X, Y, secs
+
+
+def train(net, X, Y, steps, batch=4096, lr=1e-3, seed=0, lr_decay=True):
+    """Adam on random mini-batches of (X, Y) held on the device; returns the loss history."""
+    import torch
+    xd = torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda()
+    yd = torch.from_numpy(np.ascontiguousarray(Y, np.float32)).cuda()
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    n = xd.shape[0]
+    batch = min(batch, n // 128 * 128)
+    hist = []
+    for k in range(steps):
+        idx = torch.randint(0, n, (batch,), device="cuda", generator=g)
+        rate = lr * (0.5 * (1 + np.cos(np.pi * k / steps)) if lr_decay else 1.0) + 1e-6
+        hist.append(net.train_step(xd[idx].contiguous(), yd[idx].contiguous(), rate))
+    return hist
+
+
+def predict(net, X):
+    """Network output for X (host array), padding the batch to a multiple of 128."""
+    import torch
+    n = X.shape[0]
+    npad = (n + 127) // 128 * 128
+    xp = np.zeros((npad, X.shape[1]), np.float32)
+    xp[:n] = X
+    return net.forward(torch.from_numpy(xp).cuda()).cpu().numpy()[:n]

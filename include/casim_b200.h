@@ -134,6 +134,12 @@ casim_status casim_b200_set_field(casim_h h, int32_t site, int32_t species, cons
 casim_status casim_b200_get_mouth(casim_h h, int32_t site, int32_t species, double* out);
 /* DyadSeries::GetChannelsStates (CaSim/DyadSeries.h:30): 0/1 per RyR. */
 casim_status casim_b200_get_states(casim_h h, int32_t site, int32_t* out);
+/* Overwrites the open (1) / closed (0) state of every RyR of the batch
+ * (site-major, as casim_b200_get_all_states returns them) without consuming
+ * draws; call casim_b200_update afterwards so the currents follow. Generalises
+ * DyadSeries::InitOpening (CaSim/DyadSeries.h:21), which opens one RyR per
+ * site; used to hold arbitrary open sets (surrogate training snapshots). */
+casim_status casim_b200_set_all_states(casim_h h, const int32_t* states);
 /* SRSeries::GetIons (CaSim/SRSeries.h:12): jSR concentration per ion. */
 casim_status casim_b200_get_jsr(casim_h h, int32_t site, double* out);
 /* DyadSeries::GetTotalSRCurrent (CaSim/DyadSeries.h:24): per ion. */

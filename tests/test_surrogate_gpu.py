@@ -81,3 +81,30 @@ def test_training_lowers_loss(cuda_device):
     assert last < 0.1 * first, (first, last)
     assert np.all(np.isfinite(net.get_params()))
     net.close()
+
+
+def test_surrogate_learns_rd_snapshots_and_beats_rd_cost(cuda_device):
+    """Snapshots of the plain RD method (frozen open sets, 0.25 ms relaxation)
+    train the network on the device; on held-out sites it predicts the mouth
+    Ca at a small fraction of the RD cost."""
+    import time
+    import torch
+    X, Y, rd_s = sg.rd_snapshots(8192, seed=100)
+    Xv, Yv, _ = sg.rd_snapshots(1024, seed=999)
+    net = sg.Surrogate(X.shape[1], Y.shape[1], seed=3)
+    hist = sg.train(net, X, Y, 1500, batch=4096, lr=2e-3)
+    assert np.mean(hist[-50:]) < 0.01 * hist[0]
+    P = sg.predict(net, Xv)
+    rel = np.abs(10.0 ** P - 10.0 ** Yv) / 10.0 ** Yv
+    assert np.median(rel) < 0.10, np.median(rel)
+    xd = torch.zeros((4096, X.shape[1]), dtype=torch.float32, device="cuda")
+    net.forward(xd)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    for _ in range(10):
+        net.forward(xd)
+    torch.cuda.synchronize()
+    per_site_nn = (time.time() - t0) / 10 / 4096
+    per_site_rd = rd_s / 8192
+    assert per_site_nn * 100 < per_site_rd, (per_site_nn, per_site_rd)
+    net.close()
