@@ -511,6 +511,31 @@ casim_status casim_b200_get_states(casim_h h, int32_t site, int32_t* out) {
     END_GUARD(h)
 }
 
+casim_status casim_b200_sg_features(casim_h h, int32_t max_channels, int32_t ld, float* x_dev) {
+    GUARD(h)
+    if (!x_dev || max_channels < 1 || ld < 3 * max_channels + 1 + h->d.m.n_buf) throw std::runtime_error("bad feature layout");
+    ck(cb_sg_features(h->d, max_channels, ld, x_dev, h->stream), "surrogate features");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_sg_set_mouth(casim_h h, const float* y_dev, int32_t ld, double ca_ref) {
+    GUARD(h)
+    if (!y_dev || ld < 1 || !(ca_ref > 0)) throw std::runtime_error("bad network output layout");
+    ck(cb_sg_mouth(h->d, y_dev, ld, ca_ref, h->stream), "surrogate mouth");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_sg_gate_steps(casim_h h, int64_t n) {
+    GUARD(h)
+    if (n < 0) throw std::runtime_error("negative step count");
+    if (h->d.m.cyto_type != CB_CYTO_POOL) throw std::runtime_error("surrogate gating needs the pool cytosol");
+    if (n > 0) ck(cb_sg_steps(h->d, n, h->stream), "surrogate steps");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
 casim_status casim_b200_set_all_states(casim_h h, const int32_t* states) {
     GUARD(h)
     if (!states) throw std::runtime_error("states is null");

@@ -56,6 +56,11 @@ cudaError_t cb_plain_init_opening(cb_dev& d, const int* d_first, int site_lo, in
 cudaError_t cb_plain_update(cb_dev& d, cudaStream_t st, long long* launches);
 cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);
 
+// surrogate-driven gating without the RD step (plain.cu)
+cudaError_t cb_sg_features(cb_dev& d, int max_ch, int ld, float* X, cudaStream_t st);
+cudaError_t cb_sg_mouth(cb_dev& d, const float* Y, int ld, double ca_ref, cudaStream_t st);
+cudaError_t cb_sg_steps(cb_dev& d, long long n, cudaStream_t st);
+
 // resident path (resident.cu)
 bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* why);
 cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);

@@ -459,6 +459,89 @@ cudaError_t launch_step(cb_dev& d, cudaStream_t st) {
     return launch_update<R>(d, st);
 }
 
+// ---- surrogate-driven gating (no RD): the mouth Ca comes from the surrogate network
+
+// features of every site (one thread per site): per RyR slot its open flag and
+// grid position scaled to [-1, 1] by the cleft half-widths, then the jSR Ca of
+// the first ion / 1000 uM, then each dyad buffer total relative to its config value
+__global__ void k_sg_features(int S, int n_buf, int max_ch, int ld, const cb_site* __restrict__ sites, const int* __restrict__ ch_node,
+                              const int* __restrict__ ch_state, const cb_site_scalars* __restrict__ sc, float* __restrict__ X) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const cb_site st = sites[s];
+    float* row = X + (size_t)s * ld;
+    for (int k = 0; k < ld; ++k) row[k] = 0.0f;
+    const float hx = 0.5f * (st.nx - 1), hy = 0.5f * (st.ny - 1);
+    for (int c = 0; c < st.n_ch && c < max_ch; ++c) {
+        const int node = ch_node[st.ch_off + c];
+        const int gx = node % st.nx, gy = (node / st.nx) % st.ny;
+        row[3 * c] = (float)ch_state[st.ch_off + c];
+        row[3 * c + 1] = (gx - hx) / hx;
+        row[3 * c + 2] = (gy - hy) / hy;
+    }
+    row[3 * max_ch] = (float)(sc[s].jsr_new[0] / 1000.0);
+    for (int b = 0; b < n_buf; ++b) row[3 * max_ch + 1 + b] = 1.0f;
+}
+
+// mouth Ca of every RyR from the network output: ca_ref * 10^y
+__global__ void k_sg_mouth(int S, int NS, int ca_idx, double ca_ref, int ld, const cb_site* __restrict__ sites,
+                           const float* __restrict__ Y, double* __restrict__ mouth) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const cb_site st = sites[s];
+    for (int c = 0; c < st.n_ch && c < ld; ++c)
+        mouth[(size_t)(st.ch_off + c) * NS + ca_idx] = ca_ref * exp10((double)Y[(size_t)s * ld + c]);
+}
+
+// n time steps of one site without the RD step: cytosol pool and jSR ODEs and
+// RyR gating in the order of k_pre, then the part of Update that needs no
+// field: RyR currents from the held mouth values and the jSR coupling
+__global__ void k_sg_steps(cb_model m, int S, int NS, long long n, const cb_site* __restrict__ sites, cb_site_scalars* __restrict__ sc,
+                           int* __restrict__ ch_state, const double* __restrict__ mouth, const double* __restrict__ spx0,
+                           const double* __restrict__ spc0, const double* __restrict__ spx1, const double* __restrict__ spc1) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const cb_site st = sites[s];
+    cb_site_scalars& q = sc[s];
+    const double dt = m.dt;
+    cbrng::State g;
+    for (int i = 0; i < 6; ++i) g.s[i] = q.rng[i];
+    unsigned long long draws = 0;
+    for (long long it = 0; it < n; ++it) {
+        if (m.cyto_type == CB_CYTO_POOL) pool_step(m, q, dt);
+        jsr_step(m, q, dt);
+        for (int c = 0; c < st.n_ch; ++c) {
+            const double* mo = mouth + (long long)(st.ch_off + c) * NS;
+            const double ca = mo[m.ca_idx];
+            const double mg = m.mg_idx >= 0 ? mo[m.mg_idx] : 0.0;
+            const int state = ch_state[st.ch_off + c];
+            const double r = cb_rate(m, spx0, spc0, spx1, spc1, state, ca, mg);
+            ++draws;
+            if (cbrng::u01d(g) < r * dt) {
+                (void)cbrng::u01d(g);
+                ++draws;
+                ch_state[st.ch_off + c] = 1 - state;
+            }
+        }
+        double tot[CB_MAX_IONS];
+        for (int j = 0; j < m.n_ions; ++j) tot[j] = 0;
+        for (int c = 0; c < st.n_ch; ++c) {
+            const int state = ch_state[st.ch_off + c];
+            const double* mo = mouth + (long long)(st.ch_off + c) * NS;
+            for (int j = 0; j < m.n_ions; ++j) tot[j] += state * (m.g[j] * (q.jsr_new[j] - mo[j]));
+        }
+        for (int j = 0; j < m.n_ions; ++j) q.total[j] = tot[j];
+        if (!m.jsr_const)
+            for (int i = 0; i < m.n_ions; ++i) {
+                q.IjSR[i] = q.total[i] * m.V_elem;
+                q.nsr[i] = m.nsr[i];
+                q.jsr[i] = q.jsr_new[i];
+            }
+    }
+    q.draws += draws;
+    for (int i = 0; i < 6; ++i) q.rng[i] = g.s[i];
+}
+
 template <typename R>
 cudaError_t reset_impl(cb_dev& d, cudaStream_t st) {
     dim3 g(std::max(1, std::min(64, (d.max_nodes + 255) / 256)), d.S);
@@ -498,4 +581,20 @@ cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* la
         if (launches) *launches += per;
     }
     return cudaSuccess;
+}
+
+cudaError_t cb_sg_features(cb_dev& d, int max_ch, int ld, float* X, cudaStream_t st) {
+    k_sg_features<<<(d.S + 127) / 128, 128, 0, st>>>(d.S, d.m.n_buf, max_ch, ld, d.sites, d.ch_node, d.ch_state, d.sc, X);
+    return cudaGetLastError();
+}
+
+cudaError_t cb_sg_mouth(cb_dev& d, const float* Y, int ld, double ca_ref, cudaStream_t st) {
+    k_sg_mouth<<<(d.S + 127) / 128, 128, 0, st>>>(d.S, d.NS, d.m.ca_idx, ca_ref, ld, d.sites, Y, d.mouth);
+    return cudaGetLastError();
+}
+
+cudaError_t cb_sg_steps(cb_dev& d, long long n, cudaStream_t st) {
+    k_sg_steps<<<(d.S + 127) / 128, 128, 0, st>>>(d.m, d.S, d.NS, n, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0],
+                                                  d.spx[1], d.spc[1]);
+    return cudaGetLastError();
 }

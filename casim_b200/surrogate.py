@@ -7,9 +7,11 @@ include/casim_b200.h and builds the training set from the plain RD solver of
 the same library: each snapshot is one site held at a fixed set of open RyRs
 (gating frozen) until the cleft Ca has relaxed, then read at every mouth.
 
-Features of a snapshot (config-1 layout, padded RyR slots are zero):
-    per RyR slot: open flag, x and y of the RyR scaled to [-1, 1] by the cleft
-    half-widths; then jSR Ca / 1000 uM; then each buffer total / its config value.
+Features of a site (config-1 layout, built on the device from the site's
+current state so that training and use see the same values; padded RyR slots
+are zero): per RyR slot its open flag and grid position scaled to [-1, 1] by
+the cleft half-widths; then jSR Ca / 1000 uM; then each buffer total / its
+config value.
 Targets: log10(mouth Ca / 1 uM) per RyR slot (zero for empty slots).
 
 Device data are torch tensors (torch is the device-memory plumbing here).
@@ -127,24 +129,18 @@ def gemm(a_bf16, b_bf16):
     return c
 
 
-def features(params, sites, open_mask, jsr, max_ch):
-    """Feature matrix [S, 3*max_ch + 1 + n_buf] of snapshot sites (see module doc)."""
-    S = len(sites["nx"])
-    off = np.concatenate([[0], np.cumsum(sites["n_ch"])])
-    d = params["Dyad"]
-    n_buf = len(d.get("Buffers", {}))
-    X = np.zeros((S, 3 * max_ch + 1 + n_buf), np.float32)
-    for s in range(S):
-        n = int(sites["n_ch"][s])
-        hx = 0.5 * (int(sites["nx"][s]) - 1) * float(d["dx"])
-        hy = 0.5 * (int(sites["ny"][s]) - 1) * float(d["dy"])
-        xs = sites["ch_x"][off[s]:off[s] + n]
-        ys = sites["ch_y"][off[s]:off[s] + n]
-        X[s, 0:3 * n:3] = open_mask[s, :n]
-        X[s, 1:3 * n:3] = (xs - hx) / hx
-        X[s, 2:3 * n:3] = (ys - hy) / hy
-        X[s, 3 * max_ch] = jsr[s] / 1000.0
-        X[s, 3 * max_ch + 1:] = 1.0  # buffer totals relative to the config values
+def n_features(max_ch, n_buf=2):
+    return 3 * max_ch + 1 + n_buf
+
+
+def device_features(sim, max_ch):
+    """Features of every site of a ReleaseSiteBatch from its current RyR states and
+    jSR Ca, built on the device (casim_b200_sg_features); a CUDA tensor
+    [S padded to a multiple of 128, n_features]."""
+    import torch
+    ld = n_features(max_ch, int(sim.info.n_buffers))
+    X = torch.zeros(((sim.S + 127) // 128 * 128, ld), dtype=torch.float32, device="cuda")
+    sim._ck(lib().casim_b200_sg_features(sim.h, max_ch, ld, _ptr(X)))
     return X
 
 
@@ -153,7 +149,7 @@ RELAX_STEPS = 5000  # 0.25 ms at dt = 50 ns: the time a frozen open set is held 
 CA_REF_UM = 1.0     # targets are log10(mouth Ca / CA_REF_UM)
 
 
-def snapshot_batch(n_sites, seed=0, n_ryr=20, max_open=4, jsr_range=(500.0, 1500.0)):
+def snapshot_batch(n_sites, seed=0, n_ryr=20, max_open=20, jsr_range=(100.0, 1500.0)):
     """Config-1 sites (2D 64 x 64, 20 RyRs on the jittered 31 nm lattice) with a
     random frozen open set of 1..max_open RyRs and a constant jSR Ca per site.
     Returns (params, sites, open_mask [S, n_ryr], jsr [S])."""
@@ -171,14 +167,14 @@ def snapshot_batch(n_sites, seed=0, n_ryr=20, max_open=4, jsr_range=(500.0, 1500
         xs += x
         ys += y
         seeds.append([int(v) for v in rng.integers(1, 4294944443, size=6)])
-        n_open = int(rng.integers(1, max_open + 1))
+        n_open = int(rng.integers(1, min(max_open, n_ryr) + 1))
         mask[k, rng.choice(n_ryr, size=n_open, replace=False)] = 1.0
     sites = configs.sites_table([64] * n_sites, [64] * n_sites, [1] * n_sites, [n_ryr] * n_sites, xs, ys, seeds,
                                 jsr_init=jsr.reshape(-1, 1))
     return p, sites, mask, jsr
 
 
-def rd_snapshots(n_sites, seed=0, relax_steps=RELAX_STEPS, precision="fp32", n_ryr=20, max_open=4):
+def rd_snapshots(n_sites, seed=0, relax_steps=RELAX_STEPS, precision="fp32", n_ryr=20, max_open=20):
     """Features and targets of n_sites snapshots computed by the plain RD method
     of this library: reset, open the frozen set, relax_steps RD steps, read the
     Ca at every mouth. Returns (X [S, F], Y [S, n_ryr], seconds of RD device time)."""
@@ -194,8 +190,8 @@ def rd_snapshots(n_sites, seed=0, relax_steps=RELAX_STEPS, precision="fp32", n_r
     st = sim.all_states().reshape(n_sites, n_ryr)
     assert np.array_equal(st, mask.astype(np.int32)), "gating was not frozen"
     ca = sim.all_mouth(0).reshape(n_sites, n_ryr)
+    X = device_features(sim, n_ryr)[:n_sites].cpu().numpy()
     sim.close()
-    X = features(p, s, mask, jsr, n_ryr)
     Y = np.log10(np.maximum(ca, 1e-6) / CA_REF_UM).astype(np.float32)
     return X, Y, secs
 
@@ -224,3 +220,25 @@ def predict(net, X):
     xp = np.zeros((npad, X.shape[1]), np.float32)
     xp[:n] = X
     return net.forward(torch.from_numpy(xp).cuda()).cpu().numpy()[:n]
+
+
+class SurrogateGating:
+    """Gating of a ReleaseSiteBatch (pool cytosol) driven by the surrogate's
+    mouth Ca instead of the RD step: every `window` time steps the network is
+    evaluated on the features of the current open sets and jSR Ca and the mouth
+    Ca replaced; in between, gating, the jSR and pool ODEs and the RyR currents
+    run on the device with the mouth values held (casim_b200_sg_gate_steps)."""
+
+    def __init__(self, net, sim, max_ch=20, window=20):
+        self.net, self.sim, self.max_ch, self.window = net, sim, max_ch, window
+
+    def step(self, n):
+        L = lib()
+        done = 0
+        while done < n:
+            k = min(self.window, n - done)
+            X = device_features(self.sim, self.max_ch)
+            Y = self.net.forward(X)
+            self.sim._ck(L.casim_b200_sg_set_mouth(self.sim.h, _ptr(Y), int(Y.shape[1]), CA_REF_UM))
+            self.sim._ck(L.casim_b200_sg_gate_steps(self.sim.h, k))
+            done += k

@@ -221,6 +221,19 @@ casim_status casim_b200_sg_check(casim_sg h);
 /* Kernel launches issued by the handle so far. */
 casim_status casim_b200_sg_launches(casim_sg h, int64_t* out);
 casim_status casim_b200_sg_last_error(casim_sg h, char* buf, size_t n);
+/* Surrogate-driven gating of a batch (casim_h). Features of every site into
+ * x_dev [n_sites][ld] FP32 (device): per RyR slot (max_channels slots) its
+ * open flag and grid position scaled to [-1, 1], then jSR Ca / 1000 uM, then
+ * each dyad buffer total relative to its config value
+ * (ld >= 3 max_channels + 1 + buffers). */
+casim_status casim_b200_sg_features(casim_h h, int32_t max_channels, int32_t ld, float* x_dev);
+/* Mouth Ca of every RyR = ca_ref * 10^y from the network output y_dev
+ * [n_sites][ld] FP32 (device), RyR c of a site in column c. */
+casim_status casim_b200_sg_set_mouth(casim_h h, const float* y_dev, int32_t ld, double ca_ref);
+/* n time steps without the RD step (pool cytosol only): cytosol pool and jSR
+ * ODEs, RyR gating (the draws of casim_b200_step) and RyR currents from the
+ * mouth values held since casim_b200_sg_set_mouth. */
+casim_status casim_b200_sg_gate_steps(casim_h h, int64_t n);
 /* One product C = A . B^T on the tensor cores: A [M][K] and B [N][K] BF16
  * (bit patterns), C [M][N] FP32, all device memory; M a multiple of 128,
  * N a multiple of 16 in [16, 256], K a multiple of 64. */
