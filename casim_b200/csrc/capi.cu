@@ -23,6 +23,7 @@ struct casim_b200_sim {
     std::string err;
     int path = CASIM_PATH_PLAIN;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timed = false;  // both events recorded by a step
     double last_ms = 0;
     long long last_launches = 0;
     std::vector<void*> allocs;
@@ -385,6 +386,7 @@ casim_status casim_b200_step(casim_h h, int64_t n) {
     if (h->path == CASIM_PATH_RESIDENT) ck(cb_resident_step(h->d, n, h->stream, &launches), "resident step");
     else ck(cb_plain_step(h->d, n, h->stream, &launches), "plain step");
     ck(cudaEventRecord(h->ev1, h->stream), "cudaEventRecord");
+    h->timed = true;
     h->last_launches = launches;
     return CASIM_OK;
     END_GUARD(h)
@@ -394,7 +396,12 @@ casim_status casim_b200_synchronize(casim_h h) {
     GUARD(h)
     ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
     float ms = 0;
-    if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) h->last_ms = ms;
+    // only after a step recorded both events; a failed query must not leave
+    // its error behind for the next cudaGetLastError of another library
+    if (h->timed) {
+        if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) h->last_ms = ms;
+        else cudaGetLastError();
+    }
     return CASIM_OK;
     END_GUARD(h)
 }

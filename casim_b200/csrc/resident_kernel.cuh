@@ -343,18 +343,20 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             for (int i = 0; i < 6; ++i) s_rng[lane * 6 + i] = gl.s[i];
             if (lane == 0) s_D = s_we = 0;
         }
-        // stencil partition of this rank: strips of RS rows x 32 columns over the
-        // worker warps, RS minimising the rounds x (rows per strip + 1 row of setup)
+        // stencil partition of this rank: a lane owns one interior column of a
+        // strip of RS rows; (strip, column) pairs are dealt to the worker lanes
+        // in order, so a warp may span two strips and no lane idles on a ragged
+        // row end. RS minimises the rounds x (rows per strip + 1 row of setup).
         const int ylo = max(lo, 1), yhi = min(hi, ny - 1);
         const int nrows = max(yhi - ylo, 0);
-        const int XB = (nx - 2 + 31) >> 5;
+        const int nxi = nx - 2;
         const int NW = W - 2;
         int RS = max(nrows, 1);
         {
             long long best = 1LL << 62;
             for (int rs = 1; rs <= nrows; ++rs) {
-                const int strips = XB * ((nrows + rs - 1) / rs);
-                const long long cost = (long long)((strips + NW - 1) / NW) * (rs + 1);
+                const int tasks = nxi * ((nrows + rs - 1) / rs);
+                const long long cost = (long long)((tasks + 32 * NW - 1) / (32 * NW)) * (rs + 1);
                 if (cost < best) {
                     best = cost;
                     RS = rs;
@@ -504,10 +506,9 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 // have zero coefficients), so the loops carry no species-count tests;
                 // constants are kernel-parameter operands.
                 const int wk = warp - 2;
-                for (int sI = wk; sI < XB * nchunk; sI += NW) {
-                    const int ch = sI / XB;
-                    const int x = 1 + ((sI - ch * XB) << 5) + lane;
-                    if (x > nx - 2) continue;
+                for (int t = wk * 32 + lane; t < nxi * nchunk; t += NW * 32) {
+                    const int ch = t / nxi;
+                    const int x = 1 + (t - ch * nxi);
                     const int y0 = ylo + ch * RS, y1 = min(y0 + RS, yhi);
                     // previous / current / next row of every species and layer
                     R vP[FP][NZ], vC[FP][NZ], vN[FP][NZ];

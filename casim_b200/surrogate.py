@@ -140,7 +140,11 @@ def device_features(sim, max_ch):
     import torch
     ld = n_features(max_ch, int(sim.info.n_buffers))
     X = torch.zeros(((sim.S + 127) // 128 * 128, ld), dtype=torch.float32, device="cuda")
+    # the batch runs on its own stream unless one was set: order the zero fill
+    # (torch's stream) before the kernel and the kernel before any later reader
+    torch.cuda.current_stream().synchronize()
     sim._ck(lib().casim_b200_sg_features(sim.h, max_ch, ld, _ptr(X)))
+    sim.synchronize()
     return X
 
 
@@ -227,7 +231,9 @@ class SurrogateGating:
     mouth Ca instead of the RD step: every `window` time steps the network is
     evaluated on the features of the current open sets and jSR Ca and the mouth
     Ca replaced; in between, gating, the jSR and pool ODEs and the RyR currents
-    run on the device with the mouth values held (casim_b200_sg_gate_steps)."""
+    run on the device with the mouth values held (casim_b200_sg_gate_steps).
+    The batch, the network and torch each keep their own stream; every window
+    synchronises where one hands data to another."""
 
     def __init__(self, net, sim, max_ch=20, window=20):
         self.net, self.sim, self.max_ch, self.window = net, sim, max_ch, window
@@ -237,8 +243,9 @@ class SurrogateGating:
         done = 0
         while done < n:
             k = min(self.window, n - done)
-            X = device_features(self.sim, self.max_ch)
-            Y = self.net.forward(X)
+            X = device_features(self.sim, self.max_ch)  # returns after the batch's stream is idle
+            Y = self.net.forward(X)                     # returns after the network's stream is idle
             self.sim._ck(L.casim_b200_sg_set_mouth(self.sim.h, _ptr(Y), int(Y.shape[1]), CA_REF_UM))
             self.sim._ck(L.casim_b200_sg_gate_steps(self.sim.h, k))
+            self.sim.synchronize()                      # Y may be reused once this returns
             done += k
