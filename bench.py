@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate-versus-RD report")
     return ap.parse_args()
 
 
@@ -107,6 +108,12 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_resident launches of one
+# bench step on 512 sites of the config-2 workload, per site (FP32): each launch loads
+# and stores every site once, so the traffic scales with the sites, not with the steps
+RESIDENT_DRAM_BYTES_PER_SITE = 317.9e6 / 512
+
+
 def measured_peak_hbm():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -151,6 +158,55 @@ def cpu_baseline(args, params, sites, budget_s):
     site_ms = sample * steps * params_dt_ms(params)
     return {"value": site_ms / dt, "unit": "site-ms/s", "cores": n_threads, "kind": "port",
             "sample": "%d of the workload's sites x %d time steps (CPU restatement, OpenMP over sites)" % (sample, steps)}
+
+
+def surrogate_report(sites=2048, sim_steps=20000, batches=8, train_steps=4000):
+    """Surrogate-gated versus plain-RD release sites on config-1 geometry: the
+    network is trained on the device from RD snapshots (frozen open sets), its
+    held-out mouth-Ca error is measured, then the same sites (same seeds, one
+    RyR opened) run 1 ms with RD gating and with surrogate gating (network
+    every 1 us, no RD step). Both arms are timed by wall clock around
+    synchronised device work."""
+    import torch
+    from scipy.stats import ks_2samp
+    import casim_b200 as cb
+    from casim_b200 import configs, surrogate as sg
+    Xs, Ys = [], []
+    for b in range(batches):
+        X, Y, _ = sg.rd_snapshots(4096, seed=100 + b)
+        Xs.append(X)
+        Ys.append(Y)
+    X, Y = np.concatenate(Xs), np.concatenate(Ys)
+    Xv, Yv, _ = sg.rd_snapshots(2048, seed=999)
+    net = sg.Surrogate(X.shape[1], Y.shape[1], seed=3)
+    sg.train(net, X, Y, train_steps, batch=8192, lr=2e-3)
+    rel = np.abs(10.0 ** sg.predict(net, Xv) - 10.0 ** Yv) / 10.0 ** Yv
+    p, s = configs.config1(n_sites=sites)
+    first = np.random.default_rng(5).integers(0, 20, size=sites).astype(np.int32)
+    out = {}
+    for mode in ("rd", "surrogate"):
+        sim = cb.ReleaseSiteBatch(p, s, precision="fp32", path="auto")
+        sim.start(first)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        if mode == "rd":
+            sim.step(sim_steps)
+        else:
+            sg.SurrogateGating(net, sim, window=20).step(sim_steps)
+        sim.synchronize()
+        el = time.time() - t0
+        out[mode] = (sites * sim_steps * sim.info.dt_ms / el, sim.all_states().reshape(sites, -1).sum(1),
+                     np.array([sim.release(k) for k in range(sites)]))
+        sim.close()
+    net.close()
+    return {"workload": "%d config-1 sites, 1 ms from one open RyR, fp32" % sites,
+            "rd_site_ms_per_s": out["rd"][0], "surrogate_site_ms_per_s": out["surrogate"][0],
+            "speedup": out["surrogate"][0] / out["rd"][0],
+            "held_out_mouth_rel_err_median": float(np.median(rel)), "held_out_mouth_rel_err_p90": float(np.percentile(rel, 90)),
+            "open_count_ks_p": float(ks_2samp(out["rd"][1], out["surrogate"][1]).pvalue),
+            "release_ks_p": float(ks_2samp(out["rd"][2], out["surrogate"][2]).pvalue),
+            "release_mean_ratio": float(out["surrogate"][2].mean() / out["rd"][2].mean()),
+            "training": "%d RD snapshots (0.25 ms relaxation), %d Adam steps of 8192 on the device" % (X.shape[0], train_steps)}
 
 
 def params_dt_ms(params):
@@ -288,9 +344,13 @@ def main():
         "gpu_launches": int(launches_per * args.steps),
         "finite": bool(ok_finite),
         "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                     "note": "achieved = algorithmic bytes (2 x field bytes per node-step) / device time; the resident "
-                             "path keeps fields on chip, so this is an effective bandwidth above the HBM traffic"},
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (RESIDENT_DRAM_BYTES_PER_SITE * sim.S
+                                 if sim.path == "resident" and args.precision == "fp32" and args.config == "c2" else None),
+                     "note": "achieved = algorithmic bytes (2 x field bytes per node-step) of one bench step / its device "
+                             "time; the resident path keeps fields on chip, so this is an effective bandwidth; traffic = "
+                             "ncu DRAM bytes of the launches of one bench step (0.62 MB per site per launch, measured "
+                             "on 512 sites of this workload and scaled by sites)"},
         "clocks": clk.summary(),
     }
     if not args.no_e2e:
@@ -311,6 +371,9 @@ def main():
             h2d = first.nbytes + jsr.nbytes
             d2h = mouth.nbytes + states.nbytes
         el = time.time() - t0
+        if dist:
+            from casim_b200 import dist as cdist
+            el = cdist.max_over_ranks(el, device="cuda")
         result["e2e"] = {"value": total_sites * args.chunk * n_e2e * dt_ms / el, "unit": "site-ms/s",
                          "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": n_e2e}
     if rank == 0 and not args.no_cpu_baseline:
@@ -318,6 +381,11 @@ def main():
             result["cpu_baseline"] = cpu_baseline(args, p, s, args.cpu_seconds)
         except Exception as e:  # the baseline is reported, never required
             result["cpu_baseline"] = {"error": str(e)}
+    if rank == 0 and world == 1 and not args.no_surrogate:
+        try:
+            result["surrogate"] = surrogate_report()
+        except Exception as e:  # reported next to the headline, never required
+            result["surrogate"] = {"error": str(e)}
     sim.close()
     if dist:
         dist.destroy_process_group()

@@ -235,7 +235,7 @@ bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* 
     std::vector<cb_site> sites(d.S);
     if (cudaMemcpy(sites.data(), d.sites, sizeof(cb_site) * d.S, cudaMemcpyDeviceToHost) != cudaSuccess) return no("cudaMemcpy");
     const int nz = layers_of(d.m, sites);
-    if (nz == 0) return no("3D clefts need 3 layers (the reference's z = 15 nm at dz = 5 nm)");
+    if (nz == 0) return no("the resident path is specialised for 3D clefts of 3 layers");
     std::vector<std::vector<int>> classes;
     std::vector<int> cs;
     if (!classify(d, sites, classes, cs)) return no("a site does not fit the shared memory of a 16-block cluster");
