@@ -40,7 +40,7 @@ EXPORTS = (
     "casim_b200_last_step_launches", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
     "casim_b200_rng_draws_static", "casim_b200_path_note",
     "casim_b200_set_all_states", "casim_b200_sg_features", "casim_b200_sg_set_mouth",
-    "casim_b200_sg_gate_steps", "casim_b200_sg_create", "casim_b200_sg_destroy", "casim_b200_sg_set_stream", "casim_b200_sg_num_params",
+    "casim_b200_sg_gate_steps", "casim_b200_sg_run", "casim_b200_sg_create", "casim_b200_sg_destroy", "casim_b200_sg_set_stream", "casim_b200_sg_num_params",
     "casim_b200_sg_get_params", "casim_b200_sg_set_params", "casim_b200_sg_forward", "casim_b200_sg_gradients",
     "casim_b200_sg_train_step", "casim_b200_sg_check", "casim_b200_sg_launches", "casim_b200_sg_last_error",
     "casim_b200_sg_gemm",
@@ -114,6 +114,7 @@ def lib():
         L.casim_b200_sg_features.argtypes = [vp, i32, i32, vp]
         L.casim_b200_sg_set_mouth.argtypes = [vp, vp, i32, ctypes.c_double]
         L.casim_b200_sg_gate_steps.argtypes = [vp, i64]
+        L.casim_b200_sg_run.argtypes = [vp, vp, i32, i64, i32, ctypes.c_double]
         L.casim_b200_last_step_ms.argtypes = [vp, dp]
         L.casim_b200_last_step_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.casim_b200_debug_rng.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]

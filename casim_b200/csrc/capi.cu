@@ -28,6 +28,12 @@ struct casim_b200_sim {
     long long last_launches = 0;
     std::vector<void*> allocs;
     std::string resident_why;  // how the resident path splits the batch, or why it was not chosen
+    // surrogate-driven gating: feature buffer and one captured window
+    float* sg_x = nullptr;
+    int sg_rows = 0, sg_ld = 0, sg_maxch = 0, sg_window = 0;
+    void* sg_net = nullptr;
+    const void* sg_out = nullptr;  // the network's output buffer when the window was captured
+    cudaGraphExec_t sg_exec = nullptr;
 };
 
 namespace {
@@ -260,6 +266,8 @@ casim_status casim_b200_destroy(casim_h h) {
     if (h->d.rs_counter) cudaFree(h->d.rs_counter);
     if (h->d.rs_pow2) cudaFree(h->d.rs_pow2);
     cb_resident_free(h->d);
+    if (h->sg_exec) cudaGraphExecDestroy(h->sg_exec);
+    if (h->sg_x) cudaFree(h->sg_x);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -539,6 +547,78 @@ casim_status casim_b200_sg_gate_steps(casim_h h, int64_t n) {
     if (n < 0) throw std::runtime_error("negative step count");
     if (h->d.m.cyto_type != CB_CYTO_POOL) throw std::runtime_error("surrogate gating needs the pool cytosol");
     if (n > 0) ck(cb_sg_steps(h->d, n, h->stream), "surrogate steps");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+namespace {
+
+// one surrogate window on h->stream: features, network, mouth values, `window` steps
+cudaError_t sg_window(casim_h h, casim_sg net, double ca_ref, int window) {
+    cudaError_t e = cb_sg_features(h->d, h->sg_maxch, h->sg_ld, h->sg_x, h->stream);
+    const float* y = nullptr;
+    int ld = 0;
+    if (e == cudaSuccess) e = cb_sg_net_forward(net, h->sg_x, h->sg_rows, h->stream, &y, &ld);
+    if (e == cudaSuccess) e = cb_sg_mouth(h->d, y, ld, ca_ref, h->stream);
+    if (e == cudaSuccess) e = cb_sg_steps(h->d, window, h->stream);
+    return e;
+}
+
+}  // namespace
+
+casim_status casim_b200_sg_run(casim_h h, casim_sg net, int32_t max_channels, int64_t n, int32_t window, double ca_ref) {
+    GUARD(h)
+    if (!net || n < 0 || window < 1 || !(ca_ref > 0) || max_channels < 1) throw std::runtime_error("bad surrogate run arguments");
+    if (h->d.m.cyto_type != CB_CYTO_POOL) throw std::runtime_error("surrogate gating needs the pool cytosol");
+    const int ld = 3 * max_channels + 1 + h->d.m.n_buf;
+    const int rows = (h->d.S + 127) / 128 * 128;
+    if (!h->sg_x || h->sg_rows != rows || h->sg_ld != ld) {
+        if (h->sg_x) cudaFree(h->sg_x);
+        h->sg_x = nullptr;
+        ck(cudaMalloc(&h->sg_x, sizeof(float) * (size_t)rows * ld), "cudaMalloc");
+        ck(cudaMemset(h->sg_x, 0, sizeof(float) * (size_t)rows * ld), "cudaMemset");
+        h->sg_rows = rows;
+        h->sg_ld = ld;
+    }
+    h->sg_maxch = max_channels;
+    ck(cb_sg_net_prepare(net, rows), "surrogate buffers");
+    if (h->sg_exec && (h->sg_net != (void*)net || h->sg_window != window || h->sg_out != cb_sg_net_output(net))) {
+        cudaGraphExecDestroy(h->sg_exec);
+        h->sg_exec = nullptr;
+    }
+    long long done = 0;
+    // the first full window runs eagerly (sets kernel attributes), then one
+    // window is captured into a graph and replayed
+    while (done < n) {
+        const int k = (int)std::min<long long>(window, n - done);
+        if (k == window && h->sg_exec) {
+            ck(cudaGraphLaunch(h->sg_exec, h->stream), "cudaGraphLaunch");
+        } else {
+            ck(sg_window(h, net, ca_ref, k), "surrogate window");
+            if (k == window && !h->sg_exec) {
+                cudaGraph_t g = nullptr;
+                ck(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+                const cudaError_t ew = sg_window(h, net, ca_ref, window);
+                const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+                ck(ew, "surrogate window capture");
+                ck(ec, "cudaStreamEndCapture");
+                const cudaError_t ei = cudaGraphInstantiate(&h->sg_exec, g, 0);
+                cudaGraphDestroy(g);
+                ck(ei, "cudaGraphInstantiate");
+                h->sg_net = (void*)net;
+                h->sg_window = window;
+                h->sg_out = cb_sg_net_output(net);
+            }
+        }
+        done += k;
+    }
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    const cudaError_t en = cb_sg_net_error(net);
+    if (en == cudaErrorLaunchTimeout) {
+        h->err = "a tensor-core wait of the surrogate network gave up";
+        return CASIM_ETIMEOUT;
+    }
+    ck(en, "surrogate network");
     return CASIM_OK;
     END_GUARD(h)
 }

@@ -60,6 +60,12 @@ cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* la
 cudaError_t cb_sg_features(cb_dev& d, int max_ch, int ld, float* X, cudaStream_t st);
 cudaError_t cb_sg_mouth(cb_dev& d, const float* Y, int ld, double ca_ref, cudaStream_t st);
 cudaError_t cb_sg_steps(cb_dev& d, long long n, cudaStream_t st);
+// the surrogate network (surrogate.cu)
+struct casim_surrogate_s;
+cudaError_t cb_sg_net_prepare(struct casim_surrogate_s* net, int batch);
+cudaError_t cb_sg_net_forward(struct casim_surrogate_s* net, const float* x, int batch, cudaStream_t st, const float** y, int* ld);
+cudaError_t cb_sg_net_error(struct casim_surrogate_s* net);
+const void* cb_sg_net_output(struct casim_surrogate_s* net);  // changes when its buffers are reallocated
 
 // resident path (resident.cu)
 bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* why);

@@ -59,6 +59,45 @@ CB_HD double u01d(State& g) {
     return (u < 1.0) ? u : (u - 1.0);
 }
 
+#ifdef __CUDACC__
+// The same recurrence with the modular products reduced by folding
+// (m = 2^32 - c: x = hi * 2^32 + lo == hi * c + lo), two folds and one
+// conditional subtraction instead of 64-bit remainders; bit-identical draws.
+template <uint64_t M>
+__device__ __forceinline__ uint64_t fold_mod(uint64_t x) {
+    constexpr uint64_t c = (1ULL << 32) - M;
+    uint64_t t = (x >> 32) * c + (x & 0xffffffffULL);
+    t = (t >> 32) * c + (t & 0xffffffffULL);
+    return t >= M ? t - M : t;
+}
+
+__device__ __forceinline__ double u01_fold(State& g) {
+    uint64_t a = fold_mod<M1>(A12 * g.s[1]);
+    uint64_t b = fold_mod<M1>(A13N * g.s[0]);
+    const uint64_t p1 = a >= b ? a - b : a + M1 - b;
+    g.s[0] = g.s[1];
+    g.s[1] = g.s[2];
+    g.s[2] = (uint32_t)p1;
+    a = fold_mod<M2>(A21 * g.s[5]);
+    b = fold_mod<M2>(A23N * g.s[3]);
+    const uint64_t p2 = a >= b ? a - b : a + M2 - b;
+    g.s[3] = g.s[4];
+    g.s[4] = g.s[5];
+    g.s[5] = (uint32_t)p2;
+    const double norm = 1.0 / (4294967087.0 + 1.0);
+    const double d1 = (double)p1, d2 = (double)p2;
+    return (p1 > p2) ? __dmul_rn(d1 - d2, norm) : __dmul_rn(__dadd_rn(d1 - d2, 4294967087.0), norm);
+}
+
+// u01d with the folding recurrence (CaSim/rngstream.cpp:271-283, incPrec)
+__device__ __forceinline__ double u01d_fold(State& g) {
+    double u = u01_fold(g);
+    const double v = u01_fold(g);
+    u = __dadd_rn(u, __dmul_rn(v, 5.9604644775390625e-8));
+    return (u < 1.0) ? u : (u - 1.0);
+}
+#endif
+
 // ---- host-side jump-ahead (3x3 matrix powers of the two recurrences) ----
 struct Mat3 {
     uint64_t a[3][3];

@@ -86,10 +86,10 @@ __global__ void k_init_open(const cb_site* __restrict__ sites, const int* __rest
     // CaSim/DyadChannels.cpp:83-95: one draw per channel (SetMacroState(0, .)),
     // then one more for the channel that is opened
     for (int c = 0; c < st.n_ch; ++c) {
-        (void)cbrng::u01d(g);
+        (void)cbrng::u01d_fold(g);
         ch_state[st.ch_off + c] = 0;
     }
-    (void)cbrng::u01d(g);
+    (void)cbrng::u01d_fold(g);
     int f = first[s - lo];
     if (f >= 0 && f < st.n_ch) ch_state[st.ch_off + f] = 1;
     q.draws += (unsigned long long)st.n_ch + 1;
@@ -168,8 +168,8 @@ __global__ void k_pre(cb_model m, int S, int NS, const cb_site* __restrict__ sit
         int state = ch_state[st.ch_off + c];
         double r = cb_rate(m, spx0, spc0, spx1, spc1, state, ca, mg);
         ++draws;
-        if (cbrng::u01d(g) < r * dt) {
-            (void)cbrng::u01d(g);
+        if (cbrng::u01d_fold(g) < r * dt) {
+            (void)cbrng::u01d_fold(g);
             ++draws;
             ch_state[st.ch_off + c] = 1 - state;
         }
@@ -507,18 +507,34 @@ __global__ void k_sg_steps(cb_model m, int S, int NS, long long n, const cb_site
     cbrng::State g;
     for (int i = 0; i < 6; ++i) g.s[i] = q.rng[i];
     unsigned long long draws = 0;
+    // the mouth values are held, so the transition probability of each state is
+    // fixed for the whole call: computed once for the first SG_CACHE RyRs
+    constexpr int SG_CACHE = 32;
+    double pc[2][SG_CACHE];
+    const int ncache = st.n_ch < SG_CACHE ? st.n_ch : SG_CACHE;
+    for (int c = 0; c < ncache; ++c) {
+        const double* mo = mouth + (long long)(st.ch_off + c) * NS;
+        const double ca = mo[m.ca_idx];
+        const double mg = m.mg_idx >= 0 ? mo[m.mg_idx] : 0.0;
+        pc[0][c] = cb_rate(m, spx0, spc0, spx1, spc1, 0, ca, mg) * dt;
+        pc[1][c] = cb_rate(m, spx0, spc0, spx1, spc1, 1, ca, mg) * dt;
+    }
     for (long long it = 0; it < n; ++it) {
         if (m.cyto_type == CB_CYTO_POOL) pool_step(m, q, dt);
         jsr_step(m, q, dt);
         for (int c = 0; c < st.n_ch; ++c) {
-            const double* mo = mouth + (long long)(st.ch_off + c) * NS;
-            const double ca = mo[m.ca_idx];
-            const double mg = m.mg_idx >= 0 ? mo[m.mg_idx] : 0.0;
             const int state = ch_state[st.ch_off + c];
-            const double r = cb_rate(m, spx0, spc0, spx1, spc1, state, ca, mg);
+            double p;
+            if (c < ncache) {
+                p = pc[state][c];
+            } else {
+                const double* mo = mouth + (long long)(st.ch_off + c) * NS;
+                const double mg = m.mg_idx >= 0 ? mo[m.mg_idx] : 0.0;
+                p = cb_rate(m, spx0, spc0, spx1, spc1, state, mo[m.ca_idx], mg) * dt;
+            }
             ++draws;
-            if (cbrng::u01d(g) < r * dt) {
-                (void)cbrng::u01d(g);
+            if (cbrng::u01d_fold(g) < p) {
+                (void)cbrng::u01d_fold(g);
                 ++draws;
                 ch_state[st.ch_off + c] = 1 - state;
             }

@@ -489,6 +489,29 @@ cudaError_t check_err(casim_sg h) {
 
 }  // namespace
 
+// Library-internal: network output for x [batch][n_in] enqueued on stream st
+// without any host synchronisation (capture-safe once cb_sg_net_prepare has
+// sized the buffers). The output stays in the handle: *y [batch][*ld].
+cudaError_t cb_sg_net_prepare(casim_sg h, int batch) {
+    if (!h || batch <= 0 || batch % BM) return cudaErrorInvalidValue;
+    return ensure_capacity(h, batch);
+}
+
+cudaError_t cb_sg_net_forward(casim_sg h, const float* x, int batch, cudaStream_t st, const float** y, int* ld) {
+    if (!h || batch > h->cap) return cudaErrorInvalidValue;
+    const cudaStream_t keep = h->stream;
+    h->stream = st;
+    const cudaError_t e = forward(h, x, batch, false);
+    h->stream = keep;
+    *y = h->Y;
+    *ld = h->out_pad;
+    return e;
+}
+
+cudaError_t cb_sg_net_error(casim_sg h) { return check_err(h); }
+
+const void* cb_sg_net_output(casim_sg h) { return h ? (const void*)h->Y : nullptr; }
+
 extern "C" {
 
 casim_status casim_b200_sg_create(int n_in, int n_out, int width, int depth, uint64_t seed, casim_sg* out) {

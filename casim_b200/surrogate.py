@@ -231,21 +231,11 @@ class SurrogateGating:
     mouth Ca instead of the RD step: every `window` time steps the network is
     evaluated on the features of the current open sets and jSR Ca and the mouth
     Ca replaced; in between, gating, the jSR and pool ODEs and the RyR currents
-    run on the device with the mouth values held (casim_b200_sg_gate_steps).
-    The batch, the network and torch each keep their own stream; every window
-    synchronises where one hands data to another."""
+    run with the mouth values held. The whole loop runs on the batch's stream
+    (casim_b200_sg_run, one captured window replayed as a CUDA graph)."""
 
     def __init__(self, net, sim, max_ch=20, window=20):
         self.net, self.sim, self.max_ch, self.window = net, sim, max_ch, window
 
     def step(self, n):
-        L = lib()
-        done = 0
-        while done < n:
-            k = min(self.window, n - done)
-            X = device_features(self.sim, self.max_ch)  # returns after the batch's stream is idle
-            Y = self.net.forward(X)                     # returns after the network's stream is idle
-            self.sim._ck(L.casim_b200_sg_set_mouth(self.sim.h, _ptr(Y), int(Y.shape[1]), CA_REF_UM))
-            self.sim._ck(L.casim_b200_sg_gate_steps(self.sim.h, k))
-            self.sim.synchronize()                      # Y may be reused once this returns
-            done += k
+        self.sim._ck(lib().casim_b200_sg_run(self.sim.h, self.net.h, self.max_ch, int(n), self.window, CA_REF_UM))

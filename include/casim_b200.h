@@ -234,6 +234,12 @@ casim_status casim_b200_sg_set_mouth(casim_h h, const float* y_dev, int32_t ld, 
  * ODEs, RyR gating (the draws of casim_b200_step) and RyR currents from the
  * mouth values held since casim_b200_sg_set_mouth. */
 casim_status casim_b200_sg_gate_steps(casim_h h, int64_t n);
+/* n surrogate-driven steps in windows of `window` steps, all on the batch's
+ * stream with no host round trip: features, network (ca_ref * 10^output as
+ * the mouth Ca of RyR slot c), casim_b200_sg_gate_steps(window). A full
+ * window is captured once into a CUDA graph and replayed. Returns after the
+ * stream is idle. A network handle serves one such call at a time. */
+casim_status casim_b200_sg_run(casim_h h, casim_sg net, int32_t max_channels, int64_t n, int32_t window, double ca_ref);
 /* One product C = A . B^T on the tensor cores: A [M][K] and B [N][K] BF16
  * (bit patterns), C [M][N] FP32, all device memory; M a multiple of 128,
  * N a multiple of 16 in [16, 256], K a multiple of 64. */
