@@ -60,6 +60,7 @@ cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* la
 cudaError_t cb_sg_features(cb_dev& d, int max_ch, int ld, float* X, cudaStream_t st);
 cudaError_t cb_sg_mouth(cb_dev& d, const float* Y, int ld, double ca_ref, cudaStream_t st);
 cudaError_t cb_sg_steps(cb_dev& d, long long n, cudaStream_t st);
+cudaError_t cb_sg_steps_warp(cb_dev& d, long long n, cudaStream_t st, bool* used);  // sg_gate.cu
 // the surrogate network (surrogate.cu)
 struct casim_surrogate_s;
 cudaError_t cb_sg_net_prepare(struct casim_surrogate_s* net, int batch);
@@ -71,3 +72,5 @@ const void* cb_sg_net_output(struct casim_surrogate_s* net);  // changes when it
 bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* why);
 cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);
 void cb_resident_free(cb_dev& d);
+// MRG32k3a jump table d.rs_pow2: A^(2^k), k < 64, then the ring-refill jump (resident.cu)
+cudaError_t cb_ensure_pow2(cb_dev& d);

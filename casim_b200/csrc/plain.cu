@@ -16,6 +16,7 @@
 #include "engine.h"
 #include "mrg32k3a.cuh"
 #include "physics.cuh"
+#include "pools.cuh"
 
 namespace {
 
@@ -96,58 +97,6 @@ __global__ void k_init_open(const cb_site* __restrict__ sites, const int* __rest
     for (int i = 0; i < 6; ++i) q.rng[i] = g.s[i];
 }
 
-// Cytosol pool ODE of one site (CaSim/CytosolPool.cpp:217-288).
-__device__ void pool_step(const cb_model& m, cb_site_scalars& q, double dt) {
-    double evo_i[CB_MAX_IONS], evo_p[CB_MAX_CPAIRS];
-    int ipd = 0, is = 0;
-    for (int j = 0; j < m.n_ions; ++j) {
-        double react = 0;
-        for (int p = 0; p < m.c_n_pairs; ++p) {
-            if (m.c_pair_ion[p] != j) continue;
-            double R1 = m.c_koff[p] * q.c_pairs[p] - m.c_kon[p] * q.c_ions[j] * q.c_free[m.c_pair_buf[p]];
-            evo_p[p] = -R1;
-            react += R1;
-            if (m.c_in_dyad[p]) {
-                evo_p[p] += q.efflux[m.n_ions + ipd];
-                ++ipd;
-            }
-        }
-        evo_i[j] = react + q.efflux[j];
-        if (m.c_serca[j]) {
-            double i2 = q.c_ions[j] * q.c_ions[j];
-            double K2 = m.c_Kup[is] * m.c_Kup[is];
-            double b2 = m.c_bg[is] * m.c_bg[is];
-            evo_i[j] -= m.c_Jmax[is] * (i2 / (i2 + K2) - b2 / (b2 + K2));
-            ++is;
-        }
-    }
-    for (int j = 0; j < m.n_ions; ++j) {
-        evo_i[j] -= m.c_onetau_ion[j] * (q.c_ions[j] - m.c_bg[j]);
-        q.c_ions[j] += evo_i[j] * dt;
-    }
-    ipd = 0;
-    for (int p = 0; p < m.c_n_pairs; ++p) {
-        evo_p[p] -= m.c_onetau_pair[p] * (q.c_pairs[p] - m.c_init[p]);
-        q.c_pairs[p] += evo_p[p] * dt;
-        if (m.c_in_dyad[p]) q.c_bnd[ipd++] = q.c_pairs[p];
-    }
-    for (int b = 0; b < m.c_n_buf; ++b) q.c_free[b] = m.c_Ctot[b];
-    for (int p = 0; p < m.c_n_pairs; ++p) q.c_free[m.c_pair_buf[p]] -= q.c_pairs[p];
-}
-
-// jSR pool ODE of one site (CaSim/SRPool.cpp:70-89) with the site's own beta.
-__device__ __forceinline__ void jsr_step(const cb_model& m, cb_site_scalars& q, double dt) {
-    if (m.jsr_const) return;
-    double beta = 1;
-    for (int j = 0; j < m.n_ions; ++j)
-        beta += m.nCQ[j] * m.K_CQ[j] * m.CQ / ((m.K_CQ[j] + q.jsr[j]) * (m.K_CQ[j] + q.jsr[j]));
-    for (int i = 0; i < m.n_ions; ++i) {
-        double Iref = 1 / m.tau_refill[i] * (q.nsr[i] - q.jsr[i]);
-        q.jsr_new[i] = q.jsr[i] + dt / beta * (Iref - q.IjSR[i] / m.V_jsr);
-    }
-    if (m.ca_idx >= 0) q.release += q.IjSR[m.ca_idx] * dt;
-}
-
 __global__ void k_pre(cb_model m, int S, int NS, const cb_site* __restrict__ sites, cb_site_scalars* __restrict__ sc,
                       int* __restrict__ ch_state, const double* __restrict__ mouth, const double* __restrict__ spx0,
                       const double* __restrict__ spc0, const double* __restrict__ spx1, const double* __restrict__ spc1) {
@@ -156,8 +105,8 @@ __global__ void k_pre(cb_model m, int S, int NS, const cb_site* __restrict__ sit
     const cb_site st = sites[s];
     cb_site_scalars& q = sc[s];
     const double dt = m.dt;
-    if (m.cyto_type == CB_CYTO_POOL) pool_step(m, q, dt);
-    jsr_step(m, q, dt);
+    if (m.cyto_type == CB_CYTO_POOL) cb_pool_step(m, q, dt);
+    cb_jsr_step(m, q, dt);
     cbrng::State g;
     for (int i = 0; i < 6; ++i) g.s[i] = q.rng[i];
     unsigned long long draws = 0;
@@ -520,8 +469,8 @@ __global__ void k_sg_steps(cb_model m, int S, int NS, long long n, const cb_site
         pc[1][c] = cb_rate(m, spx0, spc0, spx1, spc1, 1, ca, mg) * dt;
     }
     for (long long it = 0; it < n; ++it) {
-        if (m.cyto_type == CB_CYTO_POOL) pool_step(m, q, dt);
-        jsr_step(m, q, dt);
+        if (m.cyto_type == CB_CYTO_POOL) cb_pool_step(m, q, dt);
+        cb_jsr_step(m, q, dt);
         for (int c = 0; c < st.n_ch; ++c) {
             const int state = ch_state[st.ch_off + c];
             double p;
@@ -610,6 +559,9 @@ cudaError_t cb_sg_mouth(cb_dev& d, const float* Y, int ld, double ca_ref, cudaSt
 }
 
 cudaError_t cb_sg_steps(cb_dev& d, long long n, cudaStream_t st) {
+    bool used = false;
+    cudaError_t e = cb_sg_steps_warp(d, n, st, &used);
+    if (e != cudaSuccess || used) return e;
     k_sg_steps<<<(d.S + 127) / 128, 128, 0, st>>>(d.m, d.S, d.NS, n, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0],
                                                   d.spx[1], d.spc[1]);
     return cudaGetLastError();

@@ -129,8 +129,8 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
     off = align16(off + (size_t)maxch * 4);
     a.off_ftab = (int)off;
     off = align16(off + (size_t)(maxch + 1) * NI * rs);
-    a.off_mi = (int)off;
-    off = align16(off + (size_t)2 * maxch * NI * 8);
+    a.off_pg = (int)off;
+    off = align16(off + (size_t)2 * maxch * 8);
     a.off_ring = (int)off;
     off = align16(off + (size_t)RING * 8);
     a.off_redw = (int)off;
@@ -268,6 +268,42 @@ bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* 
     return true;
 }
 
+// MRG32k3a jump table of the batch (resident gating and surrogate gating)
+cudaError_t cb_ensure_pow2(cb_dev& d) {
+    if (d.rs_pow2) return cudaSuccess;
+    cudaError_t e;
+    // MRG32k3a: A^(2^k) for k < 64 (both components), then the refill jump A^(2*31*LANE_DRAWS)
+    std::vector<unsigned long long> p2(65 * 18);
+    cbrng::Mat3 a1 = cbrng::step_matrix1(), a2 = cbrng::step_matrix2();
+    for (int k = 0; k < 64; ++k) {
+        for (int i = 0; i < 9; ++i) {
+            p2[18 * k + i] = a1.a[i / 3][i % 3];
+            p2[18 * k + 9 + i] = a2.a[i / 3][i % 3];
+        }
+        a1 = cbrng::matmul(a1, a1, cbrng::M1);
+        a2 = cbrng::matmul(a2, a2, cbrng::M2);
+    }
+    cbrng::Mat3 j1{{{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}}, j2 = j1;
+    unsigned long long steps = 2ULL * 31 * LANE_DRAWS;
+    for (int k = 0; steps; ++k, steps >>= 1)
+        if (steps & 1ULL) {
+            cbrng::Mat3 b1, b2;
+            for (int i = 0; i < 9; ++i) {
+                b1.a[i / 3][i % 3] = p2[18 * k + i];
+                b2.a[i / 3][i % 3] = p2[18 * k + 9 + i];
+            }
+            j1 = cbrng::matmul(b1, j1, cbrng::M1);
+            j2 = cbrng::matmul(b2, j2, cbrng::M2);
+        }
+    for (int i = 0; i < 9; ++i) {
+        p2[18 * JUMP_ROW + i] = j1.a[i / 3][i % 3];
+        p2[18 * JUMP_ROW + 9 + i] = j2.a[i / 3][i % 3];
+    }
+    if ((e = cudaMalloc(&d.rs_pow2, sizeof(unsigned long long) * p2.size())) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(d.rs_pow2, p2.data(), sizeof(unsigned long long) * p2.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
 // launch plan of a batch, built on the first step and reused: one entry per
 // cluster-size class with its static arguments, block size and resident clusters
 struct cb_rs_plan {
@@ -298,35 +334,7 @@ cudaError_t build_plan(cb_dev& d) {
     if ((e = cudaMalloc(&d.rs_order, sizeof(int) * d.S)) != cudaSuccess) return e;
     if ((e = cudaMemcpy(d.rs_order, order.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&d.rs_counter, sizeof(int) * 8)) != cudaSuccess) return e;
-    // MRG32k3a: A^(2^k) for k < 64 (both components), then the refill jump A^(2*31*LANE_DRAWS)
-    std::vector<unsigned long long> p2(65 * 18);
-    cbrng::Mat3 a1 = cbrng::step_matrix1(), a2 = cbrng::step_matrix2();
-    for (int k = 0; k < 64; ++k) {
-        for (int i = 0; i < 9; ++i) {
-            p2[18 * k + i] = a1.a[i / 3][i % 3];
-            p2[18 * k + 9 + i] = a2.a[i / 3][i % 3];
-        }
-        a1 = cbrng::matmul(a1, a1, cbrng::M1);
-        a2 = cbrng::matmul(a2, a2, cbrng::M2);
-    }
-    cbrng::Mat3 j1{{{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}}, j2 = j1;
-    unsigned long long steps = 2ULL * 31 * LANE_DRAWS;
-    for (int k = 0; steps; ++k, steps >>= 1)
-        if (steps & 1ULL) {
-            cbrng::Mat3 b1, b2;
-            for (int i = 0; i < 9; ++i) {
-                b1.a[i / 3][i % 3] = p2[18 * k + i];
-                b2.a[i / 3][i % 3] = p2[18 * k + 9 + i];
-            }
-            j1 = cbrng::matmul(b1, j1, cbrng::M1);
-            j2 = cbrng::matmul(b2, j2, cbrng::M2);
-        }
-    for (int i = 0; i < 9; ++i) {
-        p2[18 * JUMP_ROW + i] = j1.a[i / 3][i % 3];
-        p2[18 * JUMP_ROW + 9 + i] = j2.a[i / 3][i % 3];
-    }
-    if ((e = cudaMalloc(&d.rs_pow2, sizeof(unsigned long long) * p2.size())) != cudaSuccess) return e;
-    if ((e = cudaMemcpy(d.rs_pow2, p2.data(), sizeof(unsigned long long) * p2.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    if ((e = cb_ensure_pow2(d)) != cudaSuccess) return e;
     cb_rs_plan* P = new cb_rs_plan();
     P->nz = nz;
     int offset = 0;

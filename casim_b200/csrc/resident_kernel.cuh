@@ -80,6 +80,19 @@ struct rs_const {
 __device__ __forceinline__ float div_fast(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ double div_fast(double a, double b) { return a / b; }
 
+// division by a per-site constant d >= 1 as a multiply-high and a shift
+// (round-up reciprocal m = floor(2^32 (2^s - d) / d) + 1, s = ceil(log2 d));
+// exact for 0 <= n < 2^31
+struct fastdiv {
+    unsigned m, s;
+};
+__device__ __forceinline__ fastdiv make_fastdiv(unsigned d) {
+    unsigned s = 0;
+    while ((1u << s) < d) ++s;
+    return {(unsigned)(((1ull << 32) * ((1ull << s) - d)) / d + 1), s};
+}
+__device__ __forceinline__ int fdiv(int n, fastdiv f) { return (int)((__umulhi((unsigned)n, f.m) + (unsigned)n) >> f.s); }
+
 template <bool B>
 struct bconst {
     static constexpr bool value = B;
@@ -117,44 +130,12 @@ struct rs_args {
     int cap_cleft;  // stored cleft nodes per species per rank
     int cap_cyto;   // stored cytosol nodes per species per rank
     int max_ch, max_terms, max_rim, FD;
-    int off_fb, off_ca, off_cb, off_chidx, off_chn, off_chs, off_cho, off_chr, off_ftab, off_mi, off_ring, off_redw,
+    int off_fb, off_ca, off_cb, off_chidx, off_chn, off_chs, off_cho, off_chr, off_ftab, off_pg, off_ring, off_redw,
         off_rede, off_redt, off_terms, off_crim, off_dptr, off_dterm, off_sc, smem_bytes;
 };
 
-// ---- MRG32k3a arithmetic by folding: m1 = 2^32 - 209, m2 = 2^32 - 22853 ----
-template <unsigned long long M>
-__device__ __forceinline__ unsigned long long fold_mod(unsigned long long x) {
-    constexpr unsigned long long c = (1ULL << 32) - M;
-    unsigned long long t = (x >> 32) * c + (x & 0xffffffffULL);
-    t = (t >> 32) * c + (t & 0xffffffffULL);
-    return t >= M ? t - M : t;
-}
-
-__device__ __forceinline__ double u01_fast(cbrng::State& g) {
-    unsigned long long a = fold_mod<cbrng::M1>(cbrng::A12 * g.s[1]);
-    unsigned long long b = fold_mod<cbrng::M1>(cbrng::A13N * g.s[0]);
-    const unsigned long long p1 = a >= b ? a - b : a + cbrng::M1 - b;
-    g.s[0] = g.s[1];
-    g.s[1] = g.s[2];
-    g.s[2] = (unsigned int)p1;
-    a = fold_mod<cbrng::M2>(cbrng::A21 * g.s[5]);
-    b = fold_mod<cbrng::M2>(cbrng::A23N * g.s[3]);
-    const unsigned long long p2 = a >= b ? a - b : a + cbrng::M2 - b;
-    g.s[3] = g.s[4];
-    g.s[4] = g.s[5];
-    g.s[5] = (unsigned int)p2;
-    const double norm = 1.0 / (4294967087.0 + 1.0);
-    const double d1 = (double)p1, d2 = (double)p2;
-    return (p1 > p2) ? __dmul_rn(d1 - d2, norm) : __dmul_rn(__dadd_rn(d1 - d2, 4294967087.0), norm);
-}
-
-// RandU01 with incPrec (CaSim/rngstream.cpp:271-283), no FMA contraction
-__device__ __forceinline__ double u01d_fast(cbrng::State& g) {
-    double u = u01_fast(g);
-    const double v = u01_fast(g);
-    u = __dadd_rn(u, __dmul_rn(v, 5.9604644775390625e-8));
-    return (u < 1.0) ? u : (u - 1.0);
-}
+using cbrng::fold_mod;
+__device__ __forceinline__ double u01d_fast(cbrng::State& g) { return cbrng::u01d_fold(g); }
 
 template <unsigned long long M>
 __device__ __forceinline__ void mat_apply(const unsigned long long* A, unsigned int* v) {
@@ -242,7 +223,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     int* cho = (int*)(smem + a.off_cho);   // site node (x + nx*(y + ny*z)) | owner flag in bit 30
     int* chr = (int*)(smem + a.off_chr);   // rim index of own RyRs on the rim, -1 otherwise
     R* ftab = (R*)(smem + a.off_ftab);     // [(1 + max_ch)][NI]: RyR currents, slot 0 is zero
-    double* mi = (double*)(smem + a.off_mi);      // [2][max_ch][NI]
+    double* pg = (double*)(smem + a.off_pg);      // [2][max_ch] transition probability of each RyR at the next gating
     double* ring = (double*)(smem + a.off_ring);
     double* redw = (double*)(smem + a.off_redw);  // [MAX_WARPS][F + NI]
     double* rede = (double*)(smem + a.off_rede);  // [2][C][F]
@@ -325,7 +306,8 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             chn[c] = ln;
             chr[c] = (x == 0 || y == 0 || x == nx - 1 || y == ny - 1) ? cb_rim_index(x, y, nx, ny) : -1;
             const double* mo = a.mouth + (size_t)(st.ch_off + c) * a.NS;
-            for (int j = 0; j < NI; ++j) mi[(a.max_ch + c) * NI + j] = mo[j];  // parity-1 slot
+            pg[a.max_ch + c] = cb_rate(m, a.spx0, a.spc0, a.spx1, a.spc1, chs[c], mo[m.ca_idx], m.mg_idx >= 0 ? mo[m.mg_idx] : 0.0) *
+                               m.dt;  // parity-1 slot
             if (own) {
                 if (owner) chidx[ln] = (unsigned short)(1 + c);
                 for (int j = 0; j < NI; ++j) {
@@ -378,6 +360,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             }
         }
         const int PL = npr > 0 ? (npr + PC - 1) / PC : 1;
+        const fastdiv fd_nxi = make_fastdiv(max(nxi, 1)), fd_ncol = make_fastdiv(max(ncol, 1)), fd_ni = make_fastdiv(max(ni, 1));
         cluster_barrier<C>();
 
         // ---------------------------------------------------------- steps
@@ -399,7 +382,8 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     if (lane == 0) s_we = we + WINDOW;
                 }
                 __syncwarp();
-                const double* mprev = mi + prv * a.max_ch * NI;
+                // probabilities of the previous Update's mouth values, computed in its phase B
+                const double* pprev = pg + prv * a.max_ch;
                 for (int base = 0; base < nch; base += 32) {
                     const int c = base + lane;
                     const int cnt = min(32, nch - base);
@@ -408,9 +392,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     int stt = 0;
                     if (act) {
                         stt = chs[c];
-                        const double cam = mprev[c * NI + m.ca_idx];
-                        const double mgm = m.mg_idx >= 0 ? mprev[c * NI + m.mg_idx] : 0.0;
-                        p = cb_rate(m, a.spx0, a.spc0, a.spx1, a.spc1, stt, cam, mgm) * dt;
+                        p = pprev[c];
                     }
                     int start = 0;
                     while (start < cnt) {
@@ -507,7 +489,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 // constants are kernel-parameter operands.
                 const int wk = warp - 2;
                 for (int t = wk * 32 + lane; t < nxi * nchunk; t += NW * 32) {
-                    const int ch = t / nxi;
+                    const int ch = fdiv(t, fd_nxi);
                     const int x = 1 + (t - ch * nxi);
                     const int y0 = ylo + ch * RS, y1 = min(y0 + RS, yhi);
                     // previous / current / next row of every species and layer
@@ -603,10 +585,11 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     // planes; all CSM species slots are stepped (unused slots are zero)
                     const int wt = tid - 64;
                     for (int t = wt; t < ncol * PC; t += NWT) {
-                        const int pc = t / ncol, col = t - pc * ncol;
+                        const int pc = fdiv(t, fd_ncol), col = t - pc * ncol;
                         const int k0 = plo + pc * PL, k1 = min(k0 + PL, phi);
                         if (k0 >= k1) continue;
-                        const int jj = 1 + col / ni, ii = 1 + (col - (col / ni) * ni);
+                        const int jq = fdiv(col, fd_ni);
+                        const int jj = 1 + jq, ii = 1 + (col - jq * ni);
                         const int cn = ii + mc * jj;
                         R uP[CSM], uC[CSM], uN[CSM];
 #pragma unroll
@@ -790,24 +773,31 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 }
             }
             // mouth gather and RyR currents of own channels (CaSim/DyadRD2DCPU.cpp:243-264, 361-380),
-            // channels from the last thread down so they meet the warps with fewer rim lines
+            // channels from the last thread down so they meet the warps with fewer rim lines; the
+            // transition probability of the next gating (CaSim/DyadChannels.cpp:97-130: rate of the
+            // current state at the mouth values x dt) is computed here, off the gating warp
             double tpart[NI];
 #pragma unroll
             for (int j = 0; j < NI; ++j) tpart[j] = 0;
             const int ct = blockDim.x - 1 - tid;
             const bool did_t = (W - 1 - warp) * 32 < nch;
-            double* mcur = mi + par * a.max_ch * NI;
+            double* pcur = pg + par * a.max_ch;
             for (int c = ct; c < nch; c += blockDim.x) {
                 const int n = chn[c];
                 if (n < 0) continue;
                 const int ri = chr[c];
                 const R* src = ri >= 0 ? fa : fb;  // the mouth is gathered before the rim is reset
                 const int stc = chs[c];
+                {
+                    const double cam = (double)src[m.ca_idx * cap + n];
+                    const double mgm = m.mg_idx >= 0 ? (double)src[m.mg_idx * cap + n] : 0.0;
+                    const double p = cb_rate(m, a.spx0, a.spc0, a.spx1, a.spc1, stc, cam, mgm) * dt;
+#pragma unroll 1
+                    for (int r = 0; r < C; ++r) peer<C>(pcur, r)[c] = p;
+                }
 #pragma unroll
                 for (int j = 0; j < NI; ++j) {
                     const double mv = (double)src[j * cap + n];
-#pragma unroll 1
-                    for (int r = 0; r < C; ++r) peer<C>(mcur, r)[c * NI + j] = mv;
                     const double cv = ri >= 0 ? (double)rim_value(j, ri) : mv;
                     const double fl = stc * (m.g[j] * (q.jsr_new[j] - cv));
                     ftab[(1 + c) * NI + j] = (R)fl;

@@ -147,3 +147,36 @@ def test_surrogate_gating_tracks_rd_open_counts_faster(cuda_device):
     (t_rd, n_rd), (t_sg, n_sg) = res["rd"], res["surrogate"]
     assert abs(n_sg - n_rd) <= 0.15 * n_rd, (n_rd, n_sg)
     assert t_sg < t_rd, (t_rd, t_sg)
+
+
+def test_warp_gating_matches_one_thread_gating(cuda_device):
+    """Surrogate-driven gating runs one warp per site while every site has at
+    most 256 RyRs and one thread per site otherwise; both consume each site's
+    MRG32k3a stream in the reference's order, so the same sites under the same
+    held mouth Ca follow identical RyR trajectories and draw counts."""
+    import ctypes
+    import torch
+    import casim_b200 as cb
+    from casim_b200 import configs
+    p, s = configs.config1(n_sites=8)
+    rng = np.random.default_rng(4)
+    xs, ys = configs.lattice(300, 63 * 5.0, 63 * 5.0, rng, jitter=0.0)
+    big = {k: (np.concatenate([v, v[:1]]) if isinstance(v, np.ndarray) and v.shape[:1] == (8,) else v) for k, v in s.items()}
+    big["n_ch"] = np.concatenate([s["n_ch"], [300]]).astype(np.int32)
+    big["ch_x"] = np.concatenate([s["ch_x"], xs])
+    big["ch_y"] = np.concatenate([s["ch_y"], ys])
+    big["first_channel"] = np.concatenate([s["first_channel"], [0]]).astype(np.int32)
+    y = torch.from_numpy(rng.uniform(1.0, 2.5, size=(128, 300)).astype(np.float32)).cuda()
+    out = []
+    for table in (s, big):
+        sim = cb.ReleaseSiteBatch(p, table, precision="fp32", path="plain")
+        sim.start(table["first_channel"])
+        sim._ck(cb.lib().casim_b200_sg_set_mouth(sim.h, ctypes.c_void_p(y.data_ptr()), 300, 1.0))
+        sim._ck(cb.lib().casim_b200_sg_gate_steps(sim.h, 4000))
+        sim.synchronize()
+        st = sim.all_states()[:160].reshape(8, 20)
+        out.append((st, [sim.draws(k) for k in range(8)]))
+        sim.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
+    assert sum(out[0][1]) > 8 * 20 * 4000  # transitions happened
