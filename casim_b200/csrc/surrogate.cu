@@ -41,6 +41,7 @@ struct gemm_args {
     const bf16* A;  // [M][K]
     const bf16* B;  // [N][K]
     int M, N, K;
+    int BN;         // columns per CTA (grid.y = N / BN)
     int mode;
     const float* bias;  // [N]
     float* C;           // [M][N] FP32 (EPI_OUT, EPI_PLAIN)
@@ -98,15 +99,15 @@ __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
 }
 
 // one K slice of A (rows m0..m0+127) and B (rows 0..N-1) into a stage, canonical layout
-__device__ __forceinline__ void load_stage(const gemm_args& g, int m0, int k0, uint32_t sa, uint32_t sb) {
+__device__ __forceinline__ void load_stage(const gemm_args& g, int m0, int n0, int k0, uint32_t sa, uint32_t sb) {
     const int tid = threadIdx.x;
     for (int p = tid; p < BM * (BK / 8); p += THREADS) {
         const int r = p >> 3, kk = p & 7;
         cp_async16(sa + (r >> 3) * SBO + kk * LBO + (r & 7) * 16, g.A + (size_t)(m0 + r) * g.K + k0 + kk * 8);
     }
-    for (int p = tid; p < g.N * (BK / 8); p += THREADS) {
+    for (int p = tid; p < g.BN * (BK / 8); p += THREADS) {
         const int r = p >> 3, kk = p & 7;
-        cp_async16(sb + (r >> 3) * SBO + kk * LBO + (r & 7) * 16, g.B + (size_t)r * g.K + k0 + kk * 8);
+        cp_async16(sb + (r >> 3) * SBO + kk * LBO + (r & 7) * 16, g.B + (size_t)(n0 + r) * g.K + k0 + kk * 8);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
@@ -116,17 +117,17 @@ __device__ __forceinline__ float gelu_grad(float z) {
     return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
-// C = A . B^T with the epilogue g.mode; grid.x = M / 128, N <= 256 and a multiple of 16,
-// K a multiple of 64; dynamic shared memory 2 * (16 KiB + N * 128 B)
+// C = A . B^T with the epilogue g.mode; grid (M / 128, N / BN), BN <= 256 and a multiple
+// of 16, K a multiple of 64; dynamic shared memory 2 * (16 KiB + BN * 128 B)
 __global__ void __launch_bounds__(THREADS, 1) k_gemm(const __grid_constant__ gemm_args g) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ uint32_t s_tmem;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * BM;
-    const int ncols = g.N <= 32 ? 32 : g.N <= 64 ? 64 : g.N <= 128 ? 128 : 256;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * g.BN;
+    const int ncols = g.BN <= 32 ? 32 : g.BN <= 64 ? 64 : g.BN <= 128 ? 128 : 256;
     const uint32_t sbase = smem_u32(smem);
-    const uint32_t b_stage = (uint32_t)g.N * (BK / 8) * 16;
+    const uint32_t b_stage = (uint32_t)g.BN * (BK / 8) * 16;
     const uint32_t sa[2] = {sbase, sbase + A_STAGE + b_stage};
     const uint32_t sb[2] = {sbase + A_STAGE, sbase + 2 * A_STAGE + b_stage};
 
@@ -143,11 +144,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm(const __grid_constant__ gem
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    const uint32_t idesc = idesc_bf16(g.N);
+    const uint32_t idesc = idesc_bf16(g.BN);
     const int kt = g.K / BK;
     bool ok = true;
 
-    load_stage(g, m0, 0, sa[0], sb[0]);
+    load_stage(g, m0, n0, 0, sa[0], sb[0]);
     for (int i = 0; i < kt; ++i) {
         const int s = i & 1;
         asm volatile("cp.async.wait_all;" ::: "memory");
@@ -163,7 +164,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm(const __grid_constant__ gem
         if (i + 1 < kt) {
             const int s2 = (i + 1) & 1;
             if (i >= 1) ok = mbar_wait(&bars[s2], (uint32_t)(((i - 1) >> 1) & 1)) && ok;  // slice i-1 consumed
-            load_stage(g, m0, (i + 1) * BK, sa[s2], sb[s2]);
+            load_stage(g, m0, n0, (i + 1) * BK, sa[s2], sb[s2]);
         }
     }
     ok = mbar_wait(&bars[(kt - 1) & 1], (uint32_t)(((kt - 1) >> 1) & 1)) && ok;
@@ -173,7 +174,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm(const __grid_constant__ gem
     // epilogue: warp w reads TMEM lanes 32w..32w+31 = rows m0 + 32w + lane
     const int row = m0 + warp * 32 + lane;
     const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-    for (int c0 = 0; c0 < g.N; c0 += 8) {
+    for (int c0 = 0; c0 < g.BN; c0 += 8) {
         uint32_t r[8];
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
@@ -183,20 +184,21 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm(const __grid_constant__ gem
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[j] = __uint_as_float(r[j]);
         if (!ok) continue;
-        const size_t o = (size_t)row * g.N + c0;
+        const int cg = n0 + c0;  // global column
+        const size_t o = (size_t)row * g.N + cg;
         if (g.mode == EPI_PLAIN) {
 #pragma unroll
             for (int j = 0; j < 8; ++j) g.C[o + j] = v[j];
         } else if (g.mode == EPI_OUT) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) g.C[o + j] = v[j] + g.bias[c0 + j];
+            for (int j = 0; j < 8; ++j) g.C[o + j] = v[j] + g.bias[cg + j];
         } else {
             __align__(16) bf16 h[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 float y;
                 if (g.mode == EPI_HIDDEN) {
-                    const float z = v[j] + g.bias[c0 + j];
+                    const float z = v[j] + g.bias[cg + j];
                     if (g.Z) g.Z[o + j] = z;
                     y = gelu(z);
                 } else {  // EPI_BACK: gradient w.r.t. the pre-activation
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm(const __grid_constant__ gem
             *(uint4*)(g.H + o) = *(const uint4*)h;
             if (g.HT)
 #pragma unroll
-                for (int j = 0; j < 8; ++j) g.HT[(size_t)(c0 + j) * g.M + row] = h[j];
+                for (int j = 0; j < 8; ++j) g.HT[(size_t)(cg + j) * g.M + row] = h[j];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -351,15 +353,25 @@ size_t gemm_smem(int N) {
     return s < 65536 ? 65536 : s;
 }
 
-cudaError_t gemm(casim_sg h, const gemm_args& g) {
-    const size_t sm = gemm_smem(g.N);
+// columns per CTA: all of N up to 128, else the widest of 128, 64, 32, 16 dividing N,
+// so that small batches still spread over twice the CTAs
+int tile_n(int N) {
+    if (N <= 128) return N;
+    for (int b : {128, 64, 32, 16})
+        if (N % b == 0) return b;
+    return 16;
+}
+
+cudaError_t gemm(casim_sg h, gemm_args g) {
     if (g.M % BM || g.K % BK || g.N % 16 || g.N > 256 || g.N < 16) return cudaErrorInvalidValue;
+    g.BN = tile_n(g.N);
+    const size_t sm = gemm_smem(g.BN);
     if (sm > h->smem_max) {
         cudaError_t e = cudaFuncSetAttribute(k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
         h->smem_max = sm;
     }
-    k_gemm<<<g.M / BM, THREADS, sm, h->stream>>>(g);
+    k_gemm<<<dim3(g.M / BM, g.N / g.BN), THREADS, sm, h->stream>>>(g);
     h->launches++;
     return cudaGetLastError();
 }
