@@ -139,6 +139,48 @@ def grid_index(coord, h):
     return int((coord + 0.5 * h) / h)
 
 
+def natural_spline(x, y):
+    """Natural cubic spline (zero second derivative at both ends) through (x, y):
+    per interval [a, b, c, d] with y(x_i + h) = a + b h + c h^2 + d h^3, from the
+    tridiagonal system for c_i = y''(x_i) / 2; plus the value, slope and c at the
+    last knot for extrapolation."""
+    x = np.asarray(x, np.float64)
+    y = np.asarray(y, np.float64)
+    n = len(x)
+    h = np.diff(x)
+    A = np.zeros((n, n))
+    r = np.zeros(n)
+    A[0, 0] = A[n - 1, n - 1] = 2.0
+    for i in range(1, n - 1):
+        A[i, i - 1] = h[i - 1] / 3.0
+        A[i, i] = 2.0 * (h[i - 1] + h[i]) / 3.0
+        A[i, i + 1] = h[i] / 3.0
+        r[i] = (y[i + 1] - y[i]) / h[i] - (y[i] - y[i - 1]) / h[i - 1]
+    c = np.linalg.solve(A, r)
+    b = np.zeros(n)
+    d = np.zeros(n)
+    for i in range(n - 1):
+        d[i] = (c[i + 1] - c[i]) / (3.0 * h[i])
+        b[i] = (y[i + 1] - y[i]) / h[i] - h[i] * (2.0 * c[i] + c[i + 1]) / 3.0
+    hl = h[-1]
+    b[n - 1] = 3.0 * d[n - 2] * hl * hl + 2.0 * c[n - 2] * hl + b[n - 2]
+    return np.c_[y, b, c, d], (y[0], b[0], 0.0), (y[n - 1], b[n - 1], 0.0)
+
+
+def _set_spline(m, w, x, y):
+    if len(x) > MAX_SPLINE:
+        raise ValueError("spline table longer than the oracle holds")
+    coef, left, right = natural_spline(x, y)
+    m.sp_n[w] = len(x)
+    for i in range(len(x)):
+        m.sp_x[w][i] = x[i]
+        for k in range(4):
+            m.sp_c[w][i][k] = coef[i, k]
+    for k in range(3):
+        m.sp_left[w][k] = left[k]
+        m.sp_right[w][k] = right[k]
+
+
 def build_model(params):
     d = params["Dyad"]
     m = OrModel()
@@ -197,6 +239,14 @@ def build_model(params):
     elif model == "TwoStateaHTG":
         m.ch_model = TWO_STATE_AHTG
         vals = [par[k] for k in ("fCa", "KCa", "fMg", "KMg", "KO0", "KMgI", "KCL", "KI", "KOL", "kclose")]
+    elif model == "TwoStateSpline":
+        # CaSim/TwoStateSplineModel.cpp:4-34: natural cubic splines through the
+        # (Ca, rate) tables, linear extrapolation beyond the ends
+        m.ch_model = TWO_STATE_SPLINE
+        vals = []
+        for w, key in enumerate(("Kopen filename", "Kclose filename")):
+            tab = np.loadtxt(ch[key]).reshape(-1, 2)
+            _set_spline(m, w, tab[:, 0], tab[:, 1])
     else:
         raise ValueError("gating model not supported by the oracle: " + model)
     for k, v in enumerate(vals):

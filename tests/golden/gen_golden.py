@@ -37,20 +37,38 @@ def coords_text():
         return f.read()
 
 
-def run_case(name, params, coords, steps, seed, first=0):
-    """Run the reference and store snapshots after each entry of `steps` (cumulative)."""
+def spline_tables():
+    """Synthetic rate tables (this project's, 1/ms against Ca in uM) for the
+    TwoStateSpline case: a saturating opening rate and a slowly falling
+    closing rate on uneven knots."""
+    ca = np.concatenate([np.linspace(0.0, 20.0, 11), np.linspace(25.0, 150.0, 26), np.linspace(175.0, 600.0, 18)])
+    x = ca / 20.0
+    kopen = 2.0 + 200.0 * x * x / (1.0 + x * x)
+    kclose = 5.0 + 5.0 * np.exp(-ca / 100.0)
+    return np.c_[ca, kopen], np.c_[ca, kclose]
+
+
+def run_case(name, params, coords, steps, seed, first=0, tables=None):
+    """Run the reference and store snapshots after each entry of `steps` (cumulative).
+    tables: (kopen, kclose) arrays for a TwoStateSpline model, stored in the fixture."""
     with tempfile.TemporaryDirectory() as td:
         cpath = os.path.join(td, "coords.txt")
         with open(cpath, "w") as f:
             f.write(coords)
         p = json.loads(json.dumps(params))
         p["Dyad"]["Channels"]["RyR"]["Coordinates"] = cpath
+        if tables is not None:
+            for key, tab, fn in zip(("Kopen filename", "Kclose filename"), tables, ("kopen.txt", "kclose.txt")):
+                np.savetxt(os.path.join(td, fn), tab, fmt="%.17g")
+                p["Dyad"]["Channels"]["RyR"][key] = os.path.join(td, fn)
         p["Dyad"]["Seed"] = list(seed)
         sim = ref.RefSim(p, 1, 1)
         sim.start([first])
         out = {"params": np.frombuffer(json.dumps(params).encode(), dtype=np.uint8),
                "coords": np.loadtxt(cpath), "seed": np.asarray(seed, dtype=np.uint32),
                "first": np.int32(first), "steps": np.asarray(steps, dtype=np.int64), "dims": np.asarray(sim.dims)}
+        if tables is not None:
+            out["sp_open"], out["sp_close"] = tables
         ions = sorted(p["Dyad"]["Ions"].keys())
         bufs = sorted(p["Dyad"]["Buffers"].keys())
         done = 0
@@ -135,6 +153,20 @@ def main():
     pm["Dyad"]["Channels"]["RyR"]["Parameters"] = {"fCa": 0.00583687, "KCa": 4.1834575, "fMg": 3.2517014,
                                                     "KMg": 92.2954937, "KO0": 10800, "KMgI": 546.4, "kclose": 0.59}
     run_case("ref2d_mwc", pm, coords_text(), [1, 2000], [11] * 6, first=3)
+    # allosteric two-state gating with Mg inhibition (CaSim/TwoStateaHTG.cpp)
+    pa = json.loads(json.dumps(base))
+    pa["Dyad"]["Channels"]["RyR"]["Model"] = "TwoStateaHTG"
+    pa["Dyad"]["Channels"]["RyR"]["Parameters"] = {"fCa": 0.00583687, "KCa": 4.1834575, "fMg": 3.2517014, "KMg": 92.2954937,
+                                                    "KO0": 10800, "KMgI": 546.4, "KCL": 0.1, "KI": 0.01, "KOL": 10.0,
+                                                    "kclose": 200.0}
+    run_case("ref2d_ahtg", pa, coords_text(), [1, 2000], [13] * 6, first=4)
+    # spline-tabulated rates (CaSim/TwoStateSplineModel.cpp, tk::spline)
+    ps = json.loads(json.dumps(base))
+    ps["Dyad"]["Channels"]["RyR"]["Model"] = "TwoStateSpline"
+    ps["Dyad"]["Channels"]["RyR"]["Parameters"] = {}
+    ps["Dyad"]["Channels"]["RyR"]["Kopen filename"] = "kopen.txt"
+    ps["Dyad"]["Channels"]["RyR"]["Kclose filename"] = "kclose.txt"
+    run_case("ref2d_spline", ps, coords_text(), [1, 1500, 3000], [17] * 6, first=6, tables=spline_tables())
     # fast gating: many open/close events in 4000 steps (identical trajectories expected)
     pf = json.loads(json.dumps(base))
     pf["Dyad"]["Channels"]["RyR"]["Parameters"].update({"kopen0": 4e5, "ncaopen": 0.5, "kopenmax": 8e5, "kclose0": 245.0 * 40})

@@ -13,7 +13,17 @@ def load_golden(name):
 
 
 def golden_case(z):
+    """(params, sites) of a fixture; spline-gated fixtures get their rate
+    tables written to a temporary directory and referenced by absolute path."""
     params = json.loads(bytes(z["params"]).decode())
+    if "sp_open" in z.files:
+        import tempfile
+        td = tempfile.mkdtemp(prefix="casim_tables_")
+        ch = params["Dyad"]["Channels"]["RyR"]
+        for key, arr in (("Kopen filename", z["sp_open"]), ("Kclose filename", z["sp_close"])):
+            path = os.path.join(td, os.path.basename(ch[key]))
+            np.savetxt(path, arr, fmt="%.17g")
+            ch[key] = path
     coords = z["coords"]
     d = params["Dyad"]
     nx = int(d["x"] / d["dx"] + 1)

@@ -7,7 +7,17 @@ import pytest
 from oracle import oracle
 from tests.helpers import golden_case, load_golden, species_index
 
-CASES = ["ref2d_sheep", "ref2d_sheep_s3", "ref3d_sheep", "ref2d_mwc"]
+CASES = ["ref2d_sheep", "ref2d_sheep_s3", "ref3d_sheep", "ref2d_mwc", "ref2d_ahtg", "ref2d_spline"]
+# the spline coefficients are solved here by another elimination order than the
+# reference's tk::spline band solver: equal to rounding, not to the bit
+TOL = {"ref2d_spline": 1e-12}
+
+
+def _same(a, b, tol):
+    if tol == 0:
+        return np.array_equal(a, b)
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.max(np.abs(a - b)) <= tol * max(np.max(np.abs(b)), 1e-300)
 
 
 def test_rng_matches_rngstream():
@@ -33,6 +43,7 @@ def test_oracle_reproduces_reference(name):
     sim = oracle.OracleSim(params, sites)
     sim.start(sites["first_channel"])
     idx = species_index(params)
+    tol = TOL.get(name, 0.0)
     done = 0
     for k, n in enumerate(z["steps"]):
         sim.step(int(n) - done)
@@ -40,12 +51,12 @@ def test_oracle_reproduces_reference(name):
         for key in z.files:
             if key.startswith("f%d_" % k):
                 sp = key.split("_", 1)[1]
-                assert np.array_equal(sim.field(0, idx[sp]), z[key]), key
+                assert _same(sim.field(0, idx[sp]), z[key], tol), key
         assert np.array_equal(sim.states(0), z["s%d" % k])
-        assert np.array_equal(sim.mouth(0, idx["Calcium"]), z["m%d_Calcium" % k])
-        assert sim.jsr(0)[0] == z["sr%d" % k][0]
-        assert sim.cyto(0)[0] == z["cy%d" % k][0]
-        assert sim.total_current(0)[0] == z["tc%d" % k][0]
+        assert _same(sim.mouth(0, idx["Calcium"]), z["m%d_Calcium" % k], tol)
+        assert _same(sim.jsr(0)[:1], z["sr%d" % k][:1], tol)
+        assert _same(sim.cyto(0)[:1], z["cy%d" % k][:1], tol)
+        assert _same(sim.total_current(0)[:1], z["tc%d" % k][:1], tol)
 
 
 def test_oracle_gating_trajectory():

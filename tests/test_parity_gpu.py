@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
 FP32_TOL = 1e-5
-GOLDEN_CASES = ["ref2d_sheep", "ref2d_sheep_s3", "ref3d_sheep", "ref2d_mwc"]
+GOLDEN_CASES = ["ref2d_sheep", "ref2d_sheep_s3", "ref3d_sheep", "ref2d_mwc", "ref2d_ahtg", "ref2d_spline"]
 PATHS = ["plain", "resident"]
 
 
