@@ -143,6 +143,12 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
     if (rd3d) off = align16(off + (size_t)2 * maxt * FD * rs);
     a.off_crim = (int)off;
     if (rd3d) off = align16(off + (size_t)maxrim * 2);
+    a.off_ulist = (int)off;
+    if (rd3d) off = align16(off + (size_t)maxrim * 2);
+    a.off_rimc = (int)off;
+    if (rd3d) off = align16(off + (size_t)CSP * maxrim * rs);
+    a.off_slot = (int)off;
+    if (rd3d) off = align16(off + (size_t)mc2 * 2);
     a.off_dptr = (int)off;
     if (rd3d) off = align16(off + (size_t)(mc2 + 1) * 2);
     a.off_dterm = (int)off;

@@ -131,7 +131,7 @@ struct rs_args {
     int cap_cyto;   // stored cytosol nodes per species per rank
     int max_ch, max_terms, max_rim, FD;
     int off_fb, off_ca, off_cb, off_chidx, off_chn, off_chs, off_cho, off_chr, off_ftab, off_pg, off_ring, off_redw,
-        off_rede, off_redt, off_terms, off_crim, off_dptr, off_dterm, off_sc, smem_bytes;
+        off_rede, off_redt, off_terms, off_crim, off_ulist, off_rimc, off_slot, off_dptr, off_dterm, off_sc, smem_bytes;
 };
 
 using cbrng::fold_mod;
@@ -202,6 +202,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     // lane l's stream at draw s_we + l*LANE_DRAWS; s_D draws consumed
     __shared__ unsigned int s_rng[32 * 6];
     __shared__ long long s_D, s_we;
+    __shared__ int s_nu;  // RD3D: slots of this rank's rim
     constexpr int CSM = NI + NPM;  // cytosol species slots
     constexpr int FP = NI + NPM;   // cleft species slots
     const cb_model& m = a.m;
@@ -229,7 +230,10 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     double* rede = (double*)(smem + a.off_rede);  // [2][C][F]
     double* redt = (double*)(smem + a.off_redt);  // [2][C][NI]
     R* terms = (R*)(smem + a.off_terms);          // [2][max_terms][FD] RD3D efflux terms (rank 0)
-    unsigned short* crim = (unsigned short*)(smem + a.off_crim);    // RD3D: rim index -> layer-0 cytosol node
+    unsigned short* crim = (unsigned short*)(smem + a.off_crim);    // RD3D: rim index -> slot of its layer-0 cytosol node
+    unsigned short* ulist = (unsigned short*)(smem + a.off_ulist);  // RD3D: layer-0 cytosol node of each slot (this rank's rim)
+    R* rimc = (R*)(smem + a.off_rimc);                              // RD3D: [CSM][max_rim] their start-of-step values
+    unsigned short* slot_of = (unsigned short*)(smem + a.off_slot); // RD3D: [mc^2] slot of a cytosol node, scratch at load
     unsigned short* dptr = (unsigned short*)(smem + a.off_dptr);    // RD3D: deposit list offsets per layer-0 node
     unsigned short* dterm = (unsigned short*)(smem + a.off_dterm);  // RD3D: efflux terms, oracle order
     cb_site_scalars& q = *(cb_site_scalars*)(smem + a.off_sc);
@@ -289,12 +293,35 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     }
                 const int nrim = cb_rim_count(nx, ny);
                 for (int k = tid; k < nrim; k += blockDim.x) crim[k] = (unsigned short)a.rim_cnode[st.rim_off + k];
+                for (int k = tid; k < mc2; k += blockDim.x) slot_of[k] = 0xFFFF;
                 const int* gp = a.dep_ptr + (size_t)s * (mc2 + 1);
                 for (int k = tid; k <= mc2; k += blockDim.x) dptr[k] = (unsigned short)gp[k];
                 for (int k = tid; k < gp[mc2]; k += blockDim.x) dterm[k] = (unsigned short)a.dep_term[st.term_off + k];
             }
         }
         __syncthreads();
+        if (rd3d && tid == 0) {
+            // the distinct layer-0 cytosol nodes under this rank's rim, in rim order: each
+            // step they are gathered from rank 0 once (phase A) instead of at every use
+            int nu = 0;
+            auto add = [&](int ri) {
+                const int cn = crim[ri];
+                if (slot_of[cn] == 0xFFFF) {
+                    slot_of[cn] = (unsigned short)nu;
+                    ulist[nu++] = (unsigned short)cn;
+                }
+                crim[ri] = slot_of[cn];
+            };
+            for (int y = lo; y < hi; ++y) {
+                add(y);
+                add(ny + y);
+            }
+            if (lo == 0)
+                for (int i = 0; i < nx - 2; ++i) add(2 * ny + i);
+            if (hi == ny)
+                for (int i = 0; i < nx - 2; ++i) add(2 * ny + nx - 2 + i);
+            s_nu = nu;
+        }
         for (int c = tid; c < nch; c += blockDim.x) {
             const int gnode = a.ch_node[st.ch_off + c];
             const int x = gnode % nx, y = (gnode / nx) % ny, z = gnode / nxy;
@@ -481,6 +508,17 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                         if (m.ca_idx >= 0) q.release += q.IjSR[m.ca_idx] * dt;
                     }
                 }
+                if (rd3d) {
+                    // rim values of this step: rank 0's cytosol plane 0 at the start of the
+                    // step (its current buffer, untouched until the step ends)
+                    const R* c0 = peer<C>(ca, 0);
+                    for (int u = lane; u < s_nu; u += 32) {
+                        const int cn = ulist[u];
+#pragma unroll
+                        for (int c = 0; c < CSM; ++c)
+                            if (c < CS) rimc[c * a.max_rim + u] = c0[c * ccap + cn];
+                    }
+                }
                 __syncwarp();
             } else {
                 // ---- worker warps: cleft stencil, strips of rows with a lane per x.
@@ -583,7 +621,8 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     // RD3D cytosol of this rank (no reference analog; see the oracle):
                     // a thread per (i, j) column marching along z through a chunk of
                     // planes; all CSM species slots are stepped (unused slots are zero)
-                    const int wt = tid - 64;
+                    // dealt from the last thread down: the cleft tasks went to the first warps
+                    const int wt = blockDim.x - 1 - tid;
                     for (int t = wt; t < ncol * PC; t += NWT) {
                         const int pc = fdiv(t, fd_ncol), col = t - pc * ncol;
                         const int k0 = plo + pc * PL, k1 = min(k0 + PL, phi);
@@ -674,15 +713,14 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             __syncthreads();
 
             // ---------------------------------------------------- phase B: Update
-            // rim values: the cytosol at the start of this step (RD3D: layer 0 of
-            // rank 0's current buffer, whose plane 0 is its local plane 0)
-            const R* c0 = peer<C>(ca, 0);
+            // rim values: the cytosol at the start of this step (pool, or the RD3D
+            // layer-0 values gathered in phase A)
             auto rim_value = [&](int f, int ri) -> R {
                 if (!rd3d) return f < NI ? (R)q.c_ions[f] : (R)q.c_bnd[f - NI];
-                const int cn = crim[ri];
-                if (f < NI) return c0[f * ccap + cn];
+                const int u = crim[ri];
+                if (f < NI) return rimc[f * a.max_rim + u];
                 const int cq = m.dyad_c_pair[f - NI];
-                return cq >= 0 ? c0[(NI + cq) * ccap + cn] : (R)m.pair_init[f - NI];
+                return cq >= 0 ? rimc[(NI + cq) * a.max_rim + u] : (R)m.pair_init[f - NI];
             };
             // lines of this rank's rim, a warp per line, lanes along it:
             //   l < 4*nz         Dirichlet rim (CaSim/DyadRD2DCPU.cpp:274-303), edge e = l & 3, layer l >> 2:
@@ -831,13 +869,17 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             __syncthreads();
             // rank partials (fixed warp order) into every rank's slot
             if (warp == 0) {
-                for (int k = lane; k < FDn; k += 32) {
-                    double v = 0;
-                    for (int w = 0; w < W; ++w) v += redw[w * FDn + k];
-#pragma unroll 1
-                    for (int r = 0; r < C; ++r) {
-                        if (k < F) peer<C>(rede, r)[(par * C + rank) * F + k] = v;
-                        else peer<C>(redt, r)[(par * C + rank) * NI + (k - F)] = v;
+                double v = 0;
+                if (lane < FDn)
+                    for (int w = 0; w < W; ++w) v += redw[w * FDn + lane];
+                // FDn (at most 20) values x C ranks: one store per lane
+                for (int b0 = 0; b0 < FDn * C; b0 += 32) {
+                    const int idx = b0 + lane;
+                    const int k = idx / C, r = idx - k * C;
+                    const double vk = __shfl_sync(0xffffffffu, v, k < FDn ? k : 0);
+                    if (idx < FDn * C) {
+                        if (k < F) peer<C>(rede, r)[(par * C + rank) * F + k] = vk;
+                        else peer<C>(redt, r)[(par * C + rank) * NI + (k - F)] = vk;
                     }
                 }
             }
