@@ -80,12 +80,14 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
     const bool rd3d = m.cyto_type == CB_CYTO_RD3D;
     // channel and efflux-term capacities are the batch maxima, so the plan of a
     // class fits whenever the plan of its largest site does
-    int cap = 0, ccap = 0, maxrim = 1;
+    int cap = 0, ccap = 0, maxrim = 1, maxlt = 1;
     const int maxch = std::max(d.max_ch, 1), maxt = std::max(d.max_terms, 1);
     for (const cb_site& st : sites) maxrim = std::max(maxrim, cb_rim_count(st.nx, st.ny));
     for (int s : idx) {
         const cb_site& st = sites[s];
         if (st.ny < 3 * C) return false;  // every rank needs three rows (y-edge efflux)
+        const int zmax = st.nz == 1 ? 1 : st.nz - 1;
+        maxlt = std::max(maxlt, 4 * (st.nz + zmax) * ((std::max(st.nx, st.ny) + 31) / 32));
         for (int r = 0; r < C; ++r) {
             int lo = (int)((long long)r * st.ny / C), hi = (int)((long long)(r + 1) * st.ny / C);
             int slo = lo > 0 ? lo - 1 : 0, shi = hi < st.ny ? hi + 1 : st.ny;
@@ -153,6 +155,8 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
     if (rd3d) off = align16(off + (size_t)(mc2 + 1) * 2);
     a.off_dterm = (int)off;
     if (rd3d) off = align16(off + (size_t)maxt * 2);
+    a.off_ltask = (int)off;
+    off = align16(off + (size_t)maxlt * 4);
     a.off_sc = (int)off;
     off = align16(off + sizeof(cb_site_scalars));
     a.smem_bytes = (int)off;
@@ -316,9 +320,19 @@ struct cb_rs_plan {
     int nz = 0;
     std::vector<rs_args> args;
     std::vector<int> cs, threads, clusters;
+    // several classes run side by side, one stream each (forked from and joined to the
+    // caller's stream), so the clusters of one fill the SMs the others leave free
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> done;
+    cudaEvent_t fork = nullptr;
 };
 
 void cb_resident_free(cb_dev& d) {
+    if (d.rs_plan) {
+        for (cudaStream_t s : d.rs_plan->streams) cudaStreamDestroy(s);
+        for (cudaEvent_t e : d.rs_plan->done) cudaEventDestroy(e);
+        if (d.rs_plan->fork) cudaEventDestroy(d.rs_plan->fork);
+    }
     delete d.rs_plan;
     d.rs_plan = nullptr;
 }
@@ -387,6 +401,23 @@ cudaError_t build_plan(cb_dev& d) {
         P->clusters.push_back(clusters);
         offset += a.S;
     }
+    if (P->args.size() > 1) {
+        if ((e = cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming)) != cudaSuccess) {
+            delete P;
+            return e;
+        }
+        for (size_t k = 0; k < P->args.size(); ++k) {
+            cudaStream_t s = nullptr;
+            cudaEvent_t ev = nullptr;
+            if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) == cudaSuccess) P->streams.push_back(s);
+            if (e == cudaSuccess && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) == cudaSuccess) P->done.push_back(ev);
+            if (e != cudaSuccess) {
+                d.rs_plan = P;
+                cb_resident_free(d);
+                return e;
+            }
+        }
+    }
     d.rs_plan = P;
     return cudaSuccess;
 }
@@ -399,14 +430,23 @@ cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long*
     if (!d.rs_plan && (e = build_plan(d)) != cudaSuccess) return e;
     const cb_rs_plan& P = *d.rs_plan;
     if ((e = cudaMemsetAsync(d.rs_counter, 0, sizeof(int) * 8, st)) != cudaSuccess) return e;
-    for (size_t k = 0; k < P.args.size(); ++k) {
-        rs_args a = P.args[k];
+    const bool side = !P.streams.empty();
+    if (side && (e = cudaEventRecord(P.fork, st)) != cudaSuccess) return e;
+    // largest clusters first: the smaller ones then fill the SMs they leave and the tail
+    for (size_t j = P.args.size(); j-- > 0;) {
+        rs_args a = P.args[j];
         a.fields = d.fields[d.cur];
         a.cyto = d.cyto[d.ccur];
         a.nsteps = n;
-        e = launch_t(d, a, P.nz, P.cs[k], P.threads[k], st, a.S, nullptr, P.clusters[k]);
+        cudaStream_t sj = side ? P.streams[j] : st;
+        if (side && (e = cudaStreamWaitEvent(sj, P.fork, 0)) != cudaSuccess) return e;
+        e = launch_t(d, a, P.nz, P.cs[j], P.threads[j], sj, a.S, nullptr, P.clusters[j]);
         if (e != cudaSuccess) return e;
         if (launches) *launches += 1;
+        if (side) {
+            if ((e = cudaEventRecord(P.done[j], sj)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(st, P.done[j], 0)) != cudaSuccess) return e;
+        }
     }
     return cudaSuccess;
 }

@@ -131,7 +131,7 @@ struct rs_args {
     int cap_cyto;   // stored cytosol nodes per species per rank
     int max_ch, max_terms, max_rim, FD;
     int off_fb, off_ca, off_cb, off_chidx, off_chn, off_chs, off_cho, off_chr, off_ftab, off_pg, off_ring, off_redw,
-        off_rede, off_redt, off_terms, off_crim, off_ulist, off_rimc, off_slot, off_dptr, off_dterm, off_sc, smem_bytes;
+        off_rede, off_redt, off_terms, off_crim, off_ulist, off_rimc, off_slot, off_dptr, off_dterm, off_ltask, off_sc, smem_bytes;
 };
 
 using cbrng::fold_mod;
@@ -202,7 +202,9 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     // lane l's stream at draw s_we + l*LANE_DRAWS; s_D draws consumed
     __shared__ unsigned int s_rng[32 * 6];
     __shared__ long long s_D, s_we;
-    __shared__ int s_nu;  // RD3D: slots of this rank's rim
+    __shared__ int s_nu;   // RD3D: slots of this rank's rim
+    __shared__ int s_nlt;  // Update rim tasks of this rank
+    __shared__ int s_nd;  // RD3D, rank 0: layer-0 cytosol nodes that receive efflux deposits
     constexpr int CSM = NI + NPM;  // cytosol species slots
     constexpr int FP = NI + NPM;   // cleft species slots
     const cb_model& m = a.m;
@@ -233,9 +235,11 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     unsigned short* crim = (unsigned short*)(smem + a.off_crim);    // RD3D: rim index -> slot of its layer-0 cytosol node
     unsigned short* ulist = (unsigned short*)(smem + a.off_ulist);  // RD3D: layer-0 cytosol node of each slot (this rank's rim)
     R* rimc = (R*)(smem + a.off_rimc);                              // RD3D: [CSM][max_rim] their start-of-step values
-    unsigned short* slot_of = (unsigned short*)(smem + a.off_slot); // RD3D: [mc^2] slot of a cytosol node, scratch at load
+    unsigned short* slot_of = (unsigned short*)(smem + a.off_slot); // RD3D: [mc^2] slot of a cytosol node, scratch at load;
+    unsigned short* dnode = slot_of;                                // then (rank 0) the nodes that receive deposits
     unsigned short* dptr = (unsigned short*)(smem + a.off_dptr);    // RD3D: deposit list offsets per layer-0 node
     unsigned short* dterm = (unsigned short*)(smem + a.off_dterm);  // RD3D: efflux terms, oracle order
+    int* ltask = (int*)(smem + a.off_ltask);                        // Update rim tasks: line | first node << 16
     cb_site_scalars& q = *(cb_site_scalars*)(smem + a.off_sc);
 
     const double dt = m.dt;
@@ -321,6 +325,34 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             if (hi == ny)
                 for (int i = 0; i < nx - 2; ++i) add(2 * ny + nx - 2 + i);
             s_nu = nu;
+            if (rank == 0) {
+                int nd = 0;
+                for (int cn = 0; cn < mc2; ++cn)
+                    if (dptr[cn + 1] > dptr[cn]) dnode[nd++] = (unsigned short)cn;
+                s_nd = nd;
+            }
+        }
+        if (tid == 32) {
+            // Update rim tasks: 32 consecutive nodes of one line, dealt chunk-major so that
+            // the long y-edge lines of the first and last rank spread over the warps
+            const int zm = NZ == 1 ? 1 : nz - 1;
+            const int nrw = max(min(hi, ny - 1) - max(lo, 1), 0);
+            int nt = 0;
+            for (int k = 0;; ++k) {
+                bool any = false;
+                for (int l = 0; l < 4 * (nz + zm); ++l) {
+                    const bool eff = l >= 4 * nz;
+                    const int e = (eff ? l - 4 * nz : l) & 3;
+                    const bool mine = e == 2 ? lo == 0 : hi == ny;
+                    const int len = e < 2 ? (eff ? nrw : hi - lo) : mine ? (eff ? nx : nx - 2) : 0;
+                    if (32 * k < len) {
+                        ltask[nt++] = l | (32 * k) << 16;
+                        any = true;
+                    }
+                }
+                if (!any) break;
+            }
+            s_nlt = nt;
         }
         for (int c = tid; c < nch; c += blockDim.x) {
             const int gnode = a.ch_node[st.ch_off + c];
@@ -525,6 +557,21 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 // All FP = NI + NPM species slots are stepped (unused slots hold zeros and
                 // have zero coefficients), so the loops carry no species-count tests;
                 // constants are kernel-parameter operands.
+                if (rd3d && rank == 0 && it > 0) {
+                    // efflux deposits of the previous Update per receiving layer-0 cytosol node
+                    // and deposit slot, summed in the oracle's term order over all worker warps;
+                    // each sum replaces its node's first term, which is all plane 0 reads
+                    R* tp = terms + (size_t)prv * a.max_terms * FD;
+                    for (int t = tid - 64; t < s_nd * FD; t += NWT) {
+                        const int k = t / FD, sl = t - k * FD;
+                        const int cn = dnode[k];
+                        double dep = 0;
+                        for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2) dep += (double)tp[dterm[q2] * FD + sl];
+                        tp[dterm[dptr[cn]] * FD + sl] = (R)dep;
+                    }
+                    // the worker warps only (warps 0 and 1 do not take part)
+                    asm volatile("bar.sync 1, %0;" ::"r"(NWT) : "memory");
+                }
                 const int wk = warp - 2;
                 for (int t = wk * 32 + lane; t < nxi * nchunk; t += NW * 32) {
                     const int ch = fdiv(t, fd_nxi);
@@ -686,13 +733,12 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                             for (int c = 0; c < CSM; ++c) {
                                 R e = evo[c];
                                 if constexpr (P0) {
-                                    // deposit of the previous Update, in the oracle's term order
+                                    // deposit of the previous Update (its node sum, formed before the stencil)
                                     double dep = 0;
                                     if (it == 0) {
                                         if (c < CS) dep = a.cin[((size_t)s * CS + c) * mc2 + cn];
-                                    } else if (a.kf.cdep[c] >= 0) {
-                                        for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2)
-                                            dep += (double)terms[(prv * a.max_terms + dterm[q2]) * FD + a.kf.cdep[c]];
+                                    } else if (a.kf.cdep[c] >= 0 && dptr[cn + 1] > dptr[cn]) {
+                                        dep = (double)terms[(prv * a.max_terms + dterm[dptr[cn]]) * FD + a.kf.cdep[c]];
                                     }
                                     e += (R)dep;
                                 }
@@ -722,7 +768,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 const int cq = m.dyad_c_pair[f - NI];
                 return cq >= 0 ? rimc[(NI + cq) * a.max_rim + u] : (R)m.pair_init[f - NI];
             };
-            // lines of this rank's rim, a warp per line, lanes along it:
+            // lines of this rank's rim in tasks of 32 nodes (a warp per task, lanes along the line):
             //   l < 4*nz         Dirichlet rim (CaSim/DyadRD2DCPU.cpp:274-303), edge e = l & 3, layer l >> 2:
             //                    e 0/1 columns x = 0 / nx-1 over y in [lo, hi); e 2/3 rows y = 0 / ny-1
             //                    over x in [1, nx-2] where this rank holds them
@@ -734,7 +780,11 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             bool did_e = false;
             {
                 R* t0 = peer<C>(terms + (size_t)par * a.max_terms * FD, 0);
-                for (int l = warp; l < 4 * (nz + zmax); l += W) {
+                // one-block sites: the last warps hold the channels (and their rate laws), so
+                // the tasks go to the others
+                const int WL = C == 1 ? max(1, W - (nch + 31) / 32) : W;
+                for (int tk = warp; tk < s_nlt && warp < WL; tk += WL) {
+                    const int l = ltask[tk] & 0xFFFF, i = (ltask[tk] >> 16) + lane;
                     const bool eff = l >= 4 * nz;
                     const int le = eff ? l - 4 * nz : l;
                     const int z = le >> 2, e = le & 3;
@@ -747,13 +797,13 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                             dxs = 0;
                             ri0 = (e ? ny : 0) + lo;
                         } else {
-                            len = (e == 2 ? lo == 0 : hi == ny) ? nx - 2 : 0;
+                            len = nx - 2;
                             x0 = 1;
                             y0 = e == 2 ? 0 : ny - 1;
                             dxs = 1;
                             ri0 = 2 * ny + (e == 2 ? 0 : nx - 2);
                         }
-                        for (int i = lane; i < len; i += 32) {
+                        if (i < len) {
                             const int x = x0 + dxs * i, y = y0 + (1 - dxs) * i;
                             const int n = x + nx * ((y - slo) + nr * z);
 #pragma unroll
@@ -762,7 +812,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                         }
                     } else {
                         did_e = true;
-                        int len, x0, y0, dxs, dys, gt0, gts;
+                        int len, x0, y0, dxs, dys, gt0;
                         double sf;
                         if (e < 2) {
                             len = nrows;
@@ -773,7 +823,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                             sf = m.sx;
                             gt0 = (e * (ny - 2) + (ylo - 1)) * zmax + z;
                         } else {
-                            len = (e == 2 ? lo == 0 : hi == ny) ? nx : 0;
+                            len = nx;
                             x0 = 0;
                             y0 = e == 2 ? 0 : ny - 1;
                             dxs = 0;
@@ -781,7 +831,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                             sf = m.sy;
                             gt0 = (2 * (ny - 2) + (e - 2) * nx) * zmax + z;
                         }
-                        for (int i = lane; i < len; i += 32) {
+                        if (i < len) {
                             // the edge node walks along the line: y for x-edges, x for y-edges
                             const int xe = e < 2 ? x0 : i, ye = e < 2 ? y0 + i : y0;
                             const int ri = e < 2 ? (e ? ny : 0) + ye
@@ -789,13 +839,18 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                                                             : xe == nx - 1 ? ny + ye : 2 * ny + (e == 2 ? 0 : nx - 2) + xe - 1);
                             const int n1 = (xe + dxs) + nx * ((ye + dys - slo) + nr * z);
                             const int n2 = (xe + 2 * dxs) + nx * ((ye + 2 * dys - slo) + nr * z);
+                            // a y-edge line's end nodes step along the x = 0 / nx-1 rim column,
+                            // whose Dirichlet values another task of this phase writes: use them directly
+                            const int rc = (e >= 2 && (xe == 0 || xe == nx - 1)) ? (xe == 0 ? 0 : ny) : -1;
                             const int gterm = gt0 + i * zmax;
 #pragma unroll
                             for (int f = 0; f < CSM; ++f) {
                                 if (f < F) {
                                     const double u0 = (double)rim_value(f, ri);
                                     const double D = f < NI ? m.D_ion[f] : m.D_pair[f - NI];
-                                    const double gr = 2 * (double)fb[f * cap + n1] - 1.5 * u0 - 0.5 * (double)fb[f * cap + n2];
+                                    const double u1 = rc >= 0 ? (double)rim_value(f, rc + ye + dys) : (double)fb[f * cap + n1];
+                                    const double u2 = rc >= 0 ? (double)rim_value(f, rc + ye + 2 * dys) : (double)fb[f * cap + n2];
+                                    const double gr = 2 * u1 - 1.5 * u0 - 0.5 * u2;
                                     if (!rd3d) {
                                         epart[f] += D * m.grad_mult * sf * gr;
                                     } else {
