@@ -334,7 +334,8 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
         }
         if (tid == 32) {
             // Update rim tasks: 32 consecutive nodes of one line, dealt chunk-major so that
-            // the long y-edge lines of the first and last rank spread over the warps
+            // the long y-edge lines of the first and last rank spread over the warps (one-block
+            // sites: whole lines, one task each)
             const int zm = NZ == 1 ? 1 : nz - 1;
             const int nrw = max(min(hi, ny - 1) - max(lo, 1), 0);
             int nt = 0;
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                         any = true;
                     }
                 }
-                if (!any) break;
+                if (!any || C == 1) break;
             }
             s_nlt = nt;
         }
@@ -784,7 +785,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 // the tasks go to the others
                 const int WL = C == 1 ? max(1, W - (nch + 31) / 32) : W;
                 for (int tk = warp; tk < s_nlt && warp < WL; tk += WL) {
-                    const int l = ltask[tk] & 0xFFFF, i = (ltask[tk] >> 16) + lane;
+                    const int l = ltask[tk] & 0xFFFF, i0 = ltask[tk] >> 16;
                     const bool eff = l >= 4 * nz;
                     const int le = eff ? l - 4 * nz : l;
                     const int z = le >> 2, e = le & 3;
@@ -803,7 +804,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                             dxs = 1;
                             ri0 = 2 * ny + (e == 2 ? 0 : nx - 2);
                         }
-                        if (i < len) {
+                        for (int i = i0 + lane; i < (C == 1 ? len : min(len, i0 + 32)); i += 32) {
                             const int x = x0 + dxs * i, y = y0 + (1 - dxs) * i;
                             const int n = x + nx * ((y - slo) + nr * z);
 #pragma unroll
@@ -831,7 +832,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                             sf = m.sy;
                             gt0 = (2 * (ny - 2) + (e - 2) * nx) * zmax + z;
                         }
-                        if (i < len) {
+                        for (int i = i0 + lane; i < (C == 1 ? len : min(len, i0 + 32)); i += 32) {
                             // the edge node walks along the line: y for x-edges, x for y-edges
                             const int xe = e < 2 ? x0 : i, ye = e < 2 ? y0 + i : y0;
                             const int ri = e < 2 ? (e ? ny : 0) + ye
