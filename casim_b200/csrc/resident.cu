@@ -171,9 +171,11 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
 }
 
 // warps 0 and 1 run gating and the pools; the rest run the stencils
-int pick_threads(const std::vector<cb_site>& sites, const std::vector<int>& idx, int C, int cap) {
+int pick_threads(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<int>& idx, int C, int cap) {
     long long mx = 0;
     for (int s : idx) mx = std::max(mx, (long long)sites[s].nx * sites[s].ny * sites[s].nz / C);
+    // RD3D: the rank's share of the cytosol, a column task per (column, plane chunk)
+    if (d.m.cyto_type == CB_CYTO_RD3D) mx += 2LL * (d.m.mc - 2) * (d.m.mc - 2) * (d.m.mc - 1) / C;
     long long t = ((mx / 8 + 31) / 32 + 2) * 32;
     return (int)std::max(128LL, std::min((long long)cap, t));
 }
@@ -257,7 +259,7 @@ bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* 
         fill_const(d.m, a.kf);
         fill_const(d.m, a.kd);
         int clusters = 0;
-        const int thr = pick_threads(sites, classes[k], cs[k], thread_cap(d, nz));
+        const int thr = pick_threads(d, sites, classes[k], cs[k], thread_cap(d, nz));
         cudaError_t e = launch_t(d, a, nz, cs[k], thr, 0, 0, &clusters);
         if (e != cudaSuccess || clusters < 1) {
             cudaGetLastError();
@@ -388,7 +390,7 @@ cudaError_t build_plan(cb_dev& d) {
         a.spc0 = d.spc[0];
         a.spx1 = d.spx[1];
         a.spc1 = d.spc[1];
-        const int threads = pick_threads(sites, classes[k], cs[k], thread_cap(d, nz));
+        const int threads = pick_threads(d, sites, classes[k], cs[k], thread_cap(d, nz));
         int clusters = 0;
         e = launch_t(d, a, nz, cs[k], threads, 0, a.S, &clusters);
         if (e != cudaSuccess || clusters < 1) {
