@@ -97,15 +97,18 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
     cap = (cap + 3) / 4 * 4;
     const int CS = m.n_ions + m.c_n_pairs;
     const int mc = m.mc, mc2 = mc * mc;
+    // cytosol planes start on 16-byte boundaries in shared memory (vector halo copies)
+    const int vr = (int)(16 / rs), cps = (mc2 + vr - 1) / vr * vr;
     if (rd3d) {
         if (mc - 1 < C) return false;
         for (int r = 0; r < C; ++r) {
             int plo = (int)((long long)r * (mc - 1) / C), phi = (int)((long long)(r + 1) * (mc - 1) / C);
             int splo = plo > 0 ? plo - 1 : 0;
-            ccap = std::max(ccap, (phi + 1 - splo) * mc2);
+            ccap = std::max(ccap, (phi + 1 - splo) * cps);
         }
         ccap = (ccap + 3) / 4 * 4;
     }
+    a.cps = cps;
     int FD = 0;
     for (int f = 0; f < m.F; ++f)
         if (f < m.n_ions || m.dyad_c_pair[f - m.n_ions] >= 0) ++FD;

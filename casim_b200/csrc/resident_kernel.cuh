@@ -129,6 +129,7 @@ struct rs_args {
     // shared-memory carve (bytes, identical for every block of the launch)
     int cap_cleft;  // stored cleft nodes per species per rank
     int cap_cyto;   // stored cytosol nodes per species per rank
+    int cps;        // stride of a stored cytosol plane (mc^2 rounded up to 16 bytes)
     int max_ch, max_terms, max_rim, FD;
     int off_fb, off_ca, off_cb, off_chidx, off_chn, off_chs, off_cho, off_chr, off_ftab, off_pg, off_ring, off_redw,
         off_rede, off_redt, off_terms, off_crim, off_ulist, off_rimc, off_slot, off_dptr, off_dterm, off_ltask, off_sc, smem_bytes;
@@ -268,7 +269,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
         const int phi = rd3d ? (int)(((long long)(rank + 1) * nplanes) / C) : 0;
         const int splo = plo > 0 ? plo - 1 : 0, sphi = phi + 1;
         const int cloc = (sphi - splo) * mc2;
-        const int cap = a.cap_cleft, ccap = a.cap_cyto;
+        const int cap = a.cap_cleft, ccap = a.cap_cyto, cps = a.cps;
 
         // ---------------------------------------------------------- load
         {
@@ -292,8 +293,9 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 for (int c = 0; c < CSM; ++c)
                     for (int k = tid; k < cloc; k += blockDim.x) {
                         const R v = c < CS ? cs[(size_t)c * nc + (size_t)splo * mc2 + k] : (R)0;
-                        ca[c * ccap + k] = v;
-                        cb[c * ccap + k] = v;
+                        const int pl = k / mc2, l = pl * cps + (k - pl * mc2);
+                        ca[c * ccap + l] = v;
+                        cb[c * ccap + l] = v;
                     }
                 const int nrim = cb_rim_count(nx, ny);
                 for (int k = tid; k < nrim; k += blockDim.x) crim[k] = (unsigned short)a.rim_cnode[st.rim_off + k];
@@ -681,17 +683,17 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                         R uP[CSM], uC[CSM], uN[CSM];
 #pragma unroll
                         for (int c = 0; c < CSM; ++c) {
-                            uC[c] = ca[c * ccap + cn + mc2 * (k0 - splo)];
-                            uP[c] = k0 > 0 ? ca[c * ccap + cn + mc2 * (k0 - 1 - splo)] : (R)0;
+                            uC[c] = ca[c * ccap + cn + cps * (k0 - splo)];
+                            uP[c] = k0 > 0 ? ca[c * ccap + cn + cps * (k0 - 1 - splo)] : (R)0;
                         }
                         // one plane; P0: plane 0, whose lower face mirrors and which
                         // receives the efflux deposit of the previous Update
                         auto plane = [&](int k, auto p0) {
                             constexpr bool P0 = decltype(p0)::value;
-                            const int ln = cn + mc2 * (k - splo);
+                            const int ln = cn + cps * (k - splo);
 #pragma unroll
                             for (int c = 0; c < CSM; ++c) {
-                                uN[c] = ca[c * ccap + ln + mc2];
+                                uN[c] = ca[c * ccap + ln + cps];
                                 if constexpr (P0) uP[c] = uN[c];  // no-flux face: mirror
                             }
                             R evo[CSM];
@@ -965,9 +967,12 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                         const int nplo = (int)(((long long)nb * nplanes) / C);
                         const int nsplo = nplo > 0 ? nplo - 1 : 0;
                         R* dst = peer<C>(cb, nb);
-                        for (int c = 0; c < CS; ++c)
-                            for (int e = tid; e < mc2; e += blockDim.x)
-                                dst[c * ccap + (k - nsplo) * mc2 + e] = cb[c * ccap + (k - splo) * mc2 + e];
+                        // whole 16-byte words of the padded plane (the padding goes along)
+                        const int nv = cps * (int)sizeof(R) / 16;
+                        for (int t = tid; t < CS * nv; t += blockDim.x) {
+                            const int c = t / nv, e = t - c * nv;
+                            ((uint4*)(dst + c * ccap + (k - nsplo) * cps))[e] = ((const uint4*)(cb + c * ccap + (k - splo) * cps))[e];
+                        }
                     }
                 }
             }
@@ -1035,8 +1040,10 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             if (rd3d) {
                 R* cd = (R*)a.cyto + (size_t)s * CS * nc;
                 for (int c = 0; c < CS; ++c)
-                    for (int k = tid; k < (phi - plo) * mc2; k += blockDim.x)
-                        cd[(size_t)c * nc + (size_t)plo * mc2 + k] = ca[c * ccap + (plo - splo) * mc2 + k];
+                    for (int k = tid; k < (phi - plo) * mc2; k += blockDim.x) {
+                        const int pl = k / mc2;
+                        cd[(size_t)c * nc + (size_t)plo * mc2 + k] = ca[c * ccap + (plo - splo + pl) * cps + (k - pl * mc2)];
+                    }
                 if (rank == 0 && a.nsteps > 0) {
                     // deposit of the final Update, for the next launch
                     const int pl = (int)((a.nsteps - 1) & 1);
