@@ -192,8 +192,8 @@ int layers_of(const cb_model& m, const std::vector<cb_site>& sites) {
 }
 
 
-int thread_cap(const cb_dev& d, int nz) {
-    return max_threads(d.precision == 0 ? 8 : 4, d.m.n_ions + npm_of(d.m.n_ions, pairs_of(d.m)), nz);
+int thread_cap(const cb_dev& d, int nz, int C) {
+    return max_threads(d.precision == 0 ? 8 : 4, d.m.n_ions + npm_of(d.m.n_ions, pairs_of(d.m)), nz, C);
 }
 
 cudaError_t launch_t(const cb_dev& d, const rs_args& a, int nz, int C, int threads, cudaStream_t st, int n, int* dry = nullptr,
@@ -262,7 +262,7 @@ bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* 
         fill_const(d.m, a.kf);
         fill_const(d.m, a.kd);
         int clusters = 0;
-        const int thr = pick_threads(d, sites, classes[k], cs[k], thread_cap(d, nz));
+        const int thr = pick_threads(d, sites, classes[k], cs[k], thread_cap(d, nz, cs[k]));
         cudaError_t e = launch_t(d, a, nz, cs[k], thr, 0, 0, &clusters);
         if (e != cudaSuccess || clusters < 1) {
             cudaGetLastError();
@@ -393,7 +393,7 @@ cudaError_t build_plan(cb_dev& d) {
         a.spc0 = d.spc[0];
         a.spx1 = d.spx[1];
         a.spc1 = d.spc[1];
-        const int threads = pick_threads(d, sites, classes[k], cs[k], thread_cap(d, nz));
+        const int threads = pick_threads(d, sites, classes[k], cs[k], thread_cap(d, nz, cs[k]));
         int clusters = 0;
         e = launch_t(d, a, nz, cs[k], threads, 0, a.S, &clusters);
         if (e != cudaSuccess || clusters < 1) {

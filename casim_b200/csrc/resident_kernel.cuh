@@ -50,7 +50,12 @@ constexpr int JUMP_ROW = 64;             // pow table row holding A^(2*31*LANE_D
 // Threads per block a kernel is compiled for. A stencil lane keeps three rows
 // of CSM species x NZ layers in registers; FP64 3D layouts with many species
 // get 255 registers per thread (256 threads) instead of 128 (512 threads).
-__host__ __device__ constexpr int max_threads(int rbytes, int csm, int nz) { return 3 * nz * csm * rbytes / 4 > 60 ? 256 : 512; }
+// block size bound of a specialisation; 16-block clusters stop at 384 threads (three warps
+// per SM sub-partition) so that the step loop keeps its values in registers (168 per
+// thread instead of 128)
+__host__ __device__ constexpr int max_threads(int rbytes, int csm, int nz, int C) {
+    return 3 * nz * csm * rbytes / 4 > 60 ? 256 : C == 16 ? 384 : 512;
+}
 // pair capacity of the kernel specialisation that serves NI ions and NP pairs
 __host__ __device__ constexpr int npm_of(int NI, int NP) { return (NI == 1 && NP <= 2) ? 2 : 4; }
 
@@ -196,7 +201,7 @@ __device__ __forceinline__ int dslot(const cb_model& m, int NI, int f) {
 }
 
 template <typename R, int NI, int NPM, int NZ, int C>
-__global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_resident(const __grid_constant__ rs_args a) {
+__global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_resident(const __grid_constant__ rs_args a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_site;
     // RNG of warp 0, kept in shared memory so it holds no registers during the stencils:
@@ -205,7 +210,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     __shared__ long long s_D, s_we;
     __shared__ int s_nu;   // RD3D: slots of this rank's rim
     __shared__ int s_nlt;  // Update rim tasks of this rank
-    __shared__ int s_nd;  // RD3D, rank 0: layer-0 cytosol nodes that receive efflux deposits
+    __shared__ int s_nd;  // RD3D, plane-0 rank: layer-0 cytosol nodes that receive efflux deposits
     constexpr int CSM = NI + NPM;  // cytosol species slots
     constexpr int FP = NI + NPM;   // cleft species slots
     const cb_model& m = a.m;
@@ -232,12 +237,12 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
     double* redw = (double*)(smem + a.off_redw);  // [MAX_WARPS][F + NI]
     double* rede = (double*)(smem + a.off_rede);  // [2][C][F]
     double* redt = (double*)(smem + a.off_redt);  // [2][C][NI]
-    R* terms = (R*)(smem + a.off_terms);          // [2][max_terms][FD] RD3D efflux terms (rank 0)
+    R* terms = (R*)(smem + a.off_terms);          // [2][max_terms][FD] RD3D efflux terms (plane-0 rank)
     unsigned short* crim = (unsigned short*)(smem + a.off_crim);    // RD3D: rim index -> slot of its layer-0 cytosol node
     unsigned short* ulist = (unsigned short*)(smem + a.off_ulist);  // RD3D: layer-0 cytosol node of each slot (this rank's rim)
     R* rimc = (R*)(smem + a.off_rimc);                              // RD3D: [CSM][max_rim] their start-of-step values
     unsigned short* slot_of = (unsigned short*)(smem + a.off_slot); // RD3D: [mc^2] slot of a cytosol node, scratch at load;
-    unsigned short* dnode = slot_of;                                // then (rank 0) the nodes that receive deposits
+    unsigned short* dnode = slot_of;                                // then (plane-0 rank) the nodes that receive deposits
     unsigned short* dptr = (unsigned short*)(smem + a.off_dptr);    // RD3D: deposit list offsets per layer-0 node
     unsigned short* dterm = (unsigned short*)(smem + a.off_dterm);  // RD3D: efflux terms, oracle order
     int* ltask = (int*)(smem + a.off_ltask);                        // Update rim tasks: line | first node << 16
@@ -265,8 +270,12 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
         const int lstride = nx * nr;  // z stride in local storage
         const int nloc = lstride * nz;
         const int nplanes = mc - 1;
-        const int plo = rd3d ? (int)(((long long)rank * nplanes) / C) : 0;
-        const int phi = rd3d ? (int)(((long long)(rank + 1) * nplanes) / C) : 0;
+        // RD3D: rank r holds plane block (r + C/2) mod C, so that plane 0 (deposits, rim
+        // values) sits on rank r0 = C - C/2, away from the first and last row blocks, which
+        // carry the long y-edge rim lines
+        const int pb = (rank + C / 2) % C, r0 = (C - C / 2) % C;
+        const int plo = rd3d ? (int)(((long long)pb * nplanes) / C) : 0;
+        const int phi = rd3d ? (int)(((long long)(pb + 1) * nplanes) / C) : 0;
         const int splo = plo > 0 ? plo - 1 : 0, sphi = phi + 1;
         const int cloc = (sphi - splo) * mc2;
         const int cap = a.cap_cleft, ccap = a.cap_cyto, cps = a.cps;
@@ -308,7 +317,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
         __syncthreads();
         if (rd3d && tid == 0) {
             // the distinct layer-0 cytosol nodes under this rank's rim, in rim order: each
-            // step they are gathered from rank 0 once (phase A) instead of at every use
+            // step they are gathered from the plane-0 rank once (phase A) instead of at every use
             int nu = 0;
             auto add = [&](int ri) {
                 const int cn = crim[ri];
@@ -327,7 +336,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             if (hi == ny)
                 for (int i = 0; i < nx - 2; ++i) add(2 * ny + nx - 2 + i);
             s_nu = nu;
-            if (rank == 0) {
+            if (rank == r0) {
                 int nd = 0;
                 for (int cn = 0; cn < mc2; ++cn)
                     if (dptr[cn + 1] > dptr[cn]) dnode[nd++] = (unsigned short)cn;
@@ -544,9 +553,9 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                     }
                 }
                 if (rd3d) {
-                    // rim values of this step: rank 0's cytosol plane 0 at the start of the
+                    // rim values of this step: the plane-0 rank's cytosol plane 0 at the start of the
                     // step (its current buffer, untouched until the step ends)
-                    const R* c0 = peer<C>(ca, 0);
+                    const R* c0 = peer<C>(ca, r0);
                     for (int u = lane; u < s_nu; u += 32) {
                         const int cn = ulist[u];
 #pragma unroll
@@ -560,7 +569,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 // All FP = NI + NPM species slots are stepped (unused slots hold zeros and
                 // have zero coefficients), so the loops carry no species-count tests;
                 // constants are kernel-parameter operands.
-                if (rd3d && rank == 0 && it > 0) {
+                if (rd3d && rank == r0 && it > 0) {
                     // efflux deposits of the previous Update per receiving layer-0 cytosol node
                     // and deposit slot, summed in the oracle's term order over all worker warps;
                     // each sum replaces its node's first term, which is all plane 0 reads
@@ -782,7 +791,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
             for (int f = 0; f < CSM; ++f) epart[f] = 0;
             bool did_e = false;
             {
-                R* t0 = peer<C>(terms + (size_t)par * a.max_terms * FD, 0);
+                R* t0 = peer<C>(terms + (size_t)par * a.max_terms * FD, r0);
                 // one-block sites: the last warps hold the channels (and their rate laws), so
                 // the tasks go to the others
                 const int WL = C == 1 ? max(1, W - (nch + 31) / 32) : W;
@@ -961,10 +970,11 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                 if (rd3d && phi > plo) {
                     // cytosol halo planes
                     for (int side = 0; side < 2; ++side) {
-                        const int nb = side == 0 ? rank - 1 : rank + 1;
-                        if (nb < 0 || nb >= C) continue;
+                        const int nbb = side == 0 ? pb - 1 : pb + 1;  // neighbour plane block
+                        if (nbb < 0 || nbb >= C) continue;
+                        const int nb = (nbb + C - C / 2) % C;
                         const int k = side == 0 ? plo : phi - 1;
-                        const int nplo = (int)(((long long)nb * nplanes) / C);
+                        const int nplo = (int)(((long long)nbb * nplanes) / C);
                         const int nsplo = nplo > 0 ? nplo - 1 : 0;
                         R* dst = peer<C>(cb, nb);
                         // whole 16-byte words of the padded plane (the padding goes along)
@@ -1044,7 +1054,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ), 1) k_res
                         const int pl = k / mc2;
                         cd[(size_t)c * nc + (size_t)plo * mc2 + k] = ca[c * ccap + (plo - splo + pl) * cps + (k - pl * mc2)];
                     }
-                if (rank == 0 && a.nsteps > 0) {
+                if (rank == r0 && a.nsteps > 0) {
                     // deposit of the final Update, for the next launch
                     const int pl = (int)((a.nsteps - 1) & 1);
                     for (int cn = tid; cn < mc2; cn += blockDim.x)
@@ -1116,7 +1126,7 @@ cudaError_t launch_c(const rs_args& a, int C, int threads, cudaStream_t st, int 
 // NP: the larger of the cleft's ion-buffer pairs and (RD3D) the cytosol's
 template <typename R, int NZ>
 cudaError_t dispatch(const rs_args& a, int NI, int NP, int C, int threads, cudaStream_t st, int n, int* dry, int known) {
-    if (threads > max_threads(sizeof(R), NI + npm_of(NI, NP), NZ)) return cudaErrorInvalidConfiguration;
+    if (threads > max_threads(sizeof(R), NI + npm_of(NI, NP), NZ, C)) return cudaErrorInvalidConfiguration;
     if (NI == 1 && NP <= 2) return launch_c<R, 1, 2, NZ>(a, C, threads, st, n, dry, known);
     if (NI == 1 && NP <= 4) return launch_c<R, 1, 4, NZ>(a, C, threads, st, n, dry, known);
     if (NI == 2 && NP <= 4) return launch_c<R, 2, 4, NZ>(a, C, threads, st, n, dry, known);
