@@ -43,7 +43,8 @@ EXPORTS = (
     "casim_b200_sg_gate_steps", "casim_b200_sg_run", "casim_b200_sg_create", "casim_b200_sg_destroy", "casim_b200_sg_set_stream", "casim_b200_sg_num_params",
     "casim_b200_sg_get_params", "casim_b200_sg_set_params", "casim_b200_sg_forward", "casim_b200_sg_gradients",
     "casim_b200_sg_train_step", "casim_b200_sg_check", "casim_b200_sg_launches", "casim_b200_sg_last_error",
-    "casim_b200_sg_gemm",
+    "casim_b200_sg_gemm", "casim_b200_trace_enable", "casim_b200_trace_count", "casim_b200_get_open_traces",
+    "casim_b200_release_analysis",
 )
 
 
@@ -121,6 +122,10 @@ def lib():
         L.casim_b200_set_site_jsr.argtypes = [vp, dp]
         L.casim_b200_path_note.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         L.casim_b200_rng_draws_static.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]
+        L.casim_b200_trace_enable.argtypes = [vp, i64, i64]
+        L.casim_b200_trace_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.casim_b200_get_open_traces.argtypes = [vp, ctypes.POINTER(ctypes.c_uint16)]
+        L.casim_b200_release_analysis.argtypes = [vp, ctypes.c_double, ctypes.c_double, i32, dp, ip, ip, ip, ip, ip]
         fp = ctypes.POINTER(ctypes.c_float)
         L.casim_b200_sg_create.argtypes = [i32, i32, i32, i32, ctypes.c_uint64, ctypes.POINTER(vp)]
         L.casim_b200_sg_destroy.argtypes = [vp]
@@ -317,6 +322,40 @@ class ReleaseSiteBatch:
         out = np.zeros(int(self.n_ch[site]), dtype=np.int32)
         self._ck(lib().casim_b200_get_states(self.h, site, _p(out, ctypes.c_int32)))
         return out
+
+    def trace_enable(self, every_steps, max_samples):
+        """Record the open-RyR count of every site now and every `every_steps` time
+        steps of step() from here on (at most `max_samples` samples)."""
+        self._ck(lib().casim_b200_trace_enable(self.h, int(every_steps), int(max_samples)))
+        self._trace_every = int(every_steps)
+
+    def open_traces(self):
+        """[sites, samples] uint16 open-RyR counts recorded since trace_enable."""
+        n = ctypes.c_int64(0)
+        self._ck(lib().casim_b200_trace_count(self.h, ctypes.byref(n)))
+        out = np.zeros((self.S, n.value), dtype=np.uint16)
+        self._ck(lib().casim_b200_get_open_traces(self.h, _p(out, ctypes.c_uint16)))
+        return out
+
+    def release_analysis(self, max_time_ms, nadir, hist_dt_ms=0.01):
+        """Release-event analysis of the recorded traces on the device (the
+        arithmetic of CaSim/IndChannelCREAnalyzer.cpp:53-138): per site amplitude,
+        time to peak, time to end, integral and mean of the open count, and the
+        time histograms of the open count over all sites, quarks, blips, sparks."""
+        nh = int(max_time_ms / hist_dt_ms)
+        mch = int(self.info.max_channels)
+        per_site = np.zeros((self.S, 5))
+        h_all = np.zeros((nh + 1, mch + 1), dtype=np.int32)
+        h_q = np.zeros((nh + 1, 2), dtype=np.int32)
+        h_b = np.zeros((nh + 1, int(nadir) + 1), dtype=np.int32)
+        h_s = np.zeros((nh + 1, mch + 1), dtype=np.int32)
+        counts = np.zeros(3, dtype=np.int32)
+        i32p = ctypes.c_int32
+        self._ck(lib().casim_b200_release_analysis(self.h, float(hist_dt_ms), float(max_time_ms), int(nadir), _p(per_site, ctypes.c_double),
+                                                   _p(h_all, i32p), _p(h_q, i32p), _p(h_b, i32p), _p(h_s, i32p), _p(counts, i32p)))
+        return {"amp": per_site[:, 0], "ttp": per_site[:, 1], "tte": per_site[:, 2], "integral": per_site[:, 3],
+                "mean": per_site[:, 4], "hist": h_all, "hist_quark": h_q, "hist_blip": h_b, "hist_spark": h_s,
+                "quarks": int(counts[0]), "blips": int(counts[1]), "sparks": int(counts[2])}
 
     def all_states(self):
         out = np.zeros(int(self.n_ch.sum()), dtype=np.int32)

@@ -34,6 +34,9 @@ struct casim_b200_sim {
     void* sg_net = nullptr;
     const void* sg_out = nullptr;  // the network's output buffer when the window was captured
     cudaGraphExec_t sg_exec = nullptr;
+    // open-RyR traces: [site][tr_max] u16, a sample every tr_every steps of casim_b200_step
+    uint16_t* tr = nullptr;
+    long long tr_every = 0, tr_max = 0, tr_n = 0, tr_phase = 0;
 };
 
 namespace {
@@ -267,6 +270,7 @@ casim_status casim_b200_destroy(casim_h h) {
     if (h->d.rs_pow2) cudaFree(h->d.rs_pow2);
     cb_resident_free(h->d);
     if (h->sg_exec) cudaGraphExecDestroy(h->sg_exec);
+    if (h->tr) cudaFree(h->tr);
     if (h->sg_x) cudaFree(h->sg_x);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -391,11 +395,107 @@ casim_status casim_b200_step(casim_h h, int64_t n) {
     if (n < 0) throw std::runtime_error("negative step count");
     long long launches = 0;
     ck(cudaEventRecord(h->ev0, h->stream), "cudaEventRecord");
-    if (h->path == CASIM_PATH_RESIDENT) ck(cb_resident_step(h->d, n, h->stream, &launches), "resident step");
-    else ck(cb_plain_step(h->d, n, h->stream, &launches), "plain step");
+    auto run = [&](long long k) {
+        if (h->path == CASIM_PATH_RESIDENT) ck(cb_resident_step(h->d, k, h->stream, &launches), "resident step");
+        else ck(cb_plain_step(h->d, k, h->stream, &launches), "plain step");
+    };
+    if (h->tr && h->tr_n < h->tr_max) {
+        // stop at every sample time of the open-RyR trace
+        long long left = n;
+        while (left > 0 && h->tr_n < h->tr_max) {
+            const long long k = std::min(left, h->tr_every - h->tr_phase);
+            run(k);
+            left -= k;
+            h->tr_phase += k;
+            if (h->tr_phase == h->tr_every) {
+                ck(cb_trace_record(h->d, h->tr, h->tr_max, h->tr_n++, h->stream), "trace record");
+                ++launches;
+                h->tr_phase = 0;
+            }
+        }
+        if (left > 0) run(left);
+    } else {
+        run(n);
+    }
     ck(cudaEventRecord(h->ev1, h->stream), "cudaEventRecord");
     h->timed = true;
     h->last_launches = launches;
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_trace_enable(casim_h h, int64_t every_steps, int64_t max_samples) {
+    GUARD(h)
+    if (every_steps < 1 || max_samples < 1) throw std::runtime_error("trace needs every_steps >= 1 and max_samples >= 1");
+    if ((double)max_samples * h->d.S * sizeof(uint16_t) > 16e9) throw std::runtime_error("trace larger than 16 GB");
+    if (h->tr) {
+        ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        ck(cudaFree(h->tr), "cudaFree");
+        h->tr = nullptr;
+    }
+    void* p = nullptr;
+    ck(cudaMalloc(&p, (size_t)max_samples * h->d.S * sizeof(uint16_t)), "cudaMalloc");
+    h->tr = (uint16_t*)p;
+    h->tr_every = every_steps;
+    h->tr_max = max_samples;
+    h->tr_n = 0;
+    h->tr_phase = 0;
+    ck(cb_trace_record(h->d, h->tr, h->tr_max, h->tr_n++, h->stream), "trace record");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_trace_count(casim_h h, int64_t* n_samples) {
+    if (!h || !n_samples) return CASIM_EINVAL;
+    *n_samples = h->tr ? h->tr_n : 0;
+    return CASIM_OK;
+}
+
+casim_status casim_b200_get_open_traces(casim_h h, uint16_t* out) {
+    GUARD(h)
+    if (!out) throw std::runtime_error("null output");
+    if (!h->tr) throw std::runtime_error("no trace: call casim_b200_trace_enable first");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    ck(cudaMemcpy2D(out, (size_t)h->tr_n * sizeof(uint16_t), h->tr, (size_t)h->tr_max * sizeof(uint16_t),
+                    (size_t)h->tr_n * sizeof(uint16_t), (size_t)h->d.S, cudaMemcpyDeviceToHost),
+       "cudaMemcpy2D");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
+casim_status casim_b200_release_analysis(casim_h h, double hist_dt_ms, double max_time_ms, int32_t nadir, double* per_site,
+                                         int32_t* hist_all, int32_t* hist_quark, int32_t* hist_blip, int32_t* hist_spark,
+                                         int32_t* class_counts) {
+    GUARD(h)
+    if (!h->tr || h->tr_n < 1) throw std::runtime_error("no trace: call casim_b200_trace_enable first");
+    if (!(hist_dt_ms > 0) || !(max_time_ms >= 0) || nadir < 0) throw std::runtime_error("bad histogram arguments");
+    if (!per_site || !hist_all || !hist_quark || !hist_blip || !hist_spark || !class_counts) throw std::runtime_error("null output");
+    const double ts = (double)h->tr_every * h->d.m.dt;  // ms between samples
+    const long long nh = (long long)(max_time_ms / hist_dt_ms);  // CaSim/IndChannelCREAnalyzer.cpp:58
+    if (nh > 100000000LL) throw std::runtime_error("histogram longer than 1e8 bins");
+    const int mch = h->d.max_ch, S = h->d.S;
+    const size_t na = (size_t)(nh + 1) * (mch + 1), nq = (size_t)(nh + 1) * 2, nb = (size_t)(nh + 1) * (nadir + 1);
+    void* buf = nullptr;
+    const size_t bytes = (size_t)S * 5 * sizeof(double) + (S + 3 + 2 * na + nq + nb) * sizeof(int);
+    ck(cudaMalloc(&buf, bytes), "cudaMalloc");
+    double* d_ps = (double*)buf;
+    int* d_cls = (int*)(d_ps + (size_t)S * 5);
+    int* d_cnt = d_cls + S;
+    int* d_all = d_cnt + 3;
+    int* d_q = d_all + na;
+    int* d_b = d_q + nq;
+    int* d_s = d_b + nb;
+    cudaError_t e = cb_cre_analysis(h->d, h->tr, h->tr_max, h->tr_n, ts, hist_dt_ms, nh, nadir, d_ps, d_cls, d_all, d_q, d_b, d_s,
+                                    d_cnt, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(per_site, d_ps, (size_t)S * 5 * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(class_counts, d_cnt, 3 * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hist_all, d_all, na * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hist_quark, d_q, nq * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hist_blip, d_b, nb * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hist_spark, d_s, na * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+    ck(e, "release analysis");
     return CASIM_OK;
     END_GUARD(h)
 }

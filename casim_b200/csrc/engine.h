@@ -61,6 +61,11 @@ cudaError_t cb_sg_features(cb_dev& d, int max_ch, int ld, float* X, cudaStream_t
 cudaError_t cb_sg_mouth(cb_dev& d, const float* Y, int ld, double ca_ref, cudaStream_t st);
 cudaError_t cb_sg_steps(cb_dev& d, long long n, cudaStream_t st);
 cudaError_t cb_sg_steps_warp(cb_dev& d, long long n, cudaStream_t st, bool* used);  // sg_gate.cu
+// analysis.cu: open-RyR trace sample j of every site; the release-event analysis of n samples
+cudaError_t cb_trace_record(const cb_dev& d, uint16_t* trace, long long max_samples, long long j, cudaStream_t st);
+cudaError_t cb_cre_analysis(const cb_dev& d, const uint16_t* trace, long long max_samples, long long n, double ts, double hd,
+                            long long nh, int nadir, double* per_site, int* cls, int* h_all, int* h_q, int* h_b, int* h_s,
+                            int* counts, cudaStream_t st);
 // the surrogate network (surrogate.cu)
 struct casim_surrogate_s;
 cudaError_t cb_sg_net_prepare(struct casim_surrogate_s* net, int batch);

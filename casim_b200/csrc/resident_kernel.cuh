@@ -244,7 +244,9 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
     unsigned short* slot_of = (unsigned short*)(smem + a.off_slot); // RD3D: [mc^2] slot of a cytosol node, scratch at load;
     unsigned short* dnode = slot_of;                                // then (plane-0 rank) the nodes that receive deposits
     unsigned short* dptr = (unsigned short*)(smem + a.off_dptr);    // RD3D: deposit list offsets per layer-0 node
-    unsigned short* dterm = (unsigned short*)(smem + a.off_dterm);  // RD3D: efflux terms, oracle order
+    // RD3D: stored position of each efflux term; the terms are stored grouped by receiving
+    // layer-0 cytosol node (node cn's in [dptr[cn], dptr[cn + 1]), the oracle's order within)
+    unsigned short* tpos = (unsigned short*)(smem + a.off_dterm);
     int* ltask = (int*)(smem + a.off_ltask);                        // Update rim tasks: line | first node << 16
     cb_site_scalars& q = *(cb_site_scalars*)(smem + a.off_sc);
 
@@ -311,7 +313,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                 for (int k = tid; k < mc2; k += blockDim.x) slot_of[k] = 0xFFFF;
                 const int* gp = a.dep_ptr + (size_t)s * (mc2 + 1);
                 for (int k = tid; k <= mc2; k += blockDim.x) dptr[k] = (unsigned short)gp[k];
-                for (int k = tid; k < gp[mc2]; k += blockDim.x) dterm[k] = (unsigned short)a.dep_term[st.term_off + k];
+                for (int k = tid; k < gp[mc2]; k += blockDim.x) tpos[a.dep_term[st.term_off + k]] = (unsigned short)k;
             }
         }
         __syncthreads();
@@ -578,8 +580,8 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                         const int k = t / FD, sl = t - k * FD;
                         const int cn = dnode[k];
                         double dep = 0;
-                        for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2) dep += (double)tp[dterm[q2] * FD + sl];
-                        tp[dterm[dptr[cn]] * FD + sl] = (R)dep;
+                        for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2) dep += (double)tp[q2 * FD + sl];
+                        tp[dptr[cn] * FD + sl] = (R)dep;
                     }
                     // the worker warps only (warps 0 and 1 do not take part)
                     asm volatile("bar.sync 1, %0;" ::"r"(NWT) : "memory");
@@ -750,7 +752,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                                     if (it == 0) {
                                         if (c < CS) dep = a.cin[((size_t)s * CS + c) * mc2 + cn];
                                     } else if (a.kf.cdep[c] >= 0 && dptr[cn + 1] > dptr[cn]) {
-                                        dep = (double)terms[(prv * a.max_terms + dterm[dptr[cn]]) * FD + a.kf.cdep[c]];
+                                        dep = (double)terms[(prv * a.max_terms + dptr[cn]) * FD + a.kf.cdep[c]];
                                     }
                                     e += (R)dep;
                                 }
@@ -869,7 +871,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                                         const double v = D * sf * gr * m.inv_hc3;
                                         epart[f] += v;
                                         const int sl = dslot(m, NI, f);
-                                        if (sl >= 0) t0[gterm * FD + sl] = (R)v;
+                                        if (sl >= 0) t0[tpos[gterm] * FD + sl] = (R)v;
                                     }
                                 }
                             }
@@ -1063,7 +1065,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                             double dep = 0;
                             if (sl >= 0)
                                 for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2)
-                                    dep += (double)terms[(pl * a.max_terms + dterm[q2]) * FD + sl];
+                                    dep += (double)terms[(pl * a.max_terms + q2) * FD + sl];
                             a.cin[((size_t)s * CS + c) * mc2 + cn] = dep;
                         }
                 }

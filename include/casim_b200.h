@@ -165,6 +165,35 @@ casim_status casim_b200_check_finite(casim_h h, int32_t* bad_site);
 casim_status casim_b200_get_all_mouth(casim_h h, int32_t species, double* out);  /* sum of channels */
 casim_status casim_b200_get_all_states(casim_h h, int32_t* out);
 
+/* Open-RyR traces recorded on the device. Replaces the host round trip of the
+ * channel states at the output cadence (CaSim/ParallelHybridSolver.cpp:316-337)
+ * that feeds the reference's release analysis. casim_b200_trace_enable allocates
+ * [sites][max_samples] u16 counts, records sample 0 (the current states) and
+ * then one sample every every_steps time steps of casim_b200_step (which stops
+ * at each sample time; surrogate-gated windows are not sampled); sample j is at
+ * j * every_steps * dt after the enable. Recording stops at max_samples. */
+casim_status casim_b200_trace_enable(casim_h h, int64_t every_steps, int64_t max_samples);
+casim_status casim_b200_trace_count(casim_h h, int64_t* n_samples);
+/* out: [site][n_samples], n_samples from casim_b200_trace_count. */
+casim_status casim_b200_get_open_traces(casim_h h, uint16_t* out);
+
+/* Release-event analysis of the recorded traces on the device, with the
+ * arithmetic of IndChannelCREAnalyzer::RunAnalysis
+ * (CaSim/IndChannelCREAnalyzer.cpp:53-138), each site one trace:
+ *   per_site [sites][5]: amplitude (most open RyRs), time to peak, time to end,
+ *     integral of the open count (ms), its mean;
+ *   histograms of open counts over time bins of hist_dt_ms (the reference's
+ *     fixed 0.01 ms, CaSim/IndChannelCREAnalyzer.cpp:7), nh + 1 rows with
+ *     nh = (long long)(max_time_ms / hist_dt_ms): hist_all [nh+1][max_ch+1],
+ *     hist_quark (amplitude 1) [nh+1][2], hist_blip (amplitude <= nadir, other
+ *     than 1) [nh+1][nadir+1], hist_spark [nh+1][max_ch+1]; column 0 of each is
+ *     the class's trace count minus the other columns (:32-38);
+ *   class_counts [3]: quarks, blips, sparks.
+ * max_ch is the largest RyR count of a site (the reference has one count). */
+casim_status casim_b200_release_analysis(casim_h h, double hist_dt_ms, double max_time_ms, int32_t nadir, double* per_site,
+                                         int32_t* hist_all, int32_t* hist_quark, int32_t* hist_blip, int32_t* hist_spark,
+                                         int32_t* class_counts);
+
 /* How the resident path splits the batch into thread-block-cluster classes,
  * or why the handle runs on the plain path. */
 casim_status casim_b200_path_note(casim_h h, char* buf, size_t n);

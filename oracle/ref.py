@@ -92,3 +92,35 @@ class RefSim:
         out = np.zeros(n, dtype=np.int32)
         L.casimref_get_states(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
         return out
+
+
+def cre_analysis(times, states, max_time, nadir):
+    """The reference's own IndChannelCREAnalyzer::RunAnalysis
+    (CaSim/IndChannelCREAnalyzer.cpp:53-138) on traces given as events: times[i] (n_i,)
+    and states[i] (n_i, n_channels) of 0/1. Returns what it writes: the per-scenario
+    table and the four time histograms (first column of the files, the bin time, dropped)."""
+    import tempfile
+    L = lib()
+    n_ch = int(np.asarray(states[0]).shape[1])
+    n_ev = np.array([len(t) for t in times], dtype=np.int32)
+    tt = np.ascontiguousarray(np.concatenate([np.asarray(t, dtype=np.float64) for t in times]))
+    ss = np.ascontiguousarray(np.concatenate([np.asarray(s, dtype=np.int32).reshape(-1, n_ch) for s in states]))
+    with tempfile.TemporaryDirectory() as d:
+        os.makedirs(os.path.join(d, "analysis"))
+        f = L.casimref_cre_analysis
+        f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                      ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        rc = f(d.encode(), len(times), n_ev.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+               tt.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ss.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+               n_ch, float(max_time), int(nadir))
+        if rc:
+            raise RuntimeError("reference analysis failed: " + L.casimref_last_error().decode())
+
+        def table(name):
+            rows = [ln.split() for ln in open(os.path.join(d, "analysis", name)) if ln.strip()]
+            return np.array([[float(v) for v in r] for r in rows])
+        out = {"per_trace": table("scenarios.txt")}
+        for key, name in (("hist", "time_hist.txt"), ("hist_quark", "time_hist_quarks.txt"),
+                          ("hist_blip", "time_hist_blips.txt"), ("hist_spark", "time_hist_sparks.txt")):
+            out[key] = table(name)[:, 1:].astype(np.int64)
+    return out

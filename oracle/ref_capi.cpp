@@ -234,3 +234,35 @@ extern "C" void casimref_rng_draws(const unsigned long* seed6, long n, double* o
     RngStream g;
     for (long k = 0; k < n; ++k) out[k] = g.RandU01();
 }
+
+// The reference's own release analysis (CaSim/IndChannelCREAnalyzer.cpp:53-138) over
+// n_scen traces given as events: times [sum(n_events)] and the open (1) / closed (0)
+// state of each of n_ch channels per event [sum(n_events)][n_ch]. Two-state channels:
+// the state-to-open map of every channel is {0, 1}. It writes dir/analysis/*.txt.
+#include "IndChannelCREAnalyzer.h"
+#undef min
+#undef max
+extern "C" int casimref_cre_analysis(const char* dir, int n_scen, const int* n_events, const double* times, const int* states,
+                                     int n_ch, double max_time, int nadir) {
+    try {
+        std::vector<std::vector<std::vector<double>>> data(n_scen);
+        long q = 0;
+        for (int i = 0; i < n_scen; ++i) {
+            data[i].resize(n_events[i]);
+            for (int j = 0; j < n_events[i]; ++j, ++q) {
+                std::vector<double> row(1 + n_ch);
+                row[0] = times[q];
+                for (int c = 0; c < n_ch; ++c) row[1 + c] = states[q * n_ch + c];
+                data[i][j] = row;
+            }
+        }
+        std::vector<std::vector<int>> channels(n_ch, std::vector<int>{0, 1});
+        std::string name(dir);
+        IndChannelCREAnalyzer a;
+        a.RunAnalysis(name, data, channels, max_time, 1, nadir);  // one thread: its class counters are not atomic
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
