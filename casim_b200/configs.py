@@ -7,6 +7,7 @@ jSR initial values, initially opened RyR). All randomness is seeded.
 
 Units follow the reference: nm, ms, uM; D in nm^2/ms; dt in ns.
 """
+import json
 import math
 
 import numpy as np
@@ -34,6 +35,32 @@ def sheep_cannell_power_law(k0_per_ms=0.1, k_half_uM=15.0, n=2.5, kclose_per_ms=
         "kclose0": kclose_per_ms * 1000.0,
         "ncaclose": 0.0,
     }
+
+
+# 60-state single-site MWC RyR of the reference's example (examples/IaparovGPU/Parameters.json)
+SINGLE_SITE_MWC = {"KCa": 4.1834575, "KMg": 92.2954937, "KMgI": 546.4, "KO0": 10800, "alphaCa": 0, "alphaI": 0, "alphaMg": 0,
+                   "alphaMgI": 0, "alphakco": 0.67057446, "alphakcoI": 0.67057446, "fCa": 0.00583687, "fCa4I": 0.00583687,
+                   "fICa": 0.00583687, "fIMg": 3.2517014, "fMg": 3.2517014, "gCa": 1, "gMg": 1, "kco": 0.00110487,
+                   "konCa": 0.71, "konMg": 0.0071, "konmgI": 5.9002e-07}
+
+
+def with_single_site_mwc(params, speed=1.0):
+    """A copy of `params` gated by the 60-state SingleSiteMWC model (CaSim/SingleSiteMWC.cpp):
+    adds a Magnesium ion (1 mM, no conductance) to the dyad, jSR and NSR; `speed`
+    scales the binding and opening rate constants (faster gating for short tests)."""
+    p = json.loads(json.dumps(params))
+    d = p["Dyad"]
+    d["Ions"]["Magnesium"] = {"Concentration": 1000.0, "D": 160000.0, "Extracell": 1000.0}
+    ch = d["Channels"]["RyR"]
+    ch["Model"] = "SingleSiteMWC"
+    par = dict(SINGLE_SITE_MWC)
+    for k in ("konCa", "konMg", "kco", "konmgI"):
+        par[k] *= speed
+    ch["Parameters"] = par
+    ch["Conductance"]["Magnesium"] = 0.0
+    p["jSR"]["Ions"]["Magnesium"] = {"Binding sites of CQ": 1, "Concentration": 1000.0, "K CQ (uM)": 1.0e6, "T refill (ms)": 10.0}
+    p["nSR"]["Ions"]["Magnesium"] = {"Concentration (uM)": 1000.0}
+    return p
 
 
 def lattice(n, cx, cy, rng, pitch=RYR_PITCH_NM, jitter=3.0):

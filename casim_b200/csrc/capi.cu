@@ -11,6 +11,7 @@
 
 #include "../../include/casim_b200.h"
 #include "engine.h"
+#include "mwc.h"
 #include "parse.h"
 #include "mrg32k3a.cuh"
 #include "physics.cuh"
@@ -184,6 +185,17 @@ void build_device(casim_b200_sim* h, int precision) {
     d.ch_owner = dupload(h, ch_owner);
     d.ch_state = dalloc<int>(h, (size_t)choff);
     ck(cudaMemset(d.ch_state, 0, sizeof(int) * (size_t)std::max(choff, 1)), "cudaMemset");
+    if (cfg.m.ch_model == CB_SINGLE_SITE_MWC) {
+        // initial distribution at the initial mouth values: the ions' concentrations
+        // (the map InitOpening reads before any gating, CaSim/DyadChannels.h:25-58)
+        cb_mwc_tab tab;
+        cb_mwc_build(cfg.m.ch_par, cfg.m.Cb[cfg.m.ca_idx], cfg.m.Cb[cfg.m.mg_idx], tab);
+        cb_mwc_tab* dt = dalloc<cb_mwc_tab>(h, 1);
+        ck(cudaMemcpy(dt, &tab, sizeof(tab), cudaMemcpyHostToDevice), "cudaMemcpy");
+        d.mwc = dt;
+        d.ch_micro = dalloc<int>(h, (size_t)choff);
+        ck(cudaMemset(d.ch_micro, 0, sizeof(int) * (size_t)std::max(choff, 1)), "cudaMemset");
+    }
     d.mouth = dalloc<double>(h, (size_t)choff * d.NS);
     ck(cudaMemset(d.mouth, 0, sizeof(double) * (size_t)std::max(choff * d.NS, 1)), "cudaMemset");
     for (int k = 0; k < 2; ++k) d.fields[k] = dalloc<char>(h, (size_t)nb * cfg.m.F * rs);
@@ -626,6 +638,19 @@ casim_status casim_b200_get_states(casim_h h, int32_t site, int32_t* out) {
     END_GUARD(h)
 }
 
+casim_status casim_b200_get_micro_states(casim_h h, int32_t site, int32_t* out) {
+    GUARD(h)
+    check_site(h, site);
+    if (!out) throw std::runtime_error("null output");
+    if (!h->d.ch_micro) throw std::runtime_error("the RyR model has no micro-states (two-state gating)");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    cb_site st;
+    ck(cudaMemcpy(&st, h->d.sites + site, sizeof(st), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    ck(cudaMemcpy(out, h->d.ch_micro + st.ch_off, sizeof(int) * st.n_ch, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
 casim_status casim_b200_sg_features(casim_h h, int32_t max_channels, int32_t ld, float* x_dev) {
     GUARD(h)
     if (!x_dev || max_channels < 1 || ld < 3 * max_channels + 1 + h->d.m.n_buf) throw std::runtime_error("bad feature layout");
@@ -646,6 +671,7 @@ casim_status casim_b200_sg_gate_steps(casim_h h, int64_t n) {
     GUARD(h)
     if (n < 0) throw std::runtime_error("negative step count");
     if (h->d.m.cyto_type != CB_CYTO_POOL) throw std::runtime_error("surrogate gating needs the pool cytosol");
+    if (h->d.m.ch_model == CB_SINGLE_SITE_MWC) throw std::runtime_error("surrogate gating serves two-state RyR models");
     if (n > 0) ck(cb_sg_steps(h->d, n, h->stream), "surrogate steps");
     return CASIM_OK;
     END_GUARD(h)
@@ -670,6 +696,7 @@ casim_status casim_b200_sg_run(casim_h h, casim_sg net, int32_t max_channels, in
     GUARD(h)
     if (!net || n < 0 || window < 1 || !(ca_ref > 0) || max_channels < 1) throw std::runtime_error("bad surrogate run arguments");
     if (h->d.m.cyto_type != CB_CYTO_POOL) throw std::runtime_error("surrogate gating needs the pool cytosol");
+    if (h->d.m.ch_model == CB_SINGLE_SITE_MWC) throw std::runtime_error("surrogate gating serves two-state RyR models");
     const int ld = 3 * max_channels + 1 + h->d.m.n_buf;
     const int rows = (h->d.S + 127) / 128 * 128;
     if (!h->sg_x || h->sg_rows != rows || h->sg_ld != ld) {
@@ -725,6 +752,7 @@ casim_status casim_b200_sg_run(casim_h h, casim_sg net, int32_t max_channels, in
 
 casim_status casim_b200_set_all_states(casim_h h, const int32_t* states) {
     GUARD(h)
+    if (h->d.ch_micro) throw std::runtime_error("set_all_states sets two-state RyRs only");
     if (!states) throw std::runtime_error("states is null");
     for (long long c = 0; c < h->d.total_ch; ++c)
         if (states[c] != 0 && states[c] != 1) throw std::runtime_error("RyR states must be 0 or 1");

@@ -27,6 +27,8 @@ struct cb_dev {
     int* ch_node = nullptr;           // local node index (x fastest) per RyR
     int* ch_owner = nullptr;          // 1 if the RyR is the highest-index one at its node
     int* ch_state = nullptr;          // open (1) / closed (0)
+    int* ch_micro = nullptr;          // SingleSiteMWC: micro-state 0..59 per RyR (else unused)
+    const struct cb_mwc_tab* mwc = nullptr;  // SingleSiteMWC: adjacency and initial distribution
     double* mouth = nullptr;          // [(ch)*NS + species]
     // RD3D cytosol
     int nc = 0;                       // nodes per site cytosol (mc^3)

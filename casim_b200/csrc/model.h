@@ -11,11 +11,11 @@
 #define CB_MAX_CPAIRS 16
 #define CB_MAX_SPECIES (CB_MAX_IONS + CB_MAX_PAIRS)
 #define CB_MAX_CSPECIES (CB_MAX_IONS + CB_MAX_CPAIRS)
-#define CB_MAX_CHPAR 16
+#define CB_MAX_CHPAR 24
 #define CB_MAX_CHANNELS 1024
 
 // gating laws (CaSim/PassiveIonChannel.cpp:10-26)
-enum { CB_SHEEP_CANNELL = 0, CB_TWO_STATE_MWC = 1, CB_TWO_STATE_AHTG = 2, CB_TWO_STATE_SPLINE = 3 };
+enum { CB_SHEEP_CANNELL = 0, CB_TWO_STATE_MWC = 1, CB_TWO_STATE_AHTG = 2, CB_TWO_STATE_SPLINE = 3, CB_SINGLE_SITE_MWC = 4 };
 enum { CB_CYTO_POOL = 0, CB_CYTO_RD3D = 1 };
 
 struct cb_model {

@@ -21,6 +21,8 @@
 
 #include "../../include/casim_b200.h"
 #include "mrg32k3a.cuh"
+#include "mwc.h"
+#include <cstring>
 
 using json = nlohmann::json;
 
@@ -134,6 +136,31 @@ void natural_spline(const std::vector<double>& x, const std::vector<double>& y, 
 std::string join(const std::string& dir, const std::string& p) {
     if (p.empty() || p[0] == '/' || dir.empty()) return p;
     return dir + "/" + p;
+}
+
+// dense solve with partial pivoting (row swaps), then back substitution
+std::vector<double> solve_pivoted(std::vector<std::vector<double>> a, std::vector<double> b) {
+    const int n = (int)b.size();
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
+        std::swap(a[c], a[piv]);
+        std::swap(b[c], b[piv]);
+        for (int r = c + 1; r < n; ++r) {
+            const double f = a[r][c] / a[c][c];
+            if (f == 0) continue;
+            for (int k = c; k < n; ++k) a[r][k] -= f * a[c][k];
+            b[r] -= f * b[c];
+        }
+    }
+    std::vector<double> x(n, 0.0);
+    for (int r = n - 1; r >= 0; --r) {
+        double v = b[r];
+        for (int k = r + 1; k < n; ++k) v -= a[r][k] * x[k];
+        x[r] = v / a[r][r];
+    }
+    return x;
 }
 
 void read_table(const std::string& path, std::vector<double>& a, std::vector<double>& b) {
@@ -275,11 +302,19 @@ cb_config cb_parse_config(const std::string& json_text, const std::string& base_
             cfg.sp_x[w] = xs;
             m.sp_n[w] = (int)xs.size();
         }
+    } else if (model == "SingleSiteMWC") {
+        // 60-state Q-matrix model (CaSim/SingleSiteMWC.cpp:5-37); absent names read as 0
+        // like the reference's std::map lookups
+        m.ch_model = CB_SINGLE_SITE_MWC;
+        const char* names[MWC_NPAR] = {"fCa4I", "fCa", "KCa", "alphaCa", "konCa", "fMg", "KMg", "konMg", "alphaMg", "alphaMgI",
+                                       "KO0", "alphakco", "alphakcoI", "kco", "KMgI", "konmgI", "fICa", "fIMg", "gMg", "gCa"};
+        for (int k = 0; k < MWC_NPAR; ++k) cp.push_back(num_or(par, names[k], 0.0));
     } else {
-        fail("gating model \"" + model + "\" is not supported by this build (SheepCannell, TwoStateMWC, TwoStateaHTG, TwoStateSpline)");
+        fail("gating model \"" + model + "\" is not supported by this build (SheepCannell, TwoStateMWC, TwoStateaHTG, TwoStateSpline, "
+             "SingleSiteMWC)");
     }
     for (size_t k = 0; k < cp.size(); ++k) m.ch_par[k] = cp[k];
-    if ((m.ch_model == CB_TWO_STATE_MWC || m.ch_model == CB_TWO_STATE_AHTG) && m.mg_idx < 0)
+    if ((m.ch_model == CB_TWO_STATE_MWC || m.ch_model == CB_TWO_STATE_AHTG || m.ch_model == CB_SINGLE_SITE_MWC) && m.mg_idx < 0)
         fail("gating model " + model + " needs a Magnesium ion");
     if (m.ca_idx < 0) fail("gating needs a Calcium ion");
     const json& cond = need(ch, "Conductance", "Channels");
@@ -475,4 +510,54 @@ cb_config cb_parse_config(const std::string& json_text, const std::string& base_
         for (int i = 0; i < m.n_ions; ++i) h.jsr0[i] = tab && tab->jsr_init ? tab->jsr_init[(long long)s * m.n_ions + i] : m.jsr0[i];
     }
     return cfg;
+}
+
+// Adjacency lists in the push order of CaSim/SingleSiteMWC.cpp:55-89 and the stationary
+// distribution p of the full Q at (ca0, mg0): p = 1^T (S S^T)^-1 with S = [Q | 1], the
+// least-squares solution of p Q = 0, sum p = 1 (CaSim/QMatrixModel.cpp:38-47).
+void cb_mwc_build(const double* P, double ca0, double mg0, cb_mwc_tab& t) {
+    std::memset(&t, 0, sizeof(t));
+    auto push = [&](int x, int y) { t.adj[x][t.nadj[x]++] = (unsigned char)y; };
+    auto in_all_blocks = [&](int x, int y) {
+        push(x, y);
+        push(x + 45, y + 45);
+        push(x + 15, y + 15);
+        push(x + 30, y + 30);
+    };
+    auto idx = [](int i, int j) { return 15 - (6 - j) * (5 - j) / 2 + i; };
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5 - i; ++j) {
+            const int c = idx(i, j);
+            if (i + j < 4) in_all_blocks(c, idx(i + 1, j));
+            if (i > 0) in_all_blocks(c, idx(i - 1, j));
+            if (i + j < 4) in_all_blocks(c, idx(i, j + 1));
+            if (j > 0) in_all_blocks(c, idx(i, j - 1));
+            push(c, c + 15);
+            push(c + 15, c);
+            push(c + 45, c + 30);
+            push(c + 30, c + 45);
+            push(c, c + 45);
+            push(c + 45, c);
+            push(c + 15, c + 30);
+            push(c + 30, c + 15);
+        }
+    std::vector<std::vector<double>> Q(CB_MWC_N, std::vector<double>(CB_MWC_N, 0.0));
+    for (int s = 0; s < CB_MWC_N; ++s) {
+        double r = 0;
+        for (int k = 0; k < t.nadj[s]; ++k) {
+            const int d = t.adj[s][k];
+            Q[s][d] = cb_mwc_q(P, s, d, ca0, mg0);
+            r += Q[s][d];
+        }
+        Q[s][s] = -r;
+    }
+    std::vector<std::vector<double>> M(CB_MWC_N, std::vector<double>(CB_MWC_N, 0.0));
+    for (int i = 0; i < CB_MWC_N; ++i)
+        for (int j = 0; j < CB_MWC_N; ++j) {
+            double v = 1.0;
+            for (int k = 0; k < CB_MWC_N; ++k) v += Q[i][k] * Q[j][k];
+            M[i][j] = v;
+        }
+    const std::vector<double> p = solve_pivoted(M, std::vector<double>(CB_MWC_N, 1.0));
+    for (int i = 0; i < CB_MWC_N; ++i) t.p_init[i] = p[i];
 }

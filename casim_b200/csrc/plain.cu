@@ -15,6 +15,7 @@
 
 #include "engine.h"
 #include "mrg32k3a.cuh"
+#include "mwc.h"
 #include "physics.cuh"
 #include "pools.cuh"
 
@@ -77,7 +78,8 @@ __global__ void k_cyto_reset(cb_model m, int nc, R* __restrict__ A, R* __restric
 }
 
 __global__ void k_init_open(const cb_site* __restrict__ sites, const int* __restrict__ first, int lo, int hi,
-                            cb_site_scalars* __restrict__ sc, int* __restrict__ ch_state) {
+                            cb_site_scalars* __restrict__ sc, int* __restrict__ ch_state, int* __restrict__ ch_micro,
+                            const cb_mwc_tab* __restrict__ mwc) {
     int s = lo + blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= hi) return;
     const cb_site st = sites[s];
@@ -86,20 +88,31 @@ __global__ void k_init_open(const cb_site* __restrict__ sites, const int* __rest
     for (int i = 0; i < 6; ++i) g.s[i] = q.rng[i];
     // CaSim/DyadChannels.cpp:83-95: one draw per channel (SetMacroState(0, .)),
     // then one more for the channel that is opened
+    // (SingleSiteMWC: each draw picks the micro-state of the macro state from the
+    // stationary distribution, CaSim/QMatrixModel.cpp:38-58)
     for (int c = 0; c < st.n_ch; ++c) {
-        (void)cbrng::u01d_fold(g);
+        const double u = cbrng::u01d_fold(g);
         ch_state[st.ch_off + c] = 0;
+        if (mwc) ch_micro[st.ch_off + c] = cb_mwc_pick(*mwc, 0, u, ch_micro[st.ch_off + c]);
     }
-    (void)cbrng::u01d_fold(g);
+    const double u = cbrng::u01d_fold(g);
     int f = first[s - lo];
-    if (f >= 0 && f < st.n_ch) ch_state[st.ch_off + f] = 1;
+    if (f >= 0 && f < st.n_ch) {
+        ch_state[st.ch_off + f] = 1;
+        if (mwc) {
+            const int mi = cb_mwc_pick(*mwc, 1, u, ch_micro[st.ch_off + f]);
+            ch_micro[st.ch_off + f] = mi;
+            ch_state[st.ch_off + f] = mi >= CB_MWC_OPEN;
+        }
+    }
     q.draws += (unsigned long long)st.n_ch + 1;
     for (int i = 0; i < 6; ++i) q.rng[i] = g.s[i];
 }
 
 __global__ void k_pre(cb_model m, int S, int NS, const cb_site* __restrict__ sites, cb_site_scalars* __restrict__ sc,
                       int* __restrict__ ch_state, const double* __restrict__ mouth, const double* __restrict__ spx0,
-                      const double* __restrict__ spc0, const double* __restrict__ spx1, const double* __restrict__ spc1) {
+                      const double* __restrict__ spc0, const double* __restrict__ spx1, const double* __restrict__ spc1,
+                      int* __restrict__ ch_micro, const cb_mwc_tab* __restrict__ mwc) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
     const cb_site st = sites[s];
@@ -114,6 +127,20 @@ __global__ void k_pre(cb_model m, int S, int NS, const cb_site* __restrict__ sit
         const double* mo = mouth + (long long)(st.ch_off + c) * NS;
         double ca = mo[m.ca_idx];
         double mg = m.mg_idx >= 0 ? mo[m.mg_idx] : 0.0;
+        if (mwc) {
+            // SingleSiteMWC: escape rate of the micro-state, the second draw picks where to
+            const int mi = ch_micro[st.ch_off + c];
+            const double r = cb_mwc_exit(m.ch_par, *mwc, mi, ca, mg);
+            ++draws;
+            if (cbrng::u01d_fold(g) < r * dt) {
+                const double u2 = cbrng::u01d_fold(g);
+                ++draws;
+                const int nx = cb_mwc_next(m.ch_par, *mwc, mi, ca, mg, r, u2);
+                ch_micro[st.ch_off + c] = nx;
+                ch_state[st.ch_off + c] = nx >= CB_MWC_OPEN;
+            }
+            continue;
+        }
         int state = ch_state[st.ch_off + c];
         double r = cb_rate(m, spx0, spc0, spx1, spc1, state, ca, mg);
         ++draws;
@@ -396,7 +423,7 @@ cudaError_t launch_update(cb_dev& d, cudaStream_t st) {
 template <typename R>
 cudaError_t launch_step(cb_dev& d, cudaStream_t st) {
     k_pre<<<(d.S + 127) / 128, 128, 0, st>>>(d.m, d.S, d.NS, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0],
-                                               d.spx[1], d.spc[1]);
+                                               d.spx[1], d.spc[1], d.ch_micro, d.mwc);
     if (d.m.cyto_type == CB_CYTO_RD3D) {
         dim3 g((d.nc + 255) / 256, d.S);
         k_cyto<R><<<g, 256, 0, st>>>(d.m, d.nc, (const R*)d.cyto[d.ccur], (R*)d.cyto[1 - d.ccur], d.cin);
@@ -529,7 +556,7 @@ cudaError_t cb_plain_reset(cb_dev& d, cudaStream_t st) {
 cudaError_t cb_plain_init_opening(cb_dev& d, const int* d_first, int lo, int hi, cudaStream_t st) {
     int n = hi - lo;
     if (n <= 0) return cudaSuccess;
-    k_init_open<<<(n + 127) / 128, 128, 0, st>>>(d.sites, d_first, lo, hi, d.sc, d.ch_state);
+    k_init_open<<<(n + 127) / 128, 128, 0, st>>>(d.sites, d_first, lo, hi, d.sc, d.ch_state, d.ch_micro, d.mwc);
     return cudaGetLastError();
 }
 

@@ -246,6 +246,7 @@ bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* 
         return false;
     };
     if (!species_supported(d.m)) return no("species layout not specialised (1-2 ions, at most 4 ion-buffer pairs)");
+    if (d.m.ch_model == CB_SINGLE_SITE_MWC) return no("60-state RyR gating runs on the plain path");
     if (2 * d.max_ch > WINDOW) return no("more than 256 RyRs in a site");
     std::vector<cb_site> sites(d.S);
     if (cudaMemcpy(sites.data(), d.sites, sizeof(cb_site) * d.S, cudaMemcpyDeviceToHost) != cudaSuccess) return no("cudaMemcpy");

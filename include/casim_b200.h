@@ -134,6 +134,10 @@ casim_status casim_b200_set_field(casim_h h, int32_t site, int32_t species, cons
 casim_status casim_b200_get_mouth(casim_h h, int32_t site, int32_t species, double* out);
 /* DyadSeries::GetChannelsStates (CaSim/DyadSeries.h:30): 0/1 per RyR. */
 casim_status casim_b200_get_states(casim_h h, int32_t site, int32_t* out);
+/* 60-state RyR models (SingleSiteMWC, CaSim/SingleSiteMWC.cpp): the micro-state
+ * 0..59 of each RyR of the site (states 45-59 open); casim_b200_get_states gives
+ * the open flags. EINVAL for two-state models. */
+casim_status casim_b200_get_micro_states(casim_h h, int32_t site, int32_t* out);
 /* Overwrites the open (1) / closed (0) state of every RyR of the batch
  * (site-major, as casim_b200_get_all_states returns them) without consuming
  * draws; call casim_b200_update afterwards so the currents follow. Generalises

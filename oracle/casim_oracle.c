@@ -153,7 +153,8 @@ typedef struct {
     double* evo_i;
     double* evo_p;
     double* cur;   /* [n_ions][N] currents grid */
-    int* state;    /* [n_ch] */
+    int* state;    /* [n_ch] open (1) / closed (0) */
+    int* micro;    /* [n_ch] SingleSiteMWC micro-state 0..59 */
     double* mouth; /* [(n_ions + n_pairs + n_buf)][n_ch] */
     double efflux[OR_MAX_IONS + OR_MAX_PAIRS];
     double total[OR_MAX_IONS];
@@ -176,7 +177,187 @@ struct or_sim {
     or_model m;
     int S;
     site_t* site;
+    /* SingleSiteMWC: adjacency lists and the stationary distribution at the initial ions */
+    int mwc_nadj[60], mwc_adj[60][6];
+    double mwc_p[60];
 };
+
+/* ------------------------------------------------ SingleSiteMWC (60 states)
+ * CaSim/SingleSiteMWC.cpp with QMatrixModel (CaSim/QMatrixModel.cpp). Parameter slots
+ * of ch_par: fCa4I fCa KCa alphaCa konCa fMg KMg konMg alphaMg alphaMgI KO0 alphakco
+ * alphakcoI kco KMgI konmgI fICa fIMg gMg gCa. */
+static int mwc_index(int i, int j) { return 15 - (6 - j) * (5 - j) / 2 + i; }
+
+/* the entries of the four blocks' rows for occupancy (i Ca, j Mg), SetRow
+ * (CaSim/SingleSiteMWC.cpp:100-151) */
+static void mwc_set_row(const double* P, int i, double ca, int j, double mg, double Q[60][60]) {
+    double fCa4I = P[0], fCa = P[1], KCa = P[2], alphaCa = P[3], konCa = P[4], fMg = P[5], KMg = P[6], konMg = P[7];
+    double alphaMg = P[8], alphaMgI = P[9], KO0 = P[10], alphakco = P[11], alphakcoI = P[12], kco = P[13], KMgI = P[14];
+    double konMgI = P[15], fICa = P[16], fIMg = P[17], gMg = P[18], gCa = P[19];
+    double koffCa = KCa * konCa, koffMg = konMg * KMg, koc = KO0 * kco, koffMgI = KMgI * KMgI * konMgI;
+    double ff = pow(fCa, i) * pow(fMg, j);
+    double fIco = pow(fICa, i) * pow(fIMg, j);
+    int c = mwc_index(i, j), c2;
+    if (i + j < 4) {
+        c2 = mwc_index(i + 1, j);
+        Q[c][c2] = (4 - i - j) * konCa * ca;
+        Q[c + 45][c2 + 45] = (4 - i - j) * konCa * ca / pow(fCa, alphaCa);
+        Q[c + 15][c2 + 15] = (4 - i - j) * konCa * ca;
+        Q[c + 30][c2 + 30] = (4 - i - j) * konCa * ca / pow(i == 3 ? fCa4I : fICa, alphaCa);
+    }
+    if (i > 0) {
+        c2 = mwc_index(i - 1, j);
+        Q[c][c2] = i * koffCa;
+        Q[c + 45][c2 + 45] = i * koffCa * pow(fCa, 1 - alphaCa);
+        Q[c + 15][c2 + 15] = i * koffCa * gCa;
+        Q[c + 30][c2 + 30] = i * koffCa * pow(i == 4 ? fCa4I : fICa, 1 - alphaCa) * gCa;
+    }
+    if (i + j < 4) {
+        c2 = mwc_index(i, j + 1);
+        Q[c][c2] = (4 - i - j) * konMg * mg;
+        Q[c + 45][c2 + 45] = (4 - i - j) * konMg * mg / pow(fMg, alphaMg);
+        Q[c + 15][c2 + 15] = (4 - i - j) * konMg * mg / pow(gMg, alphaMgI);
+        Q[c + 30][c2 + 30] = (4 - i - j) * konMg * mg / (pow(fIMg, alphaMg) * pow(gMg, alphaMgI));
+    }
+    if (j > 0) {
+        c2 = mwc_index(i, j - 1);
+        Q[c][c2] = j * koffMg;
+        Q[c + 45][c2 + 45] = j * koffMg * pow(fMg, 1 - alphaMg);
+        Q[c + 15][c2 + 15] = j * koffMg * pow(gMg, 1 - alphaMgI);
+        Q[c + 30][c2 + 30] = j * koffMg * pow(fIMg, 1 - alphaMg) * pow(gMg, 1 - alphaMgI);
+    }
+    Q[c][c + 15] = konMgI * pow(mg, 2) / pow(gMg, j);
+    Q[c + 15][c] = koffMgI * pow(gCa, i);
+    Q[c + 45][c + 30] = konMgI * pow(mg, 2) / pow(fIMg / fMg * gMg, j);
+    if (i == 4)
+        Q[c + 30][c + 45] = koffMgI * pow(fICa / fCa * gCa, 3) * fCa4I / fCa;
+    else
+        Q[c + 30][c + 45] = koffMgI * pow(fICa / fCa * gCa, i);
+    Q[c][c + 45] = kco / pow(ff, alphakco);
+    Q[c + 45][c] = koc * pow(ff, 1 - alphakco);
+    if (i == 4) fIco = pow(fICa, 3) * fCa4I;
+    Q[c + 15][c + 30] = kco / pow(fIco, alphakcoI);
+    Q[c + 30][c + 15] = koc * pow(fIco, 1 - alphakcoI);
+}
+
+/* adjacency lists in the order CaSim/SingleSiteMWC.cpp:55-89 builds them */
+static void mwc_adjacency(or_sim* s) {
+    for (int k = 0; k < 60; ++k) s->mwc_nadj[k] = 0;
+#define MWC_PUSH(x, y) (s->mwc_adj[x][s->mwc_nadj[x]++] = (y))
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5 - i; ++j) {
+            int c = mwc_index(i, j);
+            int nb[4], n = 0;
+            if (i + j < 4) nb[n++] = mwc_index(i + 1, j);
+            if (i > 0) nb[n++] = mwc_index(i - 1, j);
+            if (i + j < 4) nb[n++] = mwc_index(i, j + 1);
+            if (j > 0) nb[n++] = mwc_index(i, j - 1);
+            for (int k = 0; k < n; ++k) {
+                MWC_PUSH(c, nb[k]);
+                MWC_PUSH(c + 45, nb[k] + 45);
+                MWC_PUSH(c + 15, nb[k] + 15);
+                MWC_PUSH(c + 30, nb[k] + 30);
+            }
+            MWC_PUSH(c, c + 15);
+            MWC_PUSH(c + 15, c);
+            MWC_PUSH(c + 45, c + 30);
+            MWC_PUSH(c + 30, c + 45);
+            MWC_PUSH(c, c + 45);
+            MWC_PUSH(c + 45, c);
+            MWC_PUSH(c + 15, c + 30);
+            MWC_PUSH(c + 30, c + 15);
+        }
+#undef MWC_PUSH
+}
+
+/* (i, j) of micro-state s (CaSim/SingleSiteMWC.cpp:156-168) */
+static void mwc_occupancy(int s, int* i, int* j) {
+    int r = s % 15;
+    for (int jj = 0; jj <= 4; ++jj) {
+        if (r - (5 - jj) < 0) {
+            *i = r;
+            *j = jj;
+            return;
+        }
+        r -= 5 - jj;
+    }
+    *i = 0;
+    *j = 4;
+}
+
+/* escape rate of s and its row over the adjacency list (GetRate, CaSim/QMatrixModel.cpp:20-24) */
+static double mwc_row(const or_sim* s, int st, double ca, double mg, double* row) {
+    static __thread double Q[60][60];
+    int i, j;
+    mwc_occupancy(st, &i, &j);
+    mwc_set_row(s->m.ch_par, i, ca, j, mg, Q);
+    double r = 0;
+    for (int k = 0; k < s->mwc_nadj[st]; ++k) {
+        row[k] = Q[st][s->mwc_adj[st][k]];
+        r += row[k];
+    }
+    return r;
+}
+
+/* stationary distribution of the full Q at (ca, mg): the least-squares solution of
+ * p [Q | 1] = [0 | 1], i.e. (S S^T) p = 1 with S = [Q | 1] (CaSim/QMatrixModel.cpp:38-47),
+ * by Gaussian elimination with partial pivoting */
+static void mwc_stationary(or_sim* s, double ca, double mg) {
+    static double Q[60][60], M[60][60], b[60];
+    memset(Q, 0, sizeof(Q));
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5 - i; ++j) mwc_set_row(s->m.ch_par, i, ca, j, mg, Q);
+    for (int r = 0; r < 60; ++r) {
+        double sum = 0;
+        for (int k = 0; k < s->mwc_nadj[r]; ++k) sum += Q[r][s->mwc_adj[r][k]];
+        Q[r][r] = -sum;
+    }
+    for (int a = 0; a < 60; ++a) {
+        for (int c = 0; c < 60; ++c) {
+            double v = 1.0;
+            for (int k = 0; k < 60; ++k) v += Q[a][k] * Q[c][k];
+            M[a][c] = v;
+        }
+        b[a] = 1.0;
+    }
+    for (int c = 0; c < 60; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 60; ++r)
+            if (fabs(M[r][c]) > fabs(M[piv][c])) piv = r;
+        if (piv != c) {
+            for (int k = 0; k < 60; ++k) {
+                double t = M[c][k];
+                M[c][k] = M[piv][k];
+                M[piv][k] = t;
+            }
+            double t = b[c];
+            b[c] = b[piv];
+            b[piv] = t;
+        }
+        for (int r = c + 1; r < 60; ++r) {
+            double f = M[r][c] / M[c][c];
+            if (f == 0) continue;
+            for (int k = c; k < 60; ++k) M[r][k] -= f * M[c][k];
+            b[r] -= f * b[c];
+        }
+    }
+    for (int r = 59; r >= 0; --r) {
+        double v = b[r];
+        for (int k = r + 1; k < 60; ++k) v -= M[r][k] * s->mwc_p[k];
+        s->mwc_p[r] = v / M[r][r];
+    }
+}
+
+/* SetMacroState (CaSim/QMatrixModel.cpp:48-58): a micro-state of macro state `open` */
+static int mwc_macro_pick(const or_sim* s, int open, double u, int cur) {
+    double total = 0, acc = 0;
+    for (int i = 0; i < 60; ++i) total += ((i >= 45) == open) * s->mwc_p[i];
+    for (int i = 0; i < 60; ++i) {
+        acc += ((i >= 45) == open) * s->mwc_p[i];
+        if (acc / total >= u) return i;
+    }
+    return cur;
+}
 
 static inline long IDX(const site_t* t, int x, int y, int z) { return z + (long)t->nz * (y + (long)t->ny * x); }
 
@@ -210,6 +391,7 @@ or_sim* or_create(const or_model* m, int n_sites, const int* nx, const int* ny, 
         t->evo_p = (double*)calloc((size_t)(m->n_pairs * t->N + 1), sizeof(double));
         t->cur = (double*)calloc((size_t)(m->n_ions * t->N), sizeof(double));
         t->state = (int*)calloc((size_t)(t->n_ch + 1), sizeof(int));
+        t->micro = (int*)calloc((size_t)(t->n_ch + 1), sizeof(int));
         t->mouth = (double*)calloc((size_t)((m->n_ions + m->n_pairs + m->n_buf) * (t->n_ch + 1)), sizeof(double));
         for (int i = 0; i < 6; ++i) t->rng.s[i] = seeds[6 * k + i];
         for (int i = 0; i < m->n_ions; ++i) t->jsr0[i] = jsr_init ? jsr_init[(long)k * m->n_ions + i] : m->jsr0[i];
@@ -236,6 +418,12 @@ or_sim* or_create(const or_model* m, int n_sites, const int* nx, const int* ny, 
                 }
         }
     }
+    if (m->ch_model == OR_SINGLE_SITE_MWC) {
+        /* InitOpening reads the channel map's initial values: the ions' concentrations
+           (CaSim/DyadChannels.h:25-58) */
+        mwc_adjacency(s);
+        mwc_stationary(s, m->Cb_ion[m->ca_idx], m->Cb_ion[m->mg_idx]);
+    }
     return s;
 }
 
@@ -245,7 +433,7 @@ void or_destroy(or_sim* s) {
         site_t* t = &s->site[k];
         free(t->cx); free(t->cy); free(t->cz);
         free(t->ions); free(t->pairs); free(t->freeb); free(t->evo_i); free(t->evo_p);
-        free(t->cur); free(t->state); free(t->mouth);
+        free(t->cur); free(t->state); free(t->micro); free(t->mouth);
         free(t->cf); free(t->cf_prev); free(t->cf_evo); free(t->cf_in); free(t->rim_map);
     }
     free(s->site);
@@ -326,12 +514,20 @@ static double runif(site_t* t) {
  * draw each, then the chosen channel opened with one more draw) */
 void or_init_opening(or_sim* s, int site, int channel) {
     site_t* t = &s->site[site];
+    const int mwc = s->m.ch_model == OR_SINGLE_SITE_MWC;
     for (int c = 0; c < t->n_ch; ++c) {
-        (void)runif(t);
+        double u = runif(t);
         t->state[c] = 0;
+        if (mwc) t->micro[c] = mwc_macro_pick(s, 0, u, t->micro[c]);
     }
-    (void)runif(t);
-    if (channel >= 0 && channel < t->n_ch) t->state[channel] = 1;
+    double u = runif(t);
+    if (channel >= 0 && channel < t->n_ch) {
+        t->state[channel] = 1;
+        if (mwc) {
+            t->micro[channel] = mwc_macro_pick(s, 1, u, t->micro[channel]);
+            t->state[channel] = t->micro[channel] >= 45;
+        }
+    }
 }
 
 /* ---------------------------------------------------------------- rates */
@@ -604,12 +800,30 @@ static void sr_run(const or_model* m, site_t* t, double dt) {
 }
 
 /* CaSim/DyadChannels.cpp:97-130 for two-state models */
-static void run_mc(const or_model* m, site_t* t, double dt) {
+static void run_mc(const or_sim* s, const or_model* m, site_t* t, double dt) {
     int nsp = m->n_ions + m->n_pairs + m->n_buf;
     double mi[OR_MAX_IONS];
     (void)nsp;
     for (int c = 0; c < t->n_ch; ++c) {
         for (int j = 0; j < m->n_ions; ++j) mi[j] = t->mouth[j * t->n_ch + c];
+        if (m->ch_model == OR_SINGLE_SITE_MWC) {
+            /* QMatrixModel::GetRate / MakeTransition (CaSim/QMatrixModel.cpp:20-36) */
+            double row[6];
+            int st = t->micro[c];
+            double r = mwc_row(s, st, mi[m->ca_idx], mi[m->mg_idx], row);
+            if (runif(t) < r * dt) {
+                double u = runif(t), acc = 0;
+                for (int k = 0; k < s->mwc_nadj[st]; ++k) {
+                    acc += row[k];
+                    if (acc / r >= u) {
+                        t->micro[c] = s->mwc_adj[st][k];
+                        break;
+                    }
+                }
+                t->state[c] = t->micro[c] >= 45;
+            }
+            continue;
+        }
         double r = rate(m, t->state[c], mi, t->jsr_new);
         if (runif(t) < r * dt) {
             (void)runif(t);
@@ -758,7 +972,7 @@ void or_step(or_sim* s, long n_steps, int n_threads) {
             else cyto_rd3d(m, t, m->dt);
             dyad_rd(m, t, m->dt);
             sr_run(m, t, m->dt);
-            run_mc(m, t, m->dt);
+            run_mc(s, m, t, m->dt);
             dyad_update(m, t);
             sr_update(m, t, ve);
         }
@@ -786,6 +1000,11 @@ void or_get_mouth(const or_sim* s, int site, int species, double* out) {
 void or_get_states(const or_sim* s, int site, int* out) {
     const site_t* t = &s->site[site];
     memcpy(out, t->state, sizeof(int) * (size_t)t->n_ch);
+}
+
+void or_get_micro(const or_sim* s, int site, int* out) {
+    const site_t* t = &s->site[site];
+    memcpy(out, t->micro, sizeof(int) * (size_t)t->n_ch);
 }
 
 void or_get_jsr(const or_sim* s, int site, double* out) {

@@ -22,7 +22,7 @@
 
 /* gating models (CaSim/PassiveIonChannel.cpp:10-26) */
 enum { OR_SHEEP_CANNELL = 0, OR_TWO_STATE_MWC = 1, OR_TWO_STATE_AHTG = 2, OR_TWO_STATE_SPLINE = 3,
-       OR_FOUR_STATE_MWC = 4 };
+       OR_FOUR_STATE_MWC = 4, OR_SINGLE_SITE_MWC = 5 };
 /* cytosol models */
 enum { OR_CYTO_POOL = 0, OR_CYTO_RD3D = 1 };
 
@@ -94,6 +94,8 @@ long or_site_nodes(const or_sim* s, int site);
 void or_get_field(const or_sim* s, int site, int species, double* out);
 void or_get_mouth(const or_sim* s, int site, int species, double* out);
 void or_get_states(const or_sim* s, int site, int* out);
+/* SingleSiteMWC: micro-states 0..59 (45-59 open) */
+void or_get_micro(const or_sim* s, int site, int* out);
 void or_get_jsr(const or_sim* s, int site, double* out);           /* n_ions */
 void or_get_total_current(const or_sim* s, int site, double* out); /* n_ions */
 void or_get_efflux(const or_sim* s, int site, double* out);        /* n_ions + n_pairs */

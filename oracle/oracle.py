@@ -24,7 +24,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
 MAX_IONS, MAX_BUF, MAX_PAIRS, MAX_CBUF, MAX_CPAIRS, MAX_CHPAR, MAX_SPLINE = 4, 8, 16, 12, 24, 32, 1024
-SHEEP_CANNELL, TWO_STATE_MWC, TWO_STATE_AHTG, TWO_STATE_SPLINE, FOUR_STATE_MWC = 0, 1, 2, 3, 4
+SHEEP_CANNELL, TWO_STATE_MWC, TWO_STATE_AHTG, TWO_STATE_SPLINE, FOUR_STATE_MWC, SINGLE_SITE_MWC = 0, 1, 2, 3, 4, 5
 CYTO_POOL, CYTO_RD3D = 0, 1
 
 _D = ctypes.c_double
@@ -247,6 +247,12 @@ def build_model(params):
         for w, key in enumerate(("Kopen filename", "Kclose filename")):
             tab = np.loadtxt(ch[key]).reshape(-1, 2)
             _set_spline(m, w, tab[:, 0], tab[:, 1])
+    elif model == "SingleSiteMWC":
+        # CaSim/SingleSiteMWC.cpp:5-37 (names absent from the map read as 0)
+        m.ch_model = SINGLE_SITE_MWC
+        vals = [float(par.get(k, 0.0)) for k in ("fCa4I", "fCa", "KCa", "alphaCa", "konCa", "fMg", "KMg", "konMg", "alphaMg",
+                                                 "alphaMgI", "KO0", "alphakco", "alphakcoI", "kco", "KMgI", "konmgI", "fICa",
+                                                 "fIMg", "gMg", "gCa")]
     else:
         raise ValueError("gating model not supported by the oracle: " + model)
     for k, v in enumerate(vals):
@@ -327,6 +333,7 @@ def _lib():
     for f in ("or_get_field", "or_get_mouth"):
         getattr(L, f).argtypes = [vp, _I, _I, dp]
     L.or_get_states.argtypes = [vp, _I, ip]
+    L.or_get_micro.argtypes = [vp, _I, ip]
     for f in ("or_get_jsr", "or_get_total_current", "or_get_efflux", "or_get_cyto"):
         getattr(L, f).argtypes = [vp, _I, dp]
     L.or_get_cyto_field.argtypes = [vp, _I, _I, dp]
@@ -433,6 +440,11 @@ class OracleSim:
     def states(self, site):
         out = np.zeros(int(self.nch[site]), dtype=np.int32)
         lib().or_get_states(self.h, site, _p(out, _I))
+        return out
+
+    def micro_states(self, site):
+        out = np.zeros(int(self.nch[site]), dtype=np.int32)
+        lib().or_get_micro(self.h, site, _p(out, _I))
         return out
 
     def _vec(self, fn, site, n):

@@ -39,3 +39,24 @@ def test_config1_like_site_matches_reference(dim, tmp_path):
     assert np.array_equal(r.get("dyad:Calcium"), o.field(0, 0))
     assert np.array_equal(r.states(), o.states(0))
     assert r.get("sr")[0] == o.jsr(0)[0]
+
+
+def test_single_site_mwc_site_matches_reference(tmp_path):
+    """60-state gating (CaSim/SingleSiteMWC.cpp): the micro-state trajectory of every RyR
+    is the reference's (initial draws from the stationary distribution included) and the
+    fields agree to rounding (two ions change the reference's summation order)."""
+    params, sites = configs.config1(n_sites=1, seed0=9, nx=24, ny=28, n_ryr=6)
+    params = configs.with_single_site_mwc(params, speed=20.0)
+    r, o = _run_both(params, sites, 0, tmp_path)
+    assert np.array_equal(r.states(), o.micro_states(0))
+    changed = 0
+    for _ in range(8):
+        before = o.micro_states(0)
+        r.step(200)
+        o.step(200)
+        assert np.array_equal(r.states(), o.micro_states(0))
+        changed += int(np.sum(before != o.micro_states(0)))
+        a, b = r.get("dyad:Calcium"), o.field(0, 0)
+        assert np.max(np.abs(a - b)) <= 1e-11 * np.max(np.abs(b))
+    assert changed >= 10  # the run does make transitions
+    assert np.array_equal(o.states(0), (o.micro_states(0) >= 45).astype(np.int32))

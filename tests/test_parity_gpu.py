@@ -202,3 +202,32 @@ def test_runs_are_deterministic(cuda_device, path):
         out.append([sim.field(s, 0) for s in range(3)] + [sim.states(s) for s in range(3)])
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+def test_single_site_mwc_gating_matches_oracle(cuda_device):
+    """60-state RyR gating (CaSim/SingleSiteMWC.cpp) on the device: the micro-state of
+    every RyR and the draw count follow the oracle (pinned against the reference in
+    test_oracle_live_ref.py) step for step; the model runs on the plain path."""
+    params, sites = configs.config1(n_sites=4, seed0=5, nx=24, ny=28, n_ryr=6)
+    params = configs.with_single_site_mwc(params, speed=20.0)
+    sim = cb.ReleaseSiteBatch(params, sites, precision="fp64", path="auto")
+    assert sim.path == "plain"
+    orc = oracle.OracleSim(params, sites)
+    sim.start(sites["first_channel"])
+    orc.start(sites["first_channel"])
+    moved = 0
+    for chunk in (0, 1, 199, 800, 600):
+        before = [orc.micro_states(s) for s in range(4)]
+        sim.step(chunk)
+        orc.step(chunk)
+        for s in range(4):
+            assert np.array_equal(sim.micro_states(s), orc.micro_states(s)), (chunk, s)
+            assert np.array_equal(sim.states(s), orc.states(s))
+            assert sim.draws(s) == orc.draws(s)
+            moved += int(np.sum(before[s] != orc.micro_states(s)))
+            assert rel_err(sim.field(s, 0), orc.field(s, 0)) <= 1e-11
+    assert moved >= 20
+    sim.close()
+    with pytest.raises(cb.CasimError) as e:
+        cb.ReleaseSiteBatch(params, sites, precision="fp64", path="resident")
+    assert e.value.status == cb.EUNSUPPORTED
