@@ -44,8 +44,14 @@ EXPORTS = (
     "casim_b200_sg_get_params", "casim_b200_sg_set_params", "casim_b200_sg_forward", "casim_b200_sg_gradients",
     "casim_b200_sg_train_step", "casim_b200_sg_check", "casim_b200_sg_launches", "casim_b200_sg_last_error",
     "casim_b200_sg_gemm", "casim_b200_trace_enable", "casim_b200_trace_count", "casim_b200_get_open_traces",
-    "casim_b200_release_analysis", "casim_b200_get_micro_states",
+    "casim_b200_release_analysis", "casim_b200_get_micro_states", "casim_b200_sg_hybrid_run",
 )
+
+
+class HybridStats(ctypes.Structure):
+    """casim_sg_hybrid_stats"""
+    _fields_ = [("surrogate_steps", ctypes.c_int64), ("rd_steps", ctypes.c_int64), ("checks", ctypes.c_int64),
+                ("fallbacks", ctypes.c_int64), ("last_residual", ctypes.c_double), ("last_fail_fraction", ctypes.c_double)]
 
 
 class CasimError(RuntimeError):
@@ -117,6 +123,8 @@ def lib():
         L.casim_b200_sg_set_mouth.argtypes = [vp, vp, i32, ctypes.c_double]
         L.casim_b200_sg_gate_steps.argtypes = [vp, i64]
         L.casim_b200_sg_run.argtypes = [vp, vp, i32, i64, i32, ctypes.c_double]
+        L.casim_b200_sg_hybrid_run.argtypes = [vp, vp, i32, i64, i32, i32, i32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                               ctypes.POINTER(HybridStats)]
         L.casim_b200_last_step_ms.argtypes = [vp, dp]
         L.casim_b200_last_step_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.casim_b200_debug_rng.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]

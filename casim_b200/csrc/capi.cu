@@ -35,6 +35,7 @@ struct casim_b200_sim {
     void* sg_net = nullptr;
     const void* sg_out = nullptr;  // the network's output buffer when the window was captured
     cudaGraphExec_t sg_exec = nullptr;
+    unsigned long long* sg_res = nullptr;  // residual check: max error bits, failing sites
     // open-RyR traces: [site][tr_max] u16, a sample every tr_every steps of casim_b200_step
     uint16_t* tr = nullptr;
     long long tr_every = 0, tr_max = 0, tr_n = 0, tr_phase = 0;
@@ -283,6 +284,7 @@ casim_status casim_b200_destroy(casim_h h) {
     cb_resident_free(h->d);
     if (h->sg_exec) cudaGraphExecDestroy(h->sg_exec);
     if (h->tr) cudaFree(h->tr);
+    if (h->sg_res) cudaFree(h->sg_res);
     if (h->sg_x) cudaFree(h->sg_x);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -692,8 +694,10 @@ cudaError_t sg_window(casim_h h, casim_sg net, double ca_ref, int window) {
 
 }  // namespace
 
-casim_status casim_b200_sg_run(casim_h h, casim_sg net, int32_t max_channels, int64_t n, int32_t window, double ca_ref) {
-    GUARD(h)
+namespace {
+
+// n steps of surrogate-driven gating in windows (one window captured as a CUDA graph)
+void sg_windows(casim_h h, casim_sg net, int max_channels, long long n, int window, double ca_ref) {
     if (!net || n < 0 || window < 1 || !(ca_ref > 0) || max_channels < 1) throw std::runtime_error("bad surrogate run arguments");
     if (h->d.m.cyto_type != CB_CYTO_POOL) throw std::runtime_error("surrogate gating needs the pool cytosol");
     if (h->d.m.ch_model == CB_SINGLE_SITE_MWC) throw std::runtime_error("surrogate gating serves two-state RyR models");
@@ -739,6 +743,9 @@ casim_status casim_b200_sg_run(casim_h h, casim_sg net, int32_t max_channels, in
         }
         done += k;
     }
+}
+
+casim_status sg_net_status(casim_h h, casim_sg net) {
     ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
     const cudaError_t en = cb_sg_net_error(net);
     if (en == cudaErrorLaunchTimeout) {
@@ -747,6 +754,69 @@ casim_status casim_b200_sg_run(casim_h h, casim_sg net, int32_t max_channels, in
     }
     ck(en, "surrogate network");
     return CASIM_OK;
+}
+
+void rd_steps(casim_h h, long long n) {
+    long long launches = 0;
+    if (h->path == CASIM_PATH_RESIDENT) ck(cb_resident_step(h->d, n, h->stream, &launches), "resident step");
+    else ck(cb_plain_step(h->d, n, h->stream, &launches), "plain step");
+}
+
+}  // namespace
+
+casim_status casim_b200_sg_run(casim_h h, casim_sg net, int32_t max_channels, int64_t n, int32_t window, double ca_ref) {
+    GUARD(h)
+    sg_windows(h, net, max_channels, n, window, ca_ref);
+    return sg_net_status(h, net);
+    END_GUARD(h)
+}
+
+casim_status casim_b200_sg_hybrid_run(casim_h h, casim_sg net, int32_t max_channels, int64_t n, int32_t window,
+                                      int32_t windows_per_check, int32_t rd_correction_steps, double tol, double max_fail_fraction,
+                                      double ca_ref, casim_sg_hybrid_stats* stats) {
+    GUARD(h)
+    if (windows_per_check < 1 || rd_correction_steps < 1 || !(tol > 0) || !(max_fail_fraction >= 0) || n < 0)
+        throw std::runtime_error("bad hybrid run arguments");
+    casim_sg_hybrid_stats st{};
+    if (!h->sg_res) {
+        void* p = nullptr;
+        ck(cudaMalloc(&p, 2 * sizeof(unsigned long long)), "cudaMalloc");
+        h->sg_res = (unsigned long long*)p;
+    }
+    bool surrogate = true;
+    long long done = 0;
+    const long long period = (long long)windows_per_check * window;
+    while (done < n) {
+        const long long k = std::min(period, n - done);
+        if (surrogate) {
+            sg_windows(h, net, max_channels, k, window, ca_ref);
+            st.surrogate_steps += k;
+        } else {
+            rd_steps(h, k);
+            st.rd_steps += k;
+        }
+        done += k;
+        if (done >= n) break;
+        // full-RD correction, then the residual check of the network against it
+        const long long c = std::min<long long>(rd_correction_steps, n - done);
+        rd_steps(h, c);
+        st.rd_steps += c;
+        done += c;
+        const float* y = nullptr;
+        int ld = 0;
+        ck(cb_sg_features(h->d, h->sg_maxch, h->sg_ld, h->sg_x, h->stream), "surrogate features");
+        ck(cb_sg_net_forward(net, h->sg_x, h->sg_rows, h->stream, &y, &ld), "surrogate forward");
+        double worst = 0, frac = 0;
+        ck(cb_sg_residual(h->d, y, ld, ca_ref, tol, h->sg_res, &worst, &frac, h->stream), "residual check");
+        ++st.checks;
+        st.last_residual = worst;
+        st.last_fail_fraction = frac;
+        surrogate = frac <= max_fail_fraction;
+        if (!surrogate) ++st.fallbacks;
+    }
+    const casim_status r = sg_net_status(h, net);
+    if (stats) *stats = st;
+    return r;
     END_GUARD(h)
 }
 

@@ -62,6 +62,11 @@ cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* la
 cudaError_t cb_sg_features(cb_dev& d, int max_ch, int ld, float* X, cudaStream_t st);
 cudaError_t cb_sg_mouth(cb_dev& d, const float* Y, int ld, double ca_ref, cudaStream_t st);
 cudaError_t cb_sg_steps(cb_dev& d, long long n, cudaStream_t st);
+// residual check of the network's mouth Ca (Y) against the mouth Ca of the last RD Update at
+// the open RyRs: the largest per-site relative error and the fraction of sites above tol
+// (synchronises)
+cudaError_t cb_sg_residual(const cb_dev& d, const float* Y, int ld, double ca_ref, double tol, unsigned long long* scratch,
+                           double* worst, double* fail_fraction, cudaStream_t st);
 cudaError_t cb_sg_steps_warp(cb_dev& d, long long n, cudaStream_t st, bool* used);  // sg_gate.cu
 // analysis.cu: open-RyR trace sample j of every site; the release-event analysis of n samples
 cudaError_t cb_trace_record(const cb_dev& d, uint16_t* trace, long long max_samples, long long j, cudaStream_t st);

@@ -12,6 +12,7 @@
 // This is the straightforward GPU formulation of the reference step and the
 // denominator of the resident path's speed-up; it handles any site size.
 #include <algorithm>
+#include <cstring>
 
 #include "engine.h"
 #include "mrg32k3a.cuh"
@@ -583,6 +584,45 @@ cudaError_t cb_sg_features(cb_dev& d, int max_ch, int ld, float* X, cudaStream_t
 cudaError_t cb_sg_mouth(cb_dev& d, const float* Y, int ld, double ca_ref, cudaStream_t st) {
     k_sg_mouth<<<(d.S + 127) / 128, 128, 0, st>>>(d.S, d.NS, d.m.ca_idx, ca_ref, ld, d.sites, Y, d.mouth);
     return cudaGetLastError();
+}
+
+namespace {
+// per site: the largest relative error of the network's mouth Ca over its open RyRs (the
+// mouths whose Ca sets the release flux; a site with none open has error 0); the max over
+// sites (non-negative doubles order as their bit patterns) and the failing sites
+__global__ void k_sg_residual(int S, int NS, int ca_idx, double ca_ref, int ld, double tol, const cb_site* __restrict__ sites,
+                              const int* __restrict__ ch_state, const float* __restrict__ Y, const double* __restrict__ mouth,
+                              unsigned long long* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const cb_site st = sites[s];
+    double e = 0;
+    for (int c = 0; c < st.n_ch && c < ld; ++c) {
+        if (!ch_state[st.ch_off + c]) continue;
+        const double rd = mouth[(size_t)(st.ch_off + c) * NS + ca_idx];
+        const double pr = ca_ref * exp10((double)Y[(size_t)s * ld + c]);
+        const double r = fabs(pr - rd) / fabs(rd);
+        e = r > e ? r : (r != r ? INFINITY : e);
+    }
+    atomicMax(out, (unsigned long long)__double_as_longlong(e));
+    if (!(e <= tol)) atomicAdd(out + 1, 1ULL);
+}
+}  // namespace
+
+cudaError_t cb_sg_residual(const cb_dev& d, const float* Y, int ld, double ca_ref, double tol, unsigned long long* scratch,
+                           double* worst, double* fail_fraction, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 2 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    k_sg_residual<<<(d.S + 127) / 128, 128, 0, st>>>(d.S, d.NS, d.m.ca_idx, ca_ref, ld, tol, d.sites, d.ch_state, Y, d.mouth, scratch);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    unsigned long long h[2];
+    if ((e = cudaMemcpyAsync(h, scratch, sizeof(h), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    double w;
+    std::memcpy(&w, &h[0], sizeof(w));
+    *worst = w;
+    *fail_fraction = d.S ? (double)h[1] / d.S : 0.0;
+    return cudaSuccess;
 }
 
 cudaError_t cb_sg_steps(cb_dev& d, long long n, cudaStream_t st) {

@@ -200,6 +200,28 @@ def rd_snapshots(n_sites, seed=0, relax_steps=RELAX_STEPS, precision="fp32", n_r
     return X, Y, secs
 
 
+def dynamic_snapshots(n_sites, seed=0, every=1000, samples=20, precision="fp32"):
+    """Features and targets read from the plain RD method while it gates: config-1 sites
+    started from one random open RyR, sampled every `every` steps (`samples` times), so the
+    training set holds the open sets, jSR depletion and transient mouth Ca of real runs.
+    Returns (X [n_sites * samples, F], Y [n_sites * samples, 20])."""
+    from . import ReleaseSiteBatch
+    from . import configs
+    p, s = configs.config1(n_sites=n_sites, seed0=1000 + seed)
+    first = np.random.default_rng(seed).integers(0, 20, size=n_sites).astype(np.int32)
+    sim = ReleaseSiteBatch(p, s, precision=precision, path="auto")
+    sim.start(first)
+    Xs, Ys = [], []
+    for _ in range(samples):
+        sim.step(every)
+        sim.synchronize()
+        ca = sim.all_mouth(0).reshape(n_sites, 20)
+        Xs.append(device_features(sim, 20)[:n_sites].cpu().numpy())
+        Ys.append(np.log10(np.maximum(ca, 1e-6) / CA_REF_UM).astype(np.float32))
+    sim.close()
+    return np.concatenate(Xs), np.concatenate(Ys)
+
+
 def train(net, X, Y, steps, batch=4096, lr=1e-3, seed=0, lr_decay=True):
     """Adam on random mini-batches of (X, Y) held on the device; returns the loss history."""
     import torch
@@ -239,3 +261,16 @@ class SurrogateGating:
 
     def step(self, n):
         self.sim._ck(lib().casim_b200_sg_run(self.sim.h, self.net.h, self.max_ch, int(n), self.window, CA_REF_UM))
+
+    def hybrid_step(self, n, windows_per_check=10, rd_steps=20, tol=0.01, max_fail_fraction=0.0):
+        """n steps alternating surrogate periods (windows_per_check windows) with a
+        full-RD correction of rd_steps steps, a residual check of the network against
+        it (relative mouth-Ca error tol per site) and a fallback to the full RD method
+        for the next period when more than max_fail_fraction of the sites fail
+        (casim_b200_sg_hybrid_run). Returns the run's statistics."""
+        from . import HybridStats
+        st = HybridStats()
+        self.sim._ck(lib().casim_b200_sg_hybrid_run(self.sim.h, self.net.h, self.max_ch, int(n), self.window, int(windows_per_check),
+                                                    int(rd_steps), float(tol), float(max_fail_fraction), CA_REF_UM,
+                                                    ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in HybridStats._fields_}

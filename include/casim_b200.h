@@ -273,6 +273,26 @@ casim_status casim_b200_sg_gate_steps(casim_h h, int64_t n);
  * window is captured once into a CUDA graph and replayed. Returns after the
  * stream is idle. A network handle serves one such call at a time. */
 casim_status casim_b200_sg_run(casim_h h, casim_sg net, int32_t max_channels, int64_t n, int32_t window, double ca_ref);
+
+/* Surrogate gating with periodic full-RD corrections and a residual fallback (no
+ * counterpart in the reference). Time advances in periods of windows_per_check
+ * windows of `window` steps, each period followed by rd_correction_steps steps of the
+ * full RD method (the handle's path, gating included). After each correction the
+ * network is evaluated on the current open sets and jSR and compared with the mouth
+ * Ca the RD Update just produced: a site fails when the relative error at any of its
+ * open RyRs' mouths exceeds tol. If more than max_fail_fraction of the sites fail, the next
+ * period runs the full RD method instead of the surrogate (and is checked again
+ * after its correction); otherwise it runs the surrogate. The RD fields do not move
+ * during surrogate periods. stats (optional) counts the steps of each kind, the
+ * checks and the fallbacks, and holds the last check's largest error and failing
+ * fraction. */
+typedef struct casim_sg_hybrid_stats {
+    int64_t surrogate_steps, rd_steps, checks, fallbacks;
+    double last_residual, last_fail_fraction;
+} casim_sg_hybrid_stats;
+casim_status casim_b200_sg_hybrid_run(casim_h h, casim_sg net, int32_t max_channels, int64_t n_steps, int32_t window,
+                                      int32_t windows_per_check, int32_t rd_correction_steps, double tol, double max_fail_fraction,
+                                      double ca_ref, casim_sg_hybrid_stats* stats);
 /* One product C = A . B^T on the tensor cores: A [M][K] and B [N][K] BF16
  * (bit patterns), C [M][N] FP32, all device memory; M a multiple of 128,
  * N a multiple of 16 in [16, 256], K a multiple of 64. */

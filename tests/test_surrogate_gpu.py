@@ -110,6 +110,24 @@ def test_surrogate_learns_rd_snapshots_and_beats_rd_cost(cuda_device):
     net.close()
 
 
+_NET = []
+
+
+def _config1_net():
+    """A network trained on 32768 frozen-open-set RD snapshots of config-1 geometry
+    (trained once per test module)."""
+    if not _NET:
+        Xs, Ys = [], []
+        for b in range(8):
+            X, Y, _ = sg.rd_snapshots(4096, seed=200 + b)
+            Xs.append(X)
+            Ys.append(Y)
+        net = sg.Surrogate(Xs[0].shape[1], Ys[0].shape[1], seed=5)
+        sg.train(net, np.concatenate(Xs), np.concatenate(Ys), 3000, batch=8192, lr=2e-3)
+        _NET.append(net)
+    return _NET[0]
+
+
 def test_surrogate_gating_tracks_rd_open_counts_faster(cuda_device):
     """Sites of config-1 geometry run 1 ms from one open RyR with RD gating
     and with surrogate gating (network every 1 us, no RD step): the mean
@@ -120,13 +138,7 @@ def test_surrogate_gating_tracks_rd_open_counts_faster(cuda_device):
     import torch
     import casim_b200 as cb
     from casim_b200 import configs
-    Xs, Ys = [], []
-    for b in range(8):
-        X, Y, _ = sg.rd_snapshots(4096, seed=200 + b)
-        Xs.append(X)
-        Ys.append(Y)
-    net = sg.Surrogate(Xs[0].shape[1], Ys[0].shape[1], seed=5)
-    sg.train(net, np.concatenate(Xs), np.concatenate(Ys), 3000, batch=8192, lr=2e-3)
+    net = _config1_net()
     S, T = 2048, 19800
     p, s = configs.config1(n_sites=S)
     first = np.random.default_rng(5).integers(0, 20, size=S).astype(np.int32)
@@ -143,7 +155,6 @@ def test_surrogate_gating_tracks_rd_open_counts_faster(cuda_device):
         sim.synchronize()
         res[mode] = (time.time() - t0, sim.all_states().reshape(S, 20).sum(1).mean())
         sim.close()
-    net.close()
     (t_rd, n_rd), (t_sg, n_sg) = res["rd"], res["surrogate"]
     assert abs(n_sg - n_rd) <= 0.15 * n_rd, (n_rd, n_sg)
     assert t_sg < t_rd, (t_rd, t_sg)
@@ -180,3 +191,46 @@ def test_warp_gating_matches_one_thread_gating(cuda_device):
     assert np.array_equal(out[0][0], out[1][0])
     assert out[0][1] == out[1][1]
     assert sum(out[0][1]) > 8 * 20 * 4000  # transitions happened
+
+
+def test_hybrid_run_corrects_and_falls_back(cuda_device):
+    """Surrogate gating with a full-RD correction (20 steps) after every 10 windows and a
+    residual check at the open RyRs: with an unreachable tolerance every period after the
+    first falls back to the RD method and the run keeps the RD method's open-RyR and
+    release distributions; with no check it never falls back; with a 20 % tolerance on at
+    most 20 % of the sites it mixes both, runs faster than the RD method and keeps its
+    open-RyR distribution (the surrogate alone releases about 20 % more Ca)."""
+    import time
+    import torch
+    from scipy.stats import ks_2samp
+    import casim_b200 as cb
+    from casim_b200 import configs
+    net = _config1_net()
+    S, T = 2048, 19800
+    p, s = configs.config1(n_sites=S)
+    first = np.random.default_rng(5).integers(0, 20, size=S).astype(np.int32)
+    out = {}
+    for mode, hp in (("rd", None), ("strict", (10, 20, 0.01, 0.0)), ("none", (10, 20, 1e9, 0.0)), ("mixed", (10, 20, 0.2, 0.2))):
+        sim = cb.ReleaseSiteBatch(p, s, precision="fp32", path="auto")
+        sim.start(first)
+        gate = sg.SurrogateGating(net, sim, window=20)
+        run = sim.step if hp is None else (lambda n, hp=hp, gate=gate: gate.hybrid_step(n, *hp))
+        run(220)  # warm-up: plans, graph capture
+        sim.synchronize()
+        torch.cuda.synchronize()
+        t0 = time.time()
+        stats = run(T)
+        sim.synchronize()
+        out[mode] = (time.time() - t0, sim.all_states().reshape(S, 20).sum(1), np.array([sim.release(k) for k in range(S)]), stats)
+        sim.close()
+    t_rd, o_rd, r_rd, _ = out["rd"]
+    st = out["strict"][3]
+    assert st["checks"] == 90 and st["fallbacks"] == 90 and st["surrogate_steps"] == 200
+    assert ks_2samp(out["strict"][1], o_rd).pvalue > 0.05 and ks_2samp(out["strict"][2], r_rd).pvalue > 0.05
+    st = out["none"][3]
+    assert st["fallbacks"] == 0 and st["surrogate_steps"] == 18000 and st["rd_steps"] == 1800
+    t_mx, o_mx, r_mx, st = out["mixed"]
+    assert 0 < st["fallbacks"] < st["checks"], st
+    assert t_mx < t_rd, (t_rd, t_mx)
+    assert ks_2samp(o_mx, o_rd).pvalue > 0.05
+    assert abs(r_mx.mean() / r_rd.mean() - 1) < 0.1
