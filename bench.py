@@ -164,9 +164,11 @@ def surrogate_report(sites=2048, sim_steps=20000, batches=8, train_steps=4000):
     """Surrogate-gated versus plain-RD release sites on config-1 geometry: the
     network is trained on the device from RD snapshots (frozen open sets), its
     held-out mouth-Ca error is measured, then the same sites (same seeds, one
-    RyR opened) run 1 ms with RD gating and with surrogate gating (network
-    every 1 us, no RD step). Both arms are timed by wall clock around
-    synchronised device work."""
+    RyR opened) run 1 ms with RD gating, with surrogate gating (network
+    every 1 us, no RD step) and with the hybrid run (a 1 us full-RD correction
+    after every 10 us of surrogate gating, residual check at the open RyRs,
+    fallback to RD) at a 1 % and a 20 % tolerance. All arms are timed by wall
+    clock around synchronised device work."""
     import torch
     from scipy.stats import ks_2samp
     import casim_b200 as cb
@@ -183,22 +185,36 @@ def surrogate_report(sites=2048, sim_steps=20000, batches=8, train_steps=4000):
     rel = np.abs(10.0 ** sg.predict(net, Xv) - 10.0 ** Yv) / 10.0 ** Yv
     p, s = configs.config1(n_sites=sites)
     first = np.random.default_rng(5).integers(0, 20, size=sites).astype(np.int32)
-    out = {}
-    for mode in ("rd", "surrogate"):
+    out, stats = {}, {}
+    hybrid = {"hybrid_tol_1pct": (10, 20, 0.01, 0.0), "hybrid_tol_20pct": (10, 20, 0.2, 0.2)}
+    for mode in ("rd", "surrogate") + tuple(hybrid):
         sim = cb.ReleaseSiteBatch(p, s, precision="fp32", path="auto")
         sim.start(first)
+        gate = sg.SurrogateGating(net, sim, window=20)
         torch.cuda.synchronize()
         t0 = time.time()
         if mode == "rd":
             sim.step(sim_steps)
+        elif mode == "surrogate":
+            gate.step(sim_steps)
         else:
-            sg.SurrogateGating(net, sim, window=20).step(sim_steps)
+            stats[mode] = gate.hybrid_step(sim_steps, *hybrid[mode])
         sim.synchronize()
         el = time.time() - t0
         out[mode] = (sites * sim_steps * sim.info.dt_ms / el, sim.all_states().reshape(sites, -1).sum(1),
                      np.array([sim.release(k) for k in range(sites)]))
         sim.close()
     net.close()
+    hyb = {}
+    for mode, (wpc, rds, tol, frac) in hybrid.items():
+        st = stats[mode]
+        hyb[mode] = {"site_ms_per_s": out[mode][0], "speedup_vs_rd": out[mode][0] / out["rd"][0],
+                     "windows_per_check": wpc, "rd_correction_steps": rds, "tol": tol, "max_fail_fraction": frac,
+                     "surrogate_step_fraction": st["surrogate_steps"] / max(1, st["surrogate_steps"] + st["rd_steps"]),
+                     "fallbacks": st["fallbacks"], "checks": st["checks"],
+                     "open_count_ks_p": float(ks_2samp(out["rd"][1], out[mode][1]).pvalue),
+                     "release_ks_p": float(ks_2samp(out["rd"][2], out[mode][2]).pvalue),
+                     "release_mean_ratio": float(out[mode][2].mean() / out["rd"][2].mean())}
     return {"workload": "%d config-1 sites, 1 ms from one open RyR, fp32" % sites,
             "rd_site_ms_per_s": out["rd"][0], "surrogate_site_ms_per_s": out["surrogate"][0],
             "speedup": out["surrogate"][0] / out["rd"][0],
@@ -206,7 +222,8 @@ def surrogate_report(sites=2048, sim_steps=20000, batches=8, train_steps=4000):
             "open_count_ks_p": float(ks_2samp(out["rd"][1], out["surrogate"][1]).pvalue),
             "release_ks_p": float(ks_2samp(out["rd"][2], out["surrogate"][2]).pvalue),
             "release_mean_ratio": float(out["surrogate"][2].mean() / out["rd"][2].mean()),
-            "training": "%d RD snapshots (0.25 ms relaxation), %d Adam steps of 8192 on the device" % (X.shape[0], train_steps)}
+            "training": "%d RD snapshots (0.25 ms relaxation), %d Adam steps of 8192 on the device" % (X.shape[0], train_steps),
+            "hybrid": hyb}
 
 
 def params_dt_ms(params):
