@@ -44,7 +44,7 @@ EXPORTS = (
     "casim_b200_sg_get_params", "casim_b200_sg_set_params", "casim_b200_sg_forward", "casim_b200_sg_gradients",
     "casim_b200_sg_train_step", "casim_b200_sg_check", "casim_b200_sg_launches", "casim_b200_sg_last_error",
     "casim_b200_sg_gemm", "casim_b200_trace_enable", "casim_b200_trace_count", "casim_b200_get_open_traces",
-    "casim_b200_release_analysis", "casim_b200_get_micro_states", "casim_b200_sg_hybrid_run",
+    "casim_b200_release_analysis", "casim_b200_get_micro_states", "casim_b200_sg_hybrid_run", "casim_b200_autotune",
 )
 
 
@@ -112,6 +112,7 @@ def lib():
         L.casim_b200_set_field.argtypes = [vp, i32, i32, dp]
         L.casim_b200_get_states.argtypes = [vp, i32, ip]
         L.casim_b200_get_micro_states.argtypes = [vp, i32, ip]
+        L.casim_b200_autotune.argtypes = [vp, i64, ctypes.c_char_p, ctypes.c_size_t]
         for f in ("get_jsr", "get_total_current", "get_efflux", "get_cyto", "get_release"):
             getattr(L, "casim_b200_" + f).argtypes = [vp, i32, dp]
         L.casim_b200_get_draws.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_uint64)]
@@ -365,6 +366,12 @@ class ReleaseSiteBatch:
         return {"amp": per_site[:, 0], "ttp": per_site[:, 1], "tte": per_site[:, 2], "integral": per_site[:, 3],
                 "mean": per_site[:, 4], "hist": h_all, "hist_quark": h_q, "hist_blip": h_b, "hist_spark": h_s,
                 "quarks": int(counts[0]), "blips": int(counts[1]), "sparks": int(counts[2])}
+
+    def autotune(self, steps_per_trial=20):
+        """Choose block and cluster sizes by measurement (resident path); returns the choices."""
+        buf = ctypes.create_string_buffer(4096)
+        self._ck(lib().casim_b200_autotune(self.h, int(steps_per_trial), buf, 4096))
+        return buf.value.decode()
 
     def micro_states(self, site):
         """60-state RyR models: the micro-state 0..59 of each RyR (45-59 open)."""

@@ -514,6 +514,23 @@ casim_status casim_b200_release_analysis(casim_h h, double hist_dt_ms, double ma
     END_GUARD(h)
 }
 
+casim_status casim_b200_autotune(casim_h h, int64_t steps_per_trial, char* report, size_t n) {
+    GUARD(h)
+    if (steps_per_trial < 1) throw std::runtime_error("steps_per_trial must be >= 1");
+    std::string rep = "plain path: nothing to tune";
+    if (h->path == CASIM_PATH_RESIDENT) {
+        ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        ck(cb_resident_autotune(h->d, steps_per_trial, h->stream, &rep), "autotune");
+    }
+    if (report && n) {
+        const size_t k = std::min(n - 1, rep.size());
+        std::memcpy(report, rep.data(), k);
+        report[k] = 0;
+    }
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
 casim_status casim_b200_synchronize(casim_h h) {
     GUARD(h)
     ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");

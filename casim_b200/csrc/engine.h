@@ -83,6 +83,9 @@ const void* cb_sg_net_output(struct casim_surrogate_s* net);  // changes when it
 // resident path (resident.cu)
 bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* why);
 cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);
+// measured choice of block and cluster size per class (state unchanged); a description of
+// the choices into *report
+cudaError_t cb_resident_autotune(cb_dev& d, long long steps, cudaStream_t st, std::string* report);
 void cb_resident_free(cb_dev& d);
 // MRG32k3a jump table d.rs_pow2: A^(2^k), k < 64, then the ring-refill jump (resident.cu)
 cudaError_t cb_ensure_pow2(cb_dev& d);

@@ -456,3 +456,126 @@ cudaError_t cb_resident_step(cb_dev& d, long long n, cudaStream_t st, long long*
     }
     return cudaSuccess;
 }
+
+// ---------------------------------------------------------------- autotuning
+namespace {
+
+// the device state a resident launch reads and writes, copied aside and put back
+struct state_copy {
+    std::vector<std::pair<void*, size_t>> bufs;  // (live buffer, bytes)
+    std::vector<void*> saved;
+    cudaError_t take(const cb_dev& d) {
+        const size_t rs = d.precision == 0 ? 8 : 4;
+        bufs = {{d.fields[d.cur], (size_t)d.total_nodes * d.m.F * rs},
+                {d.curgrid, (size_t)d.total_nodes * d.m.n_ions * rs},
+                {d.ch_state, (size_t)d.total_ch * sizeof(int)},
+                {d.mouth, (size_t)d.total_ch * d.NS * sizeof(double)},
+                {d.sc, (size_t)d.S * sizeof(cb_site_scalars)}};
+        if (d.nc > 0) {
+            bufs.push_back({d.cyto[d.ccur], (size_t)d.S * d.CS * d.nc * rs});
+            bufs.push_back({d.cin, (size_t)d.S * d.CS * d.m.mc * d.m.mc * sizeof(double)});
+        }
+        for (auto& b : bufs) {
+            void* p = nullptr;
+            cudaError_t e = cudaMalloc(&p, b.second);
+            if (e != cudaSuccess) return e;
+            saved.push_back(p);
+            if ((e = cudaMemcpy(p, b.first, b.second, cudaMemcpyDeviceToDevice)) != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+    cudaError_t put_back(cudaStream_t st) {
+        for (size_t k = 0; k < bufs.size(); ++k) {
+            cudaError_t e = cudaMemcpyAsync(bufs[k].first, saved[k], bufs[k].second, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaStreamSynchronize(st);
+    }
+    ~state_copy() {
+        for (void* p : saved) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+// Block size and cluster size of every class chosen by measurement: each candidate runs
+// `steps` time steps of its class alone (the other classes idle) from the same state,
+// which is put back after every trial and at the end. Candidates: 256 to the
+// specialisation's bound in steps of 64 threads, at the class's cluster size and, where
+// the class's sites fit it, at twice that size.
+cudaError_t cb_resident_autotune(cb_dev& d, long long steps, cudaStream_t st, std::string* report) {
+    cudaError_t e;
+    if (!d.rs_plan && (e = build_plan(d)) != cudaSuccess) return e;
+    cb_rs_plan& P = *d.rs_plan;
+    if (steps < 1) return cudaErrorInvalidValue;
+    std::vector<cb_site> sites(d.S);
+    if ((e = cudaMemcpy(sites.data(), d.sites, sizeof(cb_site) * d.S, cudaMemcpyDeviceToHost)) != cudaSuccess) return e;
+    std::vector<std::vector<int>> classes;
+    std::vector<int> cs;
+    if (!classify(d, sites, classes, cs) || classes.size() != P.args.size()) return cudaErrorInvalidConfiguration;
+    state_copy snap;
+    if ((e = snap.take(d)) != cudaSuccess) return e;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::string rep;
+    for (size_t k = 0; k < P.args.size(); ++k) {
+        struct cand {
+            int C, threads, clusters;
+            rs_args a;
+            float ms;
+        };
+        std::vector<cand> cands;
+        for (int C : {cs[k], 2 * cs[k]}) {
+            if (C > 16) continue;
+            rs_args a = P.args[k];  // plan() rewrites only the shared-memory layout
+            if (C != cs[k] && !plan(d, sites, classes[k], C, a)) continue;
+            const int cap = thread_cap(d, P.nz, C);
+            for (int t = 256; t <= cap; t += 64) {
+                int clusters = 0;
+                if (launch_t(d, a, P.nz, C, t, 0, a.S, &clusters) != cudaSuccess || clusters < 1) {
+                    cudaGetLastError();
+                    continue;
+                }
+                cands.push_back({C, t, clusters, a, 0.f});
+            }
+        }
+        for (auto& c : cands) {
+            float best = 1e30f;
+            for (int rep_i = 0; rep_i < 2; ++rep_i) {  // the first run also loads the specialisation
+                rs_args a = c.a;
+                a.fields = d.fields[d.cur];
+                a.cyto = d.cyto[d.ccur];
+                a.nsteps = steps;
+                if ((e = cudaMemsetAsync(a.counter, 0, sizeof(int), st)) != cudaSuccess) return e;
+                cudaEventRecord(e0, st);
+                if ((e = launch_t(d, a, P.nz, c.C, c.threads, st, a.S, nullptr, c.clusters)) != cudaSuccess) return e;
+                cudaEventRecord(e1, st);
+                if ((e = cudaEventSynchronize(e1)) != cudaSuccess) return e;
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                best = std::min(best, ms);
+                if ((e = snap.put_back(st)) != cudaSuccess) return e;
+            }
+            c.ms = best;
+        }
+        if (cands.empty()) continue;
+        const cand* b = &cands[0];
+        for (auto& c : cands)
+            if (c.ms < b->ms) b = &c;
+        float cur_ms = -1;
+        for (auto& c : cands)
+            if (c.C == P.cs[k] && c.threads == P.threads[k]) cur_ms = c.ms;
+        rep += (k ? "; " : "") + std::to_string(classes[k].size()) + " sites: clusters of " + std::to_string(P.cs[k]) + " x " +
+               std::to_string(P.threads[k]) + " threads (" + std::to_string(cur_ms) + " ms) -> " + std::to_string(b->C) + " x " +
+               std::to_string(b->threads) + " (" + std::to_string(b->ms) + " ms)";
+        P.cs[k] = b->C;
+        P.threads[k] = b->threads;
+        P.clusters[k] = b->clusters;
+        P.args[k] = b->a;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (report) *report = rep;
+    return snap.put_back(st);
+}

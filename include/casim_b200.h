@@ -198,6 +198,16 @@ casim_status casim_b200_release_analysis(casim_h h, double hist_dt_ms, double ma
                                          int32_t* hist_all, int32_t* hist_quark, int32_t* hist_blip, int32_t* hist_spark,
                                          int32_t* class_counts);
 
+/* Launch configuration chosen by measurement (no counterpart in the reference): on the
+ * resident path, for every cluster-size class, candidate block sizes (256 up to the
+ * specialisation's bound, step 64) at the class's cluster size and at twice it (where
+ * the sites fit) each run steps_per_trial time steps of that class alone, from the same
+ * state; the fastest is kept for later casim_b200_step calls. The batch state is the
+ * same before and after. Later steps may differ from untuned ones in the last bits of
+ * the cross-warp sums, and two tunings may choose differently. report (n bytes, may be
+ * NULL) receives the choices. */
+casim_status casim_b200_autotune(casim_h h, int64_t steps_per_trial, char* report, size_t n);
+
 /* How the resident path splits the batch into thread-block-cluster classes,
  * or why the handle runs on the plain path. */
 casim_status casim_b200_path_note(casim_h h, char* buf, size_t n);

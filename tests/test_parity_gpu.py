@@ -231,3 +231,29 @@ def test_single_site_mwc_gating_matches_oracle(cuda_device):
     with pytest.raises(cb.CasimError) as e:
         cb.ReleaseSiteBatch(params, sites, precision="fp64", path="resident")
     assert e.value.status == cb.EUNSUPPORTED
+
+
+def test_autotune_keeps_the_state_and_the_results(cuda_device):
+    """casim_b200_autotune runs its trials from a copy of the state and puts it back:
+    fields, cytosol, RyR states and draw counts are bit-identical before and after, and
+    the tuned launches still follow the FP64 oracle."""
+    params, sites = configs.small_mixed(n_sites=5, seed=41, dim=3, cytosol="RD3D", side=(14, 26))
+    params["Cytosol"]["Nodes"] = 11
+    params["B200"] = {"MinClusterSize": 2}
+    sim = _make(params, sites, "fp64", "resident")
+    orc = oracle.OracleSim(params, sites)
+    sim.start(sites["first_channel"])
+    orc.start(sites["first_channel"])
+    sim.step(50)
+    orc.step(50)
+    def state():
+        return ([sim.field(s, f) for s in range(5) for f in range(2)] + [sim.states(s) for s in range(5)] +
+                [sim.cyto_field(s, 0) for s in range(5)] + [np.array([sim.draws(s) for s in range(5)])])
+    before = state()
+    report = sim.autotune(10)
+    assert "->" in report, report
+    for a, b in zip(before, state()):
+        assert np.array_equal(a, b)
+    sim.step(150)
+    orc.step(150)
+    _compare_batch(sim, orc, 1e-11)
