@@ -13,6 +13,7 @@ struct cb_dev {
     int S = 0;              // sites
     int precision = 0;      // 0 = FP64 fields, 1 = FP32 fields
     int min_cluster = 1;    // smallest thread-block cluster per site on the resident path
+    int light_rows = 0;     // start from the lighter row partition of the edge and plane-0 blocks
     int NS = 0;             // mouth species per RyR: ions + pairs + free buffers
     int max_nodes = 0;      // largest padded node count of a site
     int max_ch = 0;

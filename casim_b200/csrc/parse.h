@@ -22,6 +22,7 @@ struct cb_config {
     std::vector<double> sp_x[2], sp_c[2];
     int num_batch = 1;
     int min_cluster = 1;  // "B200": {"MinClusterSize": C}: smallest cluster per site on the resident path
+    int light_rows = 0;   // "B200": {"LightEdgeRows": true}: fewer rows on the edge and plane-0 blocks
 };
 
 // Throws std::runtime_error with a readable message on any schema problem.

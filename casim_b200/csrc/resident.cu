@@ -74,6 +74,15 @@ void fill_const(const cb_model& m, rs_const<R>& k) {
 }
 
 // shared-memory carve for the sites `idx` with cluster size C
+// row weights of the C ranks: even, or (light) 2 shares for the first and last row blocks
+// (long y-edge rim lines) and the plane-0 rank (efflux deposits) and 3 for the others
+void row_weights(rs_args& a, int C, bool light) {
+    const int r0 = (C - C / 2) % C;
+    a.rw[0] = 0;
+    for (int r = 0; r < 16; ++r)
+        a.rw[r + 1] = (unsigned short)(a.rw[r] + (light && C >= 4 && r < C ? (r == 0 || r == C - 1 || r == r0 ? 2 : 3) : 1));
+}
+
 bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<int>& idx, int C, rs_args& a) {
     const cb_model& m = d.m;
     const size_t rs = d.precision == 0 ? 8 : 4;
@@ -89,7 +98,8 @@ bool plan(const cb_dev& d, const std::vector<cb_site>& sites, const std::vector<
         const int zmax = st.nz == 1 ? 1 : st.nz - 1;
         maxlt = std::max(maxlt, 4 * (st.nz + zmax) * ((std::max(st.nx, st.ny) + 31) / 32));
         for (int r = 0; r < C; ++r) {
-            int lo = (int)((long long)r * st.ny / C), hi = (int)((long long)(r + 1) * st.ny / C);
+            const int lo = row_lo(a.rw, r, st.ny, C), hi = row_lo(a.rw, r + 1, st.ny, C);
+            if (hi - lo < 3) return false;
             int slo = lo > 0 ? lo - 1 : 0, shi = hi < st.ny ? hi + 1 : st.ny;
             cap = std::max(cap, (shi - slo) * st.nx * st.nz);
         }
@@ -219,6 +229,7 @@ bool classify(const cb_dev& d, const std::vector<cb_site>& sites, std::vector<st
         while (k < 5 && sizes[k] < d.min_cluster) ++k;
         for (; k < 5; ++k) {
             rs_args a{};
+            for (int r = 0; r <= 16; ++r) a.rw[r] = (unsigned short)r;
             std::vector<int> one{s};
             if (plan(d, sites, one, sizes[k], a)) break;
         }
@@ -258,6 +269,7 @@ bool cb_resident_fits(const cb_dev& d, int* threads, size_t* smem, std::string* 
     // every class must be schedulable (a 16-block cluster needs 16 SMs of one GPC)
     for (size_t k = 0; k < classes.size(); ++k) {
         rs_args a{};
+        for (int r = 0; r <= 16; ++r) a.rw[r] = (unsigned short)r;
         if (!plan(d, sites, classes[k], cs[k], a)) return no("the shared-memory plan of a cluster class does not fit");
         a.m = d.m;
         fill_const(d.m, a.kf);
@@ -366,6 +378,8 @@ cudaError_t build_plan(cb_dev& d) {
     int offset = 0;
     for (size_t k = 0; k < classes.size(); ++k) {
         rs_args a{};
+        row_weights(a, cs[k], d.light_rows != 0);
+        if (d.light_rows && !plan(d, sites, classes[k], cs[k], a)) row_weights(a, cs[k], false);
         if (!plan(d, sites, classes[k], cs[k], a)) {
             delete P;
             return cudaErrorInvalidConfiguration;
@@ -502,7 +516,8 @@ struct state_copy {
 // `steps` time steps of its class alone (the other classes idle) from the same state,
 // which is put back after every trial and at the end. Candidates: 256 to the
 // specialisation's bound in steps of 64 threads, at the class's cluster size and, where
-// the class's sites fit it, at twice that size.
+// the class's sites fit it, at twice that size; from 4 blocks on, with even rows and with
+// fewer rows on the ranks that carry the y-edge rim lines and the plane-0 deposits.
 cudaError_t cb_resident_autotune(cb_dev& d, long long steps, cudaStream_t st, std::string* report) {
     cudaError_t e;
     if (!d.rs_plan && (e = build_plan(d)) != cudaSuccess) return e;
@@ -521,23 +536,28 @@ cudaError_t cb_resident_autotune(cb_dev& d, long long steps, cudaStream_t st, st
     std::string rep;
     for (size_t k = 0; k < P.args.size(); ++k) {
         struct cand {
-            int C, threads, clusters;
+            int C, threads, clusters, light;
             rs_args a;
             float ms;
         };
         std::vector<cand> cands;
         for (int C : {cs[k], 2 * cs[k]}) {
             if (C > 16) continue;
-            rs_args a = P.args[k];  // plan() rewrites only the shared-memory layout
-            if (C != cs[k] && !plan(d, sites, classes[k], C, a)) continue;
-            const int cap = thread_cap(d, P.nz, C);
-            for (int t = 256; t <= cap; t += 64) {
-                int clusters = 0;
-                if (launch_t(d, a, P.nz, C, t, 0, a.S, &clusters) != cudaSuccess || clusters < 1) {
-                    cudaGetLastError();
-                    continue;
+            for (int light = 0; light < (C >= 4 ? 2 : 1); ++light) {
+                // light: the first and last row blocks (long y-edge rim lines) and the rank of
+                // plane 0 (efflux deposits) take 2 shares of the rows, the others 3
+                rs_args a = P.args[k];  // plan() rewrites only the shared-memory layout
+                row_weights(a, C, light != 0);
+                if (!plan(d, sites, classes[k], C, a)) continue;
+                const int cap = thread_cap(d, P.nz, C);
+                for (int t = 256; t <= cap; t += 64) {
+                    int clusters = 0;
+                    if (launch_t(d, a, P.nz, C, t, 0, a.S, &clusters) != cudaSuccess || clusters < 1) {
+                        cudaGetLastError();
+                        continue;
+                    }
+                    cands.push_back({C, t, clusters, light, a, 0.f});
                 }
-                cands.push_back({C, t, clusters, a, 0.f});
             }
         }
         for (auto& c : cands) {
@@ -565,10 +585,10 @@ cudaError_t cb_resident_autotune(cb_dev& d, long long steps, cudaStream_t st, st
             if (c.ms < b->ms) b = &c;
         float cur_ms = -1;
         for (auto& c : cands)
-            if (c.C == P.cs[k] && c.threads == P.threads[k]) cur_ms = c.ms;
+            if (c.C == P.cs[k] && c.threads == P.threads[k] && !c.light) cur_ms = c.ms;
         rep += (k ? "; " : "") + std::to_string(classes[k].size()) + " sites: clusters of " + std::to_string(P.cs[k]) + " x " +
                std::to_string(P.threads[k]) + " threads (" + std::to_string(cur_ms) + " ms) -> " + std::to_string(b->C) + " x " +
-               std::to_string(b->threads) + " (" + std::to_string(b->ms) + " ms)";
+               std::to_string(b->threads) + (b->light ? " light edge rows" : "") + " (" + std::to_string(b->ms) + " ms)";
         P.cs[k] = b->C;
         P.threads[k] = b->threads;
         P.clusters[k] = b->clusters;

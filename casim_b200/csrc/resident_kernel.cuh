@@ -104,6 +104,8 @@ struct bconst {
 };
 
 struct rs_args {
+    // cumulative row weights of the ranks: rank r holds rows [ny*rw[r]/rw[C], ny*rw[r+1]/rw[C])
+    unsigned short rw[17];
     cb_model m;
     rs_const<float> kf;
     rs_const<double> kd;
@@ -190,7 +192,9 @@ __device__ __forceinline__ T* peer(T* p, int r) {
     else return cg::this_cluster().map_shared_rank(p, r);
 }
 
-__host__ __device__ __forceinline__ int row_lo(int r, int ny, int C) { return (int)(((long long)r * ny) / C); }
+__host__ __device__ __forceinline__ int row_lo(const unsigned short* rw, int r, int ny, int C) {
+    return (int)(((long long)rw[r] * ny) / rw[C]);
+}
 
 // deposit slot of dyad species f (its index among species with a cytosol counterpart), or -1
 __device__ __forceinline__ int dslot(const cb_model& m, int NI, int f) {
@@ -210,6 +214,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
     __shared__ long long s_D, s_we;
     __shared__ int s_nu;   // RD3D: slots of this rank's rim
     __shared__ int s_nlt;  // Update rim tasks of this rank
+    __shared__ int s_nrow[4];  // first and end row of the lower and the upper neighbour rank
     __shared__ int s_nd;  // RD3D, plane-0 rank: layer-0 cytosol nodes that receive efflux deposits
     constexpr int CSM = NI + NPM;  // cytosol species slots
     constexpr int FP = NI + NPM;   // cleft species slots
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
         const int nx = st.nx, ny = st.ny, nz = st.nz, nxy = nx * ny, np = st.npad;
         const int nch = st.n_ch;
         const int zmax = NZ == 1 ? 1 : nz - 1;
-        const int lo = row_lo(rank, ny, C), hi = row_lo(rank + 1, ny, C);
+        const int lo = row_lo(a.rw, rank, ny, C), hi = row_lo(a.rw, rank + 1, ny, C);
         const int slo = lo > 0 ? lo - 1 : 0, shi = hi < ny ? hi + 1 : ny;
         const int nr = shi - slo;
         const int lstride = nx * nr;  // z stride in local storage
@@ -343,6 +348,14 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                 for (int cn = 0; cn < mc2; ++cn)
                     if (dptr[cn + 1] > dptr[cn]) dnode[nd++] = (unsigned short)cn;
                 s_nd = nd;
+            }
+        }
+        if (tid == 33) {
+            for (int side = 0; side < 2; ++side) {
+                const int nb = side == 0 ? rank - 1 : rank + 1;
+                const bool in = nb >= 0 && nb < C;
+                s_nrow[2 * side] = in ? row_lo(a.rw, nb, ny, C) : 0;
+                s_nrow[2 * side + 1] = in ? row_lo(a.rw, nb + 1, ny, C) : 0;
             }
         }
         if (tid == 32) {
@@ -958,7 +971,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                     const int nb = side == 0 ? rank - 1 : rank + 1;
                     if (nb < 0 || nb >= C) continue;
                     const int y = side == 0 ? lo : hi - 1;
-                    const int nlo = row_lo(nb, ny, C), nhi = row_lo(nb + 1, ny, C);
+                    const int nlo = s_nrow[2 * side], nhi = s_nrow[2 * side + 1];
                     const int nslo = nlo > 0 ? nlo - 1 : 0;
                     const int nnr = (nhi < ny ? nhi + 1 : ny) - nslo;
                     R* dst = peer<C>(fb, nb);

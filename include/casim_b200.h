@@ -201,7 +201,9 @@ casim_status casim_b200_release_analysis(casim_h h, double hist_dt_ms, double ma
 /* Launch configuration chosen by measurement (no counterpart in the reference): on the
  * resident path, for every cluster-size class, candidate block sizes (256 up to the
  * specialisation's bound, step 64) at the class's cluster size and at twice it (where
- * the sites fit) each run steps_per_trial time steps of that class alone, from the same
+ * the sites fit), and from 4 blocks on with even rows per block or with fewer rows on the
+ * blocks that carry extra rim and deposit work, each run steps_per_trial time steps of that
+ * class alone, from the same
  * state; the fastest is kept for later casim_b200_step calls. The batch state is the
  * same before and after. Later steps may differ from untuned ones in the last bits of
  * the cross-warp sums, and two tunings may choose differently. report (n bytes, may be

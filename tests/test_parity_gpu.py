@@ -138,14 +138,16 @@ def test_fp64_sites_split_over_block_clusters(cuda_device, dim, cytosol, cluster
     _check_uneven(sim, params, sites, cytosol, "resident")
 
 
+@pytest.mark.parametrize("light", [False, True])
 @pytest.mark.parametrize("cluster", [8, 16])
-def test_fp64_rd3d_sites_split_over_large_clusters(cuda_device, cluster):
+def test_fp64_rd3d_sites_split_over_large_clusters(cuda_device, cluster, light):
     """RD3D sites over 8- and 16-block clusters: every rank holds a few cleft rows and
     one or two cytosol planes, and the plane-0 rank (deposits, rim values) is not the
-    rank of the first row block."""
-    params, sites = configs.small_mixed(n_sites=3, seed=29, dim=3, cytosol="RD3D", side=(48, 54))
+    rank of the first row block; with LightEdgeRows the first, last and plane-0 ranks
+    hold fewer rows than the others."""
+    params, sites = configs.small_mixed(n_sites=3, seed=29, dim=3, cytosol="RD3D", side=(48, 54) if cluster == 8 else (68, 74))
     params["Cytosol"]["Nodes"] = 17
-    params["B200"] = {"MinClusterSize": cluster}
+    params["B200"] = {"MinClusterSize": cluster, "LightEdgeRows": light}
     sim = _make(params, sites, "fp64", "resident")
     assert "clusters of %d" % cluster in sim.path_note()
     _check_uneven(sim, params, sites, "RD3D", "resident")
