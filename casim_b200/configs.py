@@ -191,6 +191,87 @@ def config3(n_sites=1024, seed=3, n_ryr=50):
     return _clean(p), sites_table([64] * n_sites, [64] * n_sites, [1] * n_sites, [n_ryr] * n_sites, xs, ys, seeds, jsr_init=jsr)
 
 
+def with_magnesium(params):
+    """A copy of `params` with a Magnesium ion (1 mM, no RyR conductance) in the
+    dyad, the jSR and the NSR (the second ion of the reference's Mg-aware models)."""
+    p = json.loads(json.dumps(params))
+    p["Dyad"]["Ions"]["Magnesium"] = {"Concentration": 1000.0, "D": 160000.0, "Extracell": 1000.0}
+    p["Dyad"]["Channels"]["RyR"]["Conductance"]["Magnesium"] = 0.0
+    p["jSR"]["Ions"]["Magnesium"] = {"Binding sites of CQ": 1, "Concentration": 1000.0, "K CQ (uM)": 1.0e6, "T refill (ms)": 10.0}
+    p["nSR"]["Ions"]["Magnesium"] = {"Concentration (uM)": 1000.0}
+    return p
+
+
+# Tetrameric MWC gating of the large sweep: Ca activation Kd 10 uM, allosteric
+# coupling factor 0.1, 1 mM Mg competing at the activation site and inhibiting
+# (the Po law of CaSim/TwoStateMWC.cpp:15-23; fMg, KMg, KMgI as the reference's
+# example model, KO0 and kclose chosen for the sweep)
+SWEEP_MWC = {"fCa": 0.1, "KCa": 10.0, "fMg": 3.2517014, "KMg": 92.2954937, "KO0": 1000.0, "KMgI": 546.4, "kclose": 1.0}
+
+
+def mwc_open_rate(ca, mg=1000.0, par=SWEEP_MWC):
+    """kopen(Ca) of the TwoStateMWC law: kclose * Po / (1 - Po) (1/ms)."""
+    ca = np.asarray(ca, dtype=np.float64)
+    inac = par["KMgI"] ** 2 / (par["KMgI"] ** 2 + mg * mg)
+    a = (ca + par["KCa"] * par["fCa"] * (1 + mg / (par["fMg"] * par["KMg"]))) ** 4
+    b = par["KO0"] * (par["fCa"] * (ca + par["KCa"] * (1 + mg / par["KMg"]))) ** 4
+    po = inac * a / (a + b)
+    return par["kclose"] * po / (1 - po)
+
+
+def sweep_spline_tables(directory):
+    """Rate tables of the spline-gated half: kopen(Ca) tabulated from the MWC law
+    at 0 and 160 log-spaced Ca values in [0.01, 5000] uM, kclose constant.
+    Returns the (kopen, kclose) file paths."""
+    import os
+    ca = np.concatenate([[0.0], np.logspace(-2, np.log10(5000.0), 160)])
+    paths = []
+    for name, y in (("kopen_mwc.txt", mwc_open_rate(ca)), ("kclose_mwc.txt", np.full(ca.size, SWEEP_MWC["kclose"]))):
+        path = os.path.join(directory, name)
+        np.savetxt(path, np.column_stack([ca, y]), fmt="%.17g")
+        paths.append(path)
+    return paths
+
+
+def config5(n_sites=16384, seed=5, side=(40, 120), ryr=(10, 150), cytosol="RD3D", table_dir=None):
+    """Large sweep: 3D clefts as config 2 (side ~ U{40..120} x 3 layers, 25^3
+    RD cytosol) with RyR count ~ U{10..150}, capped at the jittered 31 nm
+    lattice that fits inside the rim; 1 mM Mg. Returns two halves, each
+    (params, sites): the first gated by the tetrameric MWC law (SWEEP_MWC),
+    the second by the same law tabulated for TwoStateSpline (tables written
+    to `table_dir`, a temporary directory by default)."""
+    import tempfile
+    rng = np.random.default_rng(seed)
+    n = rng.integers(side[0], side[1] + 1, size=n_sites)
+    fit = (np.floor((n - 5) * 10.0 / RYR_PITCH_NM) + 1) ** 2
+    nr = np.minimum(rng.integers(ryr[0], ryr[1] + 1, size=n_sites), fit).astype(np.int64)
+    xs, ys, seeds, first = [], [], [], []
+    for k in range(n_sites):
+        x, y = lattice(int(nr[k]), (n[k] - 1) * 5.0, (n[k] - 1) * 5.0, rng)
+        xs.append(x)
+        ys.append(y)
+        seeds.append([int(v) for v in rng.integers(1, 4294944443, size=6)])
+        first.append(int(rng.integers(0, nr[k])))
+    base = with_magnesium(base_params(dim=3, nx=64, ny=64, cytosol=cytosol))
+    pm = json.loads(json.dumps(base))
+    pm["Dyad"]["Channels"]["RyR"]["Model"] = "TwoStateMWC"
+    pm["Dyad"]["Channels"]["RyR"]["Parameters"] = dict(SWEEP_MWC)
+    ps = json.loads(json.dumps(base))
+    kopen, kclose = sweep_spline_tables(table_dir or tempfile.mkdtemp(prefix="casim_sweep_"))
+    ps["Dyad"]["Channels"]["RyR"]["Model"] = "TwoStateSpline"
+    ps["Dyad"]["Channels"]["RyR"]["Parameters"] = {}
+    ps["Dyad"]["Channels"]["RyR"]["Kopen filename"] = kopen
+    ps["Dyad"]["Channels"]["RyR"]["Kclose filename"] = kclose
+    halves = []
+    for p, idx in ((pm, range(0, n_sites // 2)), (ps, range(n_sites // 2, n_sites))):
+        idx = list(idx)
+        cx = [v for k in idx for v in xs[k]]
+        cy = [v for k in idx for v in ys[k]]
+        halves.append((_clean(p), sites_table(n[idx], n[idx], [3] * len(idx), nr[idx], cx, cy, [seeds[k] for k in idx],
+                                              first=[first[k] for k in idx])))
+    return halves
+
+
 def small_mixed(n_sites=6, seed=11, dim=2, cytosol="Pool", side=(12, 24), ryr=(2, 9)):
     """Small uneven sites for parity tests at sizes the oracle finishes in seconds."""
     p = base_params(dim=dim, nx=16, ny=16, cytosol=cytosol, sarcolemma=True)

@@ -1,0 +1,38 @@
+"""Synthetic workload builders: the large-sweep halves (tetrameric MWC and its
+spline tabulation) and the precision-study sites, checked on the CPU."""
+import numpy as np
+
+from casim_b200 import configs
+from oracle import oracle
+
+
+def test_config5_halves(tmp_path):
+    halves = configs.config5(n_sites=64, seed=1, table_dir=str(tmp_path))
+    assert [p["Dyad"]["Channels"]["RyR"]["Model"] for p, _ in halves] == ["TwoStateMWC", "TwoStateSpline"]
+    for p, s in halves:
+        assert len(s["nx"]) == 32
+        assert s["n_ch"].min() >= 10 and s["n_ch"].max() <= 150
+        # every RyR lies inside the rim of its cleft
+        off = np.concatenate([[0], np.cumsum(s["n_ch"])])
+        for k in range(32):
+            edge = (s["nx"][k] - 1) * 10.0
+            x, y = s["ch_x"][off[k]:off[k + 1]], s["ch_y"][off[k]:off[k + 1]]
+            assert x.min() > 0 and y.min() > 0 and x.max() < edge and y.max() < edge
+        assert "Magnesium" in p["Dyad"]["Ions"]
+    # the tabulated opening rate is the MWC law at its knots
+    t = np.loadtxt(halves[1][0]["Dyad"]["Channels"]["RyR"]["Kopen filename"])
+    assert np.allclose(t[:, 1], configs.mwc_open_rate(t[:, 0]), rtol=1e-15, atol=0)
+
+
+def test_config5_spline_follows_mwc(tmp_path):
+    """The natural spline through the tabulated opening rate (the oracle's
+    restatement of the spline model) stays within 1 % of the analytic MWC law
+    between the knots over the Ca range of a cleft (0.1 uM .. 1 mM)."""
+    halves = configs.config5(n_sites=2, seed=2, side=(40, 40), table_dir=str(tmp_path))
+    t = np.loadtxt(halves[1][0]["Dyad"]["Channels"]["RyR"]["Kopen filename"])
+    coef, _, _ = oracle.natural_spline(t[:, 0], t[:, 1])
+    ca = np.logspace(-1, 3, 400)
+    i = np.searchsorted(t[:, 0], ca, side="right") - 1
+    h = ca - t[i, 0]
+    got = coef[i, 0] + h * (coef[i, 1] + h * (coef[i, 2] + h * coef[i, 3]))
+    assert np.max(np.abs(got / configs.mwc_open_rate(ca) - 1)) < 1e-2
