@@ -1,0 +1,127 @@
+"""Precision study of the mixed-precision path (config 3).
+
+The production precision keeps the cleft stencil and buffer kinetics in FP32
+and the jSR pool, the cytosol pool and the accumulated release flux in FP64.
+This module runs the same sites twice on the device, once in that mixed mode
+and once all in FP64 (the FP64 device path matches the C restatement of the
+reference's CPU classes to 1e-11 and draw for draw; a CPU run of 1024 sites
+for 100 ms, 8e12 node-steps, is out of reach), and reports at each horizon:
+
+* mouth Ca: relative error of the Ca at every RyR mouth;
+* jSR depletion: relative error of jSR_init - jSR(t);
+* total release: relative error of the accumulated RyR flux of the site.
+
+Both runs draw the same MRG32k3a numbers, but a draw that falls within the
+rounding difference of a transition probability takes the two runs apart.
+Errors are therefore taken over the sites still in lockstep (identical RyR
+states and identical draw counts), and every site enters a two-sample
+Kolmogorov-Smirnov comparison of the release and jSR distributions.
+
+    python -m casim_b200.precision --sites 1024 --horizons 10,100
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import ReleaseSiteBatch, configs
+
+
+def _rel(a, b, floor):
+    return np.abs(a - b) / np.maximum(np.abs(b), floor)
+
+
+def _summary(x):
+    if x.size == 0:
+        return {"median": None, "p99": None, "max": None}
+    return {"median": float(np.median(x)), "p99": float(np.quantile(x, 0.99)), "max": float(np.max(x))}
+
+
+def snapshot(sim):
+    """Per-site state of a batch: RyR states, mouth Ca, jSR Ca, release, draws."""
+    S = sim.S
+    return {
+        "states": sim.all_states(),
+        "mouth": sim.all_mouth(0),
+        "jsr": np.array([sim.jsr(s)[0] for s in range(S)]),
+        "release": np.array([sim.release(s) for s in range(S)]),
+        "draws": np.array([sim.draws(s) for s in range(S)], dtype=np.int64),
+    }
+
+
+def compare(a, b, n_ch, jsr_init):
+    """Errors of snapshot `a` (mixed precision) against snapshot `b` (FP64)."""
+    from scipy.stats import ks_2samp
+    off = np.concatenate([[0], np.cumsum(n_ch)])
+    S = len(n_ch)
+    same = np.array([a["draws"][s] == b["draws"][s] and np.array_equal(a["states"][off[s]:off[s + 1]], b["states"][off[s]:off[s + 1]])
+                     for s in range(S)])
+    ch_same = np.repeat(same, n_ch)
+    mouth = _rel(a["mouth"][ch_same], b["mouth"][ch_same], 1e-30)
+    open_mouth = _rel(a["mouth"][ch_same & (b["states"] == 1)], b["mouth"][ch_same & (b["states"] == 1)], 1e-30)
+    dep_a, dep_b = jsr_init - a["jsr"], jsr_init - b["jsr"]
+    # depletion relative to its own size, floored at 1e-6 of the initial jSR Ca
+    dep = _rel(dep_a[same], dep_b[same], 1e-6 * jsr_init[same])
+    rel = _rel(a["release"][same], b["release"][same], 1e-30)
+    openc_a = np.add.reduceat(a["states"], off[:-1])
+    openc_b = np.add.reduceat(b["states"], off[:-1])
+    return {
+        "lockstep_sites": int(same.sum()), "sites": S,
+        "mouth_ca_rel_err": _summary(mouth), "open_mouth_ca_rel_err": _summary(open_mouth),
+        "jsr_depletion_rel_err": _summary(dep), "release_rel_err": _summary(rel),
+        "ks_p_release": float(ks_2samp(a["release"], b["release"]).pvalue),
+        "ks_p_jsr": float(ks_2samp(a["jsr"], b["jsr"]).pvalue),
+        "ks_p_open": float(ks_2samp(openc_a, openc_b).pvalue),
+        "mean_release": [float(a["release"].mean()), float(b["release"].mean())],
+        "mean_jsr_depletion": [float(dep_a.mean()), float(dep_b.mean())],
+    }
+
+
+def precision_study(n_sites=1024, horizons_ms=(10.0, 100.0), seed=3, chunk=20000, path="auto"):
+    """Config 3: `n_sites` 2D 64x64 clefts with 50 RyRs and jSR Ca ~ U[0.5, 1.5]
+    mM, one RyR opened at t = 0; mixed precision against FP64 at each horizon."""
+    p, s = configs.config3(n_sites=n_sites, seed=seed)
+    jsr_init = s["jsr_init"][:, 0].copy()
+    sims = {prec: ReleaseSiteBatch(p, s, precision=prec, path=path) for prec in ("fp32", "fp64")}
+    for sim in sims.values():
+        sim.start(s["first_channel"])
+    dt_ms = sims["fp32"].info.dt_ms
+    done = {k: 0 for k in sims}
+    dev_ms = {k: 0.0 for k in sims}
+    out = {"workload": "%d 2D 64x64 clefts, 50 RyR, jSR Ca ~U[0.5,1.5] mM (config 3)" % n_sites,
+           "paths": {k: v.path for k, v in sims.items()}, "horizons": []}
+    for h in horizons_ms:
+        target = int(round(h / dt_ms))
+        for k, sim in sims.items():
+            while done[k] < target:
+                n = min(chunk, target - done[k])
+                sim.step(n)
+                sim.synchronize()
+                dev_ms[k] += sim.last_step_ms()
+                done[k] += n
+        row = {"t_ms": h}
+        row.update(compare(snapshot(sims["fp32"]), snapshot(sims["fp64"]), np.asarray(s["n_ch"]), jsr_init))
+        row["site_ms_per_s"] = {k: n_sites * done[k] * dt_ms / (dev_ms[k] / 1e3) for k in sims}
+        out["horizons"].append(row)
+    for sim in sims.values():
+        sim.close()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--sites", type=int, default=1024)
+    ap.add_argument("--horizons", default="10,100", help="report times in ms, comma separated")
+    ap.add_argument("--seed", type=int, default=3)
+    a = ap.parse_args()
+    import torch
+    torch.cuda.init()
+    t0 = time.time()
+    res = precision_study(a.sites, tuple(float(x) for x in a.horizons.split(",")), seed=a.seed)
+    res["wall_s"] = time.time() - t0
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

@@ -36,3 +36,25 @@ def test_config5_spline_follows_mwc(tmp_path):
     h = ca - t[i, 0]
     got = coef[i, 0] + h * (coef[i, 1] + h * (coef[i, 2] + h * coef[i, 3]))
     assert np.max(np.abs(got / configs.mwc_open_rate(ca) - 1)) < 1e-2
+
+
+def test_precision_compare_lockstep_and_errors():
+    """Host logic of the precision study: a site whose states or draw count
+    differ leaves the error statistics; relative errors are taken per RyR
+    mouth and per site."""
+    from casim_b200.precision import compare
+    n_ch = np.array([2, 3])
+    jsr0 = np.array([1000.0, 800.0])
+    b = {"states": np.array([1, 0, 0, 1, 0]), "mouth": np.array([200.0, 1.0, 2.0, 150.0, 0.5]),
+         "jsr": np.array([900.0, 700.0]), "release": np.array([10.0, 20.0]), "draws": np.array([100, 200])}
+    a = {k: v.copy() for k, v in b.items()}
+    a["mouth"][0] *= 1.001
+    a["jsr"][0] = 899.9           # depletion 100.1 against 100
+    a["release"][0] = 10.002
+    a["states"][3] = 0            # site 1 left lockstep
+    r = compare(a, b, n_ch, jsr0)
+    assert r["lockstep_sites"] == 1 and r["sites"] == 2
+    assert abs(r["mouth_ca_rel_err"]["max"] - 1e-3) < 1e-12
+    assert abs(r["open_mouth_ca_rel_err"]["max"] - 1e-3) < 1e-12
+    assert abs(r["jsr_depletion_rel_err"]["max"] - 1e-3) < 1e-9
+    assert abs(r["release_rel_err"]["max"] - 2e-4) < 1e-12

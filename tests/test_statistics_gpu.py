@@ -59,3 +59,40 @@ def test_gpu_fp32_and_oracle_fp64_distributions_agree(cuda_device):
     for name, a, b in zip(("release", "transitions", "open at end"), gpu, cpu):
         p = ks_2samp(a, b).pvalue
         assert p > 0.05, (name, p, np.mean(a), np.mean(b))
+
+
+EVERY = 100  # time steps between open-count samples (5 us)
+
+
+def test_release_event_distributions_agree(cuda_device):
+    """Release-event amplitude (peak open RyRs) and latency (time to peak)
+    from the device's traces and device analysis against the same metrics
+    of FP64 oracle runs from other seeds (the oracle's open counts sampled at
+    the same times, analysed by the CPU restatement of the reference's
+    analyzer): two-sample KS, p > 0.05."""
+    import os
+    from oracle import analysis
+    pg, sg_ = _sites(3)
+    po, so = _sites(4)
+    n_samples = STEPS // EVERY + 1
+    sim = cb.ReleaseSiteBatch(pg, sg_, precision="fp32", path="resident")
+    sim.start(sg_["first_channel"])
+    sim.trace_enable(EVERY, n_samples)
+    sim.step(STEPS)
+    ts = EVERY * sim.info.dt_ms
+    max_time = STEPS * sim.info.dt_ms
+    gpu = sim.release_analysis(max_time, 2, hist_dt_ms=ts)
+    sim.close()
+    orc = oracle.OracleSim(po, so)
+    orc.start(so["first_channel"])
+    opens = np.zeros((N_RUNS, n_samples), dtype=np.int64)
+    opens[:, 0] = [int(np.sum(orc.states(k))) for k in range(N_RUNS)]
+    for j in range(1, n_samples):
+        orc.step(EVERY, os.cpu_count() or 1)
+        opens[:, j] = [int(np.sum(orc.states(k))) for k in range(N_RUNS)]
+    times = [np.arange(n_samples) * ts for _ in range(N_RUNS)]
+    cpu = analysis.cre_analysis(times, list(opens), N_RYR, max_time, 2, dt=ts)["per_trace"]
+    assert np.std(gpu["amp"]) > 0 and np.std(gpu["ttp"]) > 0
+    for name, a, b in (("amplitude", gpu["amp"], cpu[:, 0]), ("time to peak", gpu["ttp"], cpu[:, 1])):
+        p = ks_2samp(a, b).pvalue
+        assert p > 0.05, (name, p, np.mean(a), np.mean(b))
