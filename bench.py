@@ -111,7 +111,7 @@ class Clocks:
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_resident launches of one
 # bench step on 512 sites of the config-2 workload, per site (FP32): each launch loads
 # and stores every site once, so the traffic scales with the sites, not with the steps
-RESIDENT_DRAM_BYTES_PER_SITE = 330.3e6 / 512
+RESIDENT_DRAM_BYTES_PER_SITE = 322.4e6 / 512
 
 
 def measured_peak_hbm():
@@ -366,7 +366,7 @@ def main():
                                  if sim.path == "resident" and args.precision == "fp32" and args.config == "c2" else None),
                      "note": "achieved = algorithmic bytes (2 x field bytes per node-step) of one bench step / its device "
                              "time; the resident path keeps fields on chip, so this is an effective bandwidth; traffic = "
-                             "ncu DRAM bytes of the launches of one bench step (0.62 MB per site per launch, measured "
+                             "ncu DRAM bytes of the launches of one bench step (0.63 MB per site per launch, measured "
                              "on 512 sites of this workload and scaled by sites)"},
         "clocks": clk.summary(),
     }

@@ -57,7 +57,7 @@ __host__ __device__ constexpr int max_threads(int rbytes, int csm, int nz, int C
     return 3 * nz * csm * rbytes / 4 > 60 ? 256 : C == 16 ? 384 : 512;
 }
 // pair capacity of the kernel specialisation that serves NI ions and NP pairs
-__host__ __device__ constexpr int npm_of(int NI, int NP) { return (NI == 1 && NP <= 2) ? 2 : 4; }
+__host__ __device__ constexpr int npm_of(int NI, int NP) { return NP <= 2 ? 2 : 4; }
 
 // Stencil constants in the field precision R, so that they are kernel-parameter
 // operands of the arithmetic (each value is the (R) cast of the model's double,
@@ -1144,6 +1144,7 @@ cudaError_t dispatch(const rs_args& a, int NI, int NP, int C, int threads, cudaS
     if (threads > max_threads(sizeof(R), NI + npm_of(NI, NP), NZ, C)) return cudaErrorInvalidConfiguration;
     if (NI == 1 && NP <= 2) return launch_c<R, 1, 2, NZ>(a, C, threads, st, n, dry, known);
     if (NI == 1 && NP <= 4) return launch_c<R, 1, 4, NZ>(a, C, threads, st, n, dry, known);
+    if (NI == 2 && NP <= 2) return launch_c<R, 2, 2, NZ>(a, C, threads, st, n, dry, known);
     if (NI == 2 && NP <= 4) return launch_c<R, 2, 4, NZ>(a, C, threads, st, n, dry, known);
     return cudaErrorInvalidConfiguration;
 }
