@@ -233,6 +233,18 @@ def sweep_spline_tables(directory):
     return paths
 
 
+def subset_sites(sites, idx):
+    """The sites table restricted to the sites `idx`, in that order."""
+    idx = np.asarray(idx, dtype=np.int64)
+    off = np.concatenate([[0], np.cumsum(sites["n_ch"])])
+    ch = np.concatenate([np.arange(off[k], off[k + 1]) for k in idx]) if idx.size else np.zeros(0, np.int64)
+    out = {k: (None if sites.get(k) is None else np.asarray(sites[k])[idx])
+           for k in ("nx", "ny", "nz", "n_ch", "seeds", "jsr_init", "first_channel")}
+    out["ch_x"] = np.asarray(sites["ch_x"])[ch]
+    out["ch_y"] = np.asarray(sites["ch_y"])[ch]
+    return out
+
+
 def config5(n_sites=16384, seed=5, side=(40, 120), ryr=(10, 150), cytosol="RD3D", table_dir=None):
     """Large sweep: 3D clefts as config 2 (side ~ U{40..120} x 3 layers, 25^3
     RD cytosol) with RyR count ~ U{10..150}, capped at the jittered 31 nm

@@ -2,11 +2,15 @@
 Mg, half gated by the tetrameric MWC law (TwoStateMWC) and half by the same
 law tabulated for TwoStateSpline, run side by side on one GPU.
 
-The two halves are two batches (a batch holds one gating model), each on its
-own CUDA stream; the simulated site-ms/s counts both. After the run the open
-RyR counts and the released Ca of the halves are compared by two-sample KS
-tests: the tabulated law is the analytic one up to the spline's interpolation
-error, so the distributions should agree.
+A batch holds one gating model, and the resident path takes a batch only if
+every site fits the shared memory of a 16-block cluster, which the largest
+sites with the second ion do not. So each half is ordered by size and split
+at the largest cleft side whose sites the resident path still takes: the
+smaller sites run resident, the rest on the plain path. The (up to four)
+batches run on their own CUDA streams; the simulated site-ms/s counts all of
+them. After the run the open RyR counts and the released Ca of the halves are
+compared by two-sample KS tests: the tabulated law is the analytic one up to
+the spline's interpolation error, so the distributions should agree.
 
     python -m casim_b200.sweep --sites 16384 --ms 0.2
 """
@@ -16,21 +20,61 @@ import time
 
 import numpy as np
 
-from . import ReleaseSiteBatch, configs
+from . import EUNSUPPORTED, CasimError, ReleaseSiteBatch, configs
+
+
+def split_resident(params, sites, precision):
+    """[(site indices, path)]: the sites ordered by cleft side and RyR count,
+    split at the largest side whose sites the resident path takes (found by
+    bisection over the distinct sides, each probe a batch that is built and
+    released); the rest run on the plain path."""
+    order = np.lexsort((np.asarray(sites["n_ch"]), np.asarray(sites["nx"])))
+    side = np.asarray(sites["nx"])[order]
+    sides = np.unique(side)
+
+    def fits(k):  # the sites with side <= sides[k]
+        idx = order[side <= sides[k]]
+        try:
+            ReleaseSiteBatch(params, configs.subset_sites(sites, idx), precision=precision, path="resident").close()
+            return True
+        except CasimError as e:
+            if e.status != EUNSUPPORTED:
+                raise
+            return False
+
+    if fits(len(sides) - 1):
+        return [(order, "resident")]
+    lo, hi = -1, len(sides) - 1  # fits(lo) (none, trivially), not fits(hi)
+    while hi - lo > 1:
+        mid = (lo + hi) // 2
+        if fits(mid):
+            lo = mid
+        else:
+            hi = mid
+    if lo < 0:
+        return [(order, "plain")]
+    cut = int(np.searchsorted(side, sides[lo], side="right"))
+    return [(order[:cut], "resident"), (order[cut:], "plain")]
 
 
 def run_sweep(n_sites=16384, t_ms=0.2, chunk=200, precision="fp32", seed=5, path="auto"):
     import torch
     from scipy.stats import ks_2samp
     halves = configs.config5(n_sites=n_sites, seed=seed)
-    sims, streams = [], []
-    for p, s in halves:
-        sim = ReleaseSiteBatch(p, s, precision=precision, path=path)
-        st = torch.cuda.Stream()
-        sim.set_stream(st.cuda_stream)
-        sim.start(s["first_channel"])
-        sims.append(sim)
-        streams.append(st)
+    sims, streams, parts = [], [], []
+    for h, (p, s) in enumerate(halves):
+        split = split_resident(p, s, precision) if path == "auto" else [(np.arange(len(s["nx"])), path)]
+        for idx, pth in split:
+            if idx.size == 0:
+                continue
+            sub = configs.subset_sites(s, idx)
+            sim = ReleaseSiteBatch(p, sub, precision=precision, path=pth)
+            st = torch.cuda.Stream()
+            sim.set_stream(st.cuda_stream)
+            sim.start(sub["first_channel"])
+            sims.append(sim)
+            streams.append(st)
+            parts.append((h, sub))
     dt_ms = sims[0].info.dt_ms
     n_steps = int(round(t_ms / dt_ms))
     torch.cuda.synchronize()
@@ -54,19 +98,20 @@ def run_sweep(n_sites=16384, t_ms=0.2, chunk=200, precision="fp32", seed=5, path
     ms = ev0.elapsed_time(ev1)
     out = {"workload": "%d 3D dyads side~U{40..120}x3, 10..150 RyR, 25^3 RD cytosol, 1 mM Mg; "
                        "half TwoStateMWC, half TwoStateSpline (config 5)" % n_sites,
-           "precision": precision, "paths": [sim.path for sim in sims], "t_ms": n_steps * dt_ms,
+           "precision": precision, "batches": [{"half": h, "sites": sim.S, "path": sim.path, "max_side": int(sub["nx"].max())}
+                                               for sim, (h, sub) in zip(sims, parts)], "t_ms": n_steps * dt_ms,
            "device_ms": ms, "site_ms_per_s": n_sites * n_steps * dt_ms / (ms / 1e3), "gpu_launches": launches,
            "finite": [bool(sim.check_finite()[0]) for sim in sims], "halves": []}
-    opens, rels = [], []
-    for sim, (p, s) in zip(sims, halves):
-        off = np.concatenate([[0], np.cumsum(s["n_ch"])])
-        st = sim.all_states()
-        oc = np.add.reduceat(st, off[:-1])
-        rel = np.array([sim.release(k) for k in range(sim.S)])
-        opens.append(oc)
-        rels.append(rel)
-        out["halves"].append({"model": p["Dyad"]["Channels"]["RyR"]["Model"], "sites": sim.S,
-                              "mean_open": float(oc.mean()), "mean_release": float(rel.mean())})
+    opens, rels = [[], []], [[], []]
+    for sim, (h, sub) in zip(sims, parts):
+        off = np.concatenate([[0], np.cumsum(sub["n_ch"])])
+        opens[h].append(np.add.reduceat(sim.all_states(), off[:-1]))
+        rels[h].append(np.array([sim.release(k) for k in range(sim.S)]))
+    opens = [np.concatenate(o) for o in opens]
+    rels = [np.concatenate(r) for r in rels]
+    for h, (p, _) in enumerate(halves):
+        out["halves"].append({"model": p["Dyad"]["Channels"]["RyR"]["Model"], "sites": int(opens[h].size),
+                              "mean_open": float(opens[h].mean()), "mean_release": float(rels[h].mean())})
     out["ks_p_open"] = float(ks_2samp(opens[0], opens[1]).pvalue)
     out["ks_p_release"] = float(ks_2samp(rels[0], rels[1]).pvalue)
     for sim in sims:

@@ -58,3 +58,13 @@ def test_precision_compare_lockstep_and_errors():
     assert abs(r["open_mouth_ca_rel_err"]["max"] - 1e-3) < 1e-12
     assert abs(r["jsr_depletion_rel_err"]["max"] - 1e-3) < 1e-9
     assert abs(r["release_rel_err"]["max"] - 2e-4) < 1e-12
+
+
+def test_subset_sites_keeps_each_sites_rows():
+    _, s = configs.config2(n_sites=6, seed=4)
+    sub = configs.subset_sites(s, [4, 1])
+    off = np.concatenate([[0], np.cumsum(s["n_ch"])])
+    assert list(sub["nx"]) == [s["nx"][4], s["nx"][1]]
+    assert np.array_equal(sub["ch_x"], np.concatenate([s["ch_x"][off[4]:off[5]], s["ch_x"][off[1]:off[2]]]))
+    assert np.array_equal(sub["seeds"], s["seeds"][[4, 1]])
+    assert list(sub["first_channel"]) == [s["first_channel"][4], s["first_channel"][1]]
