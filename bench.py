@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate-versus-RD report")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the mouth-Ca error check against FP64")
     return ap.parse_args()
 
 
@@ -226,6 +227,35 @@ def surrogate_report(sites=2048, sim_steps=20000, batches=8, train_steps=4000):
             "hybrid": hyb}
 
 
+def accuracy_report(args, params, sites, n_sites=64, steps=2000):
+    """Mouth-Ca error of the benchmarked precision on the bench's own workload:
+    the first `n_sites` sites run `steps` time steps in the bench's precision
+    and all in FP64 from the same seeds (the FP64 device path matches the C
+    restatement of the reference to 1e-11); errors over the sites still in
+    lockstep (identical RyR states and draw counts)."""
+    import casim_b200 as cb
+    from casim_b200 import configs
+    from casim_b200.precision import compare, snapshot
+    idx = np.arange(min(n_sites, len(sites["nx"])))
+    sub = configs.subset_sites(sites, idx)
+    snaps = []
+    for prec in (args.precision, "fp64"):
+        sim = cb.ReleaseSiteBatch(params, sub, precision=prec, path="auto")
+        sim.start(sub["first_channel"])
+        sim.step(steps)
+        sim.synchronize()
+        snaps.append(snapshot(sim))
+        sim.close()
+    if sub.get("jsr_init") is None:
+        jsr0 = np.full(idx.size, float(params["jSR"]["Ions"]["Calcium"]["Concentration"]))
+    else:
+        jsr0 = np.asarray(sub["jsr_init"], dtype=np.float64)[:, 0]
+    r = compare(snaps[0], snaps[1], np.asarray(sub["n_ch"]), jsr0)
+    return {"against": "fp64 device path, same seeds", "sites": int(idx.size), "time_steps": steps,
+            "lockstep_sites": r["lockstep_sites"], "mouth_ca_rel_err_max": r["mouth_ca_rel_err"]["max"],
+            "mouth_ca_rel_err_median": r["mouth_ca_rel_err"]["median"], "release_rel_err_max": r["release_rel_err"]["max"]}
+
+
 def params_dt_ms(params):
     return float(params["dt, ns"]) * 1e-6
 
@@ -398,6 +428,11 @@ def main():
             result["cpu_baseline"] = cpu_baseline(args, p, s, args.cpu_seconds)
         except Exception as e:  # the baseline is reported, never required
             result["cpu_baseline"] = {"error": str(e)}
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        try:
+            result["accuracy"] = accuracy_report(args, p, s)
+        except Exception as e:  # reported next to the headline, never required
+            result["accuracy"] = {"error": str(e)}
     if rank == 0 and world == 1 and not args.no_surrogate:
         try:
             result["surrogate"] = surrogate_report()
