@@ -23,17 +23,35 @@ import numpy as np
 from . import EUNSUPPORTED, CasimError, ReleaseSiteBatch, configs
 
 
-def split_resident(params, sites, precision):
+def split_by_side(sides_of_sites, n_ch, fits):
     """[(site indices, path)]: the sites ordered by cleft side and RyR count,
-    split at the largest side whose sites the resident path takes (found by
-    bisection over the distinct sides, each probe a batch that is built and
-    released); the rest run on the plain path."""
-    order = np.lexsort((np.asarray(sites["n_ch"]), np.asarray(sites["nx"])))
-    side = np.asarray(sites["nx"])[order]
+    split at the largest side for which fits(indices of the sites with that
+    side or less) holds (bisection over the distinct sides, so fits is
+    called O(log sides) times and must be monotone); the rest run plain."""
+    order = np.lexsort((np.asarray(n_ch), np.asarray(sides_of_sites)))
+    side = np.asarray(sides_of_sites)[order]
     sides = np.unique(side)
+    if sides.size == 0:
+        return []
+    if fits(order[side <= sides[-1]]):
+        return [(order, "resident")]
+    lo, hi = -1, len(sides) - 1  # fits for lo (no site, trivially), not for hi
+    while hi - lo > 1:
+        mid = (lo + hi) // 2
+        if fits(order[side <= sides[mid]]):
+            lo = mid
+        else:
+            hi = mid
+    if lo < 0:
+        return [(order, "plain")]
+    cut = int(np.searchsorted(side, sides[lo], side="right"))
+    return [(order[:cut], "resident"), (order[cut:], "plain")]
 
-    def fits(k):  # the sites with side <= sides[k]
-        idx = order[side <= sides[k]]
+
+def split_resident(params, sites, precision):
+    """split_by_side with the resident path's own answer: each probe builds a
+    batch of the candidate sites on the resident path and releases it."""
+    def fits(idx):
         try:
             ReleaseSiteBatch(params, configs.subset_sites(sites, idx), precision=precision, path="resident").close()
             return True
@@ -42,19 +60,7 @@ def split_resident(params, sites, precision):
                 raise
             return False
 
-    if fits(len(sides) - 1):
-        return [(order, "resident")]
-    lo, hi = -1, len(sides) - 1  # fits(lo) (none, trivially), not fits(hi)
-    while hi - lo > 1:
-        mid = (lo + hi) // 2
-        if fits(mid):
-            lo = mid
-        else:
-            hi = mid
-    if lo < 0:
-        return [(order, "plain")]
-    cut = int(np.searchsorted(side, sides[lo], side="right"))
-    return [(order[:cut], "resident"), (order[cut:], "plain")]
+    return split_by_side(sites["nx"], sites["n_ch"], fits)
 
 
 def run_sweep(n_sites=16384, t_ms=0.2, chunk=200, precision="fp32", seed=5, path="auto"):

@@ -68,3 +68,28 @@ def test_subset_sites_keeps_each_sites_rows():
     assert np.array_equal(sub["ch_x"], np.concatenate([s["ch_x"][off[4]:off[5]], s["ch_x"][off[1]:off[2]]]))
     assert np.array_equal(sub["seeds"], s["seeds"][[4, 1]])
     assert list(sub["first_channel"]) == [s["first_channel"][4], s["first_channel"][1]]
+
+
+def test_sweep_split_by_side():
+    """The sweep's resident/plain split: the largest sides go plain, the
+    threshold is the largest side the predicate accepts, every site lands in
+    exactly one part, and the predicate is probed O(log sides) times."""
+    from casim_b200.sweep import split_by_side
+    rng = np.random.default_rng(0)
+    sides = rng.integers(40, 121, size=500)
+    n_ch = rng.integers(10, 151, size=500)
+    calls = []
+
+    def fits(idx):
+        calls.append(len(idx))
+        return sides[idx].max() <= 108
+
+    parts = split_by_side(sides, n_ch, fits)
+    assert [p for _, p in parts] == ["resident", "plain"]
+    res, pla = parts[0][0], parts[1][0]
+    assert sides[res].max() <= 108 and sides[pla].min() > 108
+    assert sorted(np.concatenate([res, pla]).tolist()) == list(range(500))
+    assert len(calls) <= 1 + int(np.ceil(np.log2(len(np.unique(sides))))) + 1
+    assert split_by_side(sides, n_ch, lambda idx: True)[0][1] == "resident"
+    none = split_by_side(sides, n_ch, lambda idx: False)
+    assert len(none) == 1 and none[0][1] == "plain" and len(none[0][0]) == 500
