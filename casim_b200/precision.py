@@ -18,6 +18,7 @@ states and identical draw counts), and every site enters a two-sample
 Kolmogorov-Smirnov comparison of the release and jSR distributions.
 
     python -m casim_b200.precision --sites 1024 --horizons 10,100
+    python -m casim_b200.precision --distributions 2000
 """
 import argparse
 import json
@@ -109,16 +110,50 @@ def precision_study(n_sites=1024, horizons_ms=(10.0, 100.0), seed=3, chunk=20000
     return out
 
 
+def distribution_study(n_sites=2000, t_ms=1.0, every=100, nadir=2):
+    """Config 1 (2D 64 x 64, 20 RyRs, one RyR opened at t = 0) run `n_sites`
+    times in the mixed precision and `n_sites` times all in FP64 from
+    disjoint seeds; two-sample KS tests of the per-run release-event metrics
+    of the device analysis (peak open RyRs, time to peak, time to end,
+    integral, open probability = mean open count / RyRs) and of the released
+    Ca. Open-RyR counts are sampled every `every` time steps."""
+    from scipy.stats import ks_2samp
+    runs = {}
+    for prec, seed0 in (("fp32", 1), ("fp64", 1 + 10 * n_sites)):
+        p, s = configs.config1(n_sites=n_sites, seed0=seed0)
+        sim = ReleaseSiteBatch(p, s, precision=prec, path="auto")
+        sim.start(s["first_channel"])
+        steps = int(round(t_ms / sim.info.dt_ms))
+        sim.trace_enable(every, steps // every + 1)
+        sim.step(steps)
+        an = sim.release_analysis(t_ms, nadir, hist_dt_ms=every * sim.info.dt_ms)
+        runs[prec] = {"amplitude": an["amp"], "time_to_peak": an["ttp"], "time_to_end": an["tte"],
+                      "integral": an["integral"], "open_probability": an["mean"] / float(s["n_ch"][0]),
+                      "release": np.array([sim.release(k) for k in range(sim.S)])}
+        sim.close()
+    out = {"workload": "config 1, %d runs per precision, %.3g ms, seeds disjoint" % (n_sites, t_ms), "metrics": {}}
+    for k in runs["fp32"]:
+        a, b = runs["fp32"][k], runs["fp64"][k]
+        out["metrics"][k] = {"mean_fp32": float(np.mean(a)), "mean_fp64": float(np.mean(b)),
+                             "ks_p": float(ks_2samp(a, b).pvalue)}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--sites", type=int, default=1024)
     ap.add_argument("--horizons", default="10,100", help="report times in ms, comma separated")
     ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--distributions", type=int, default=0,
+                    help="instead: release-event distributions of this many config-1 runs per precision")
     a = ap.parse_args()
     import torch
     torch.cuda.init()
     t0 = time.time()
-    res = precision_study(a.sites, tuple(float(x) for x in a.horizons.split(",")), seed=a.seed)
+    if a.distributions:
+        res = distribution_study(a.distributions)
+    else:
+        res = precision_study(a.sites, tuple(float(x) for x in a.horizons.split(",")), seed=a.seed)
     res["wall_s"] = time.time() - t0
     print(json.dumps(res))
 
