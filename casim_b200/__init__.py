@@ -35,7 +35,7 @@ EXPORTS = (
     "casim_b200_update", "casim_b200_start", "casim_b200_step", "casim_b200_synchronize",
     "casim_b200_get_field", "casim_b200_set_field", "casim_b200_get_mouth", "casim_b200_get_states",
     "casim_b200_get_jsr", "casim_b200_get_total_current", "casim_b200_get_efflux", "casim_b200_get_cyto",
-    "casim_b200_get_cyto_field", "casim_b200_get_draws", "casim_b200_get_release", "casim_b200_check_finite",
+    "casim_b200_get_cyto_field", "casim_b200_set_cyto_field", "casim_b200_get_draws", "casim_b200_get_release", "casim_b200_check_finite",
     "casim_b200_get_all_mouth", "casim_b200_get_all_states", "casim_b200_last_step_ms",
     "casim_b200_last_step_launches", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
     "casim_b200_rng_draws_static", "casim_b200_path_note",
@@ -110,6 +110,7 @@ def lib():
         for f in ("get_field", "get_mouth", "get_cyto_field"):
             getattr(L, "casim_b200_" + f).argtypes = [vp, i32, i32, dp]
         L.casim_b200_set_field.argtypes = [vp, i32, i32, dp]
+        L.casim_b200_set_cyto_field.argtypes = [vp, i32, i32, dp]
         L.casim_b200_get_states.argtypes = [vp, i32, ip]
         L.casim_b200_get_micro_states.argtypes = [vp, i32, ip]
         L.casim_b200_autotune.argtypes = [vp, i64, ctypes.c_char_p, ctypes.c_size_t]
@@ -180,11 +181,18 @@ class ReleaseSiteBatch:
     Mirrors the reference's compartment interfaces for the RD path:
     DyadSeries (CaSim/DyadSeries.h:9-44), SRSeries (CaSim/SRSeries.h:7-16),
     CytosolSeries (CaSim/CytosolSeries.h:10-21), NSRSeries (CaSim/NSRSeries.h:5-12),
-    stepped together as ParallelHybridSolver does (CaSim/ParallelHybridSolver.cpp:519-548).
+    stepped together as ParallelHybridSolver does (CaSim/ParallelHybridSolver.cpp:408-437).
     """
 
-    def __init__(self, params, sites=None, precision="fp64", path="auto", base_dir=None):
+    def __init__(self, params=None, sites=None, precision="fp64", path="auto", base_dir=None, json_text=None):
+        """params: a Parameters.json dict, or json_text: its text, passed to the library
+        unchanged (relative file names in it resolve from base_dir)."""
         L = lib()
+        if json_text is not None:
+            params = json.loads(json_text)
+            raw = json_text.encode() if isinstance(json_text, str) else bytes(json_text)
+        else:
+            raw = json.dumps(params).encode()
         self.params = params
         prec = {"fp64": FP64, "fp32": FP32}[precision]
         pth = {"auto": PATH_AUTO, "plain": PATH_PLAIN, "resident": PATH_RESIDENT}[path]
@@ -211,7 +219,7 @@ class ReleaseSiteBatch:
             tab.seeds = arr("seeds", np.uint32, ctypes.c_uint32)
             tab.jsr_init = arr("jsr_init", np.float64, ctypes.c_double)
         h = ctypes.c_void_p()
-        st = L.casim_b200_create(json.dumps(params).encode(), (base_dir or "").encode(), prec, pth,
+        st = L.casim_b200_create(raw, (base_dir or "").encode(), prec, pth,
                                  ctypes.byref(tab) if tab is not None else None, ctypes.byref(h))
         if st:
             raise CasimError(st, last_error())
@@ -415,6 +423,11 @@ class ReleaseSiteBatch:
         out = np.zeros(self.info.cyto_nodes, dtype=np.float64)
         self._ck(lib().casim_b200_get_cyto_field(self.h, site, species, _p(out, ctypes.c_double)))
         return out
+
+    def set_cyto_field(self, site, species, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        assert v.size == self.info.cyto_nodes
+        self._ck(lib().casim_b200_set_cyto_field(self.h, site, species, _p(v, ctypes.c_double)))
 
     def release(self, site):
         return float(self._vec("get_release", site, 1)[0])

@@ -154,7 +154,7 @@ def config1(n_sites=100, seed0=1, nx=64, ny=64, n_ryr=20):
         xs += x
         ys += y
         seeds.append([s] * 6)
-    # RunSimulations opens channel (n_threads*i + j)/sc_per_channel (CaSim/ParallelHybridSolver.cpp:521-528)
+    # RunSimulations opens channel (n_threads*i + j)/sc_per_channel (CaSim/ParallelHybridSolver.cpp:411-417)
     first = [0] * n_sites
     return _clean(p), sites_table([nx] * n_sites, [ny] * n_sites, [1] * n_sites, [n_ryr] * n_sites, xs, ys, seeds, first=first)
 

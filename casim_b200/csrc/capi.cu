@@ -921,6 +921,24 @@ casim_status casim_b200_get_cyto_field(casim_h h, int32_t site, int32_t species,
     END_GUARD(h)
 }
 
+casim_status casim_b200_set_cyto_field(casim_h h, int32_t site, int32_t species, const double* in) {
+    GUARD(h)
+    check_site(h, site);
+    if (h->d.m.cyto_type != CB_CYTO_RD3D) throw std::runtime_error("the cytosol is not RD3D");
+    if (species < 0 || species >= h->d.CS) throw std::runtime_error("species out of range");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    size_t rs = h->d.precision == 0 ? 8 : 4;
+    std::vector<char> raw((size_t)h->d.nc * rs);
+    for (int n = 0; n < h->d.nc; ++n) {
+        if (rs == 8) ((double*)raw.data())[n] = in[n];
+        else ((float*)raw.data())[n] = (float)in[n];
+    }
+    char* base = (char*)h->d.cyto[h->d.ccur] + ((size_t)site * h->d.CS + species) * h->d.nc * rs;
+    ck(cudaMemcpy(base, raw.data(), raw.size(), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
 casim_status casim_b200_get_draws(casim_h h, int32_t site, uint64_t* out) {
     GUARD(h)
     cb_site_scalars q;
@@ -952,13 +970,29 @@ casim_status casim_b200_check_finite(casim_h h, int32_t* bad_site) {
         raw.resize((size_t)st[s].npad * m.F * rs);
         const char* base = (const char*)h->d.fields[h->d.cur] + (size_t)st[s].node_base * m.F * rs;
         ck(cudaMemcpy(raw.data(), base, raw.size(), cudaMemcpyDeviceToHost), "cudaMemcpy");
+        // cleft fields, then (RD3D) the site's cytosol grid
+        if (m.cyto_type == CB_CYTO_RD3D && h->d.nc > 0) {
+            const size_t nf = raw.size(), nci = (size_t)h->d.CS * h->d.nc * rs;
+            raw.resize(nf + nci);
+            const char* cb = (const char*)h->d.cyto[h->d.ccur] + (size_t)s * nci;
+            ck(cudaMemcpy(raw.data() + nf, cb, nci, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        }
         size_t n = raw.size() / rs;
-        for (size_t k = 0; k < n; ++k) {
+        bool bad = false;
+        for (size_t k = 0; k < n && !bad; ++k) {
             double v = rs == 8 ? ((double*)raw.data())[k] : (double)((float*)raw.data())[k];
-            if (!std::isfinite(v)) {
-                if (bad_site) *bad_site = s;
-                return set_err(h, CASIM_ENONFINITE, "non-finite value in site " + std::to_string(s));
-            }
+            bad = !std::isfinite(v);
+        }
+        if (!bad) {
+            // FP64 pool scalars: jSR, cytosol pool, release accumulator
+            cb_site_scalars q;
+            ck(cudaMemcpy(&q, h->d.sc + s, sizeof(q), cudaMemcpyDeviceToHost), "cudaMemcpy");
+            for (int j = 0; j < m.n_ions; ++j) bad = bad || !std::isfinite(q.jsr[j]) || !std::isfinite(q.c_ions[j]);
+            bad = bad || !std::isfinite(q.release);
+        }
+        if (bad) {
+            if (bad_site) *bad_site = s;
+            return set_err(h, CASIM_ENONFINITE, "non-finite value in site " + std::to_string(s));
         }
     }
     return CASIM_OK;
@@ -976,6 +1010,12 @@ __global__ void k_debug_rng(cbrng::State g, long long n, double* out) {
 
 extern "C" casim_status casim_b200_debug_rng(const uint32_t seed[6], int64_t n, double* out) {
     if (!seed || !out || n < 0) return set_err(nullptr, CASIM_EINVAL, "bad argument");
+    {
+        // the rules of RngStream's CheckSeed (CaSim/rngstream.cpp:200-234): a seed word at or
+        // above its modulus, or three zero words in one component, is rejected
+        const uint64_t s6[6] = {seed[0], seed[1], seed[2], seed[3], seed[4], seed[5]};
+        if (!cbrng::seed_ok(s6)) return set_err(nullptr, CASIM_EINVAL, "debug_rng: not a valid MRG32k3a seed");
+    }
     try {
         cbrng::State g;
         for (int i = 0; i < 6; ++i) g.s[i] = seed[i];

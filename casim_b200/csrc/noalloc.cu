@@ -9,7 +9,6 @@
 // library holds until the process exits.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/casim_b200.h"
@@ -20,13 +19,9 @@ void cb_set_create_error(const std::string& msg);  // capi.cu
 namespace {
 
 constexpr int64_t CB_STATIC_RNG_MAX = 262144;  // draws per call (2 MiB of doubles)
-constexpr int CB_MAX_DEVICES = 64;
 
 // One staging array per device, shared by every call on that device.
 __device__ __align__(256) double g_rng_scratch[CB_STATIC_RNG_MAX];
-
-std::mutex g_mu;
-double* g_scratch_addr[CB_MAX_DEVICES] = {};
 
 __global__ void k_rng_static(cbrng::State g, long long n, double* out) {
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -45,25 +40,19 @@ extern "C" casim_status casim_b200_rng_draws_static(const uint32_t seed[6], int6
     if (n > CB_STATIC_RNG_MAX)
         return fail(CASIM_EINVAL, "rng_draws_static: " + std::to_string(n) + " draws exceed the fixed scratch of " +
                                       std::to_string(CB_STATIC_RNG_MAX));
-    if (n == 0) return CASIM_OK;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return fail(CASIM_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= CB_MAX_DEVICES) return fail(CASIM_EUNSUPPORTED, "rng_draws_static: device index too large");
-    double* scratch = nullptr;
     {
-        // first call on this device (with it current): resolve the device
-        // address of the array; the host-side name is only a stand-in
-        std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratch_addr[dev]) {
-            e = cudaGetSymbolAddress((void**)&g_scratch_addr[dev], g_rng_scratch);
-            if (e != cudaSuccess) {
-                g_scratch_addr[dev] = nullptr;
-                return fail(CASIM_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            }
-        }
-        scratch = g_scratch_addr[dev];
+        // RngStream's CheckSeed rules (CaSim/rngstream.cpp:200-234)
+        const uint64_t s6[6] = {seed[0], seed[1], seed[2], seed[3], seed[4], seed[5]};
+        if (!cbrng::seed_ok(s6)) return fail(CASIM_EINVAL, "rng_draws_static: not a valid MRG32k3a seed");
     }
+    if (n == 0) return CASIM_OK;
+    // The host-side name of the array is only a stand-in: its device address is
+    // looked up on every call, with the calling thread's current device, so a
+    // context that was torn down and rebuilt (cudaDeviceReset) never leaves a
+    // stale address behind. The lookup is a host-side table read.
+    double* scratch = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&scratch, g_rng_scratch);
+    if (e != cudaSuccess) return fail(CASIM_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     cbrng::State g;
     for (int i = 0; i < 6; ++i) g.s[i] = seed[i];
     // every element read back below is written by this launch first, so the

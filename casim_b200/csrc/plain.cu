@@ -7,7 +7,7 @@
 //   k_rd      cleft RD step of every interior node (CaSim/DyadRD2DCPU.cpp:394-490,
 //             CaSim/DyadRDCPU.cpp:404-506), ping-pong buffers
 //   k_update  one block per site: mouth gather, Dirichlet edges, efflux,
-//             RyR currents, jSR coupling (CaSim/ParallelHybridSolver.cpp:270-286)
+//             RyR currents, jSR coupling (CaSim/ParallelHybridSolver.cpp:159-175)
 //
 // This is the straightforward GPU formulation of the reference step and the
 // denominator of the resident path's speed-up; it handles any site size.

@@ -369,10 +369,18 @@ cudaError_t build_plan(cb_dev& d) {
     if (nz == 0) return cudaErrorInvalidConfiguration;
     std::vector<int> order;
     for (auto& c : classes) order.insert(order.end(), c.begin(), c.end());
-    if ((e = cudaMalloc(&d.rs_order, sizeof(int) * d.S)) != cudaSuccess) return e;
-    if ((e = cudaMemcpy(d.rs_order, order.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&d.rs_counter, sizeof(int) * 8)) != cudaSuccess) return e;
-    if ((e = cb_ensure_pow2(d)) != cudaSuccess) return e;
+    // a failed build leaves no device buffers behind, so that the next call starts clean
+    auto undo = [&](cudaError_t err) {
+        cudaFree(d.rs_order);
+        cudaFree(d.rs_counter);
+        d.rs_order = nullptr;
+        d.rs_counter = nullptr;
+        return err;
+    };
+    if ((e = cudaMalloc(&d.rs_order, sizeof(int) * d.S)) != cudaSuccess) return undo(e);
+    if ((e = cudaMemcpy(d.rs_order, order.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice)) != cudaSuccess) return undo(e);
+    if ((e = cudaMalloc(&d.rs_counter, sizeof(int) * 8)) != cudaSuccess) return undo(e);
+    if ((e = cb_ensure_pow2(d)) != cudaSuccess) return undo(e);
     cb_rs_plan* P = new cb_rs_plan();
     P->nz = nz;
     int offset = 0;
@@ -382,7 +390,7 @@ cudaError_t build_plan(cb_dev& d) {
         if (d.light_rows && !plan(d, sites, classes[k], cs[k], a)) row_weights(a, cs[k], false);
         if (!plan(d, sites, classes[k], cs[k], a)) {
             delete P;
-            return cudaErrorInvalidConfiguration;
+            return undo(cudaErrorInvalidConfiguration);
         }
         a.m = d.m;
         fill_const(d.m, a.kf);
@@ -413,7 +421,7 @@ cudaError_t build_plan(cb_dev& d) {
         e = launch_t(d, a, nz, cs[k], threads, 0, a.S, &clusters);
         if (e != cudaSuccess || clusters < 1) {
             delete P;
-            return e != cudaSuccess ? e : cudaErrorInvalidConfiguration;
+            return undo(e != cudaSuccess ? e : cudaErrorInvalidConfiguration);
         }
         P->args.push_back(a);
         P->cs.push_back(cs[k]);
@@ -424,7 +432,7 @@ cudaError_t build_plan(cb_dev& d) {
     if (P->args.size() > 1) {
         if ((e = cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming)) != cudaSuccess) {
             delete P;
-            return e;
+            return undo(e);
         }
         for (size_t k = 0; k < P->args.size(); ++k) {
             cudaStream_t s = nullptr;
@@ -434,7 +442,7 @@ cudaError_t build_plan(cb_dev& d) {
             if (e != cudaSuccess) {
                 d.rs_plan = P;
                 cb_resident_free(d);
-                return e;
+                return undo(e);
             }
         }
     }

@@ -7,7 +7,7 @@
 //           row on each side, all x and z, every stored species, ping-pong;
 //   RD3D    cytosol planes k in [plo_r, phi_r) of the updated range [0, mc-1),
 //           stored with one halo plane on each side, ping-pong.
-// Per step (the reference loop body CaSim/ParallelHybridSolver.cpp:532-540
+// Per step (the reference loop body CaSim/ParallelHybridSolver.cpp:421-429
 // followed by Update(), :270-286):
 //   phase A  warp 0: RyR gating (CaSim/DyadChannels.cpp:97-130);
 //            warp 1: reductions of the previous Update, jSR coupling, cytosol

@@ -10,7 +10,7 @@
  * Plain C types only. Every call returns a casim_status; on failure
  * casim_b200_last_error() describes it. Handles are not thread-safe: one host
  * thread drives one handle (the reference drives its GPU classes from one
- * thread too, CaSim/ParallelHybridSolver.cpp:497-508).
+ * thread too, CaSim/ParallelHybridSolver.cpp:373-405).
  *
  * Node order used by every field getter/setter is the reference's:
  *   2D: y + ny*x            (CaSim/DyadRD2DCPU.cpp:270-272)
@@ -85,7 +85,7 @@ typedef struct casim_info {
 
 /* Build a batch from a reference-schema Parameters.json text.
  * Replaces the compartment construction in ParallelHybridSolver's constructor
- * (CaSim/ParallelHybridSolver.cpp:169-241) for the dyad, jSR, nSR and cytosol.
+ * (CaSim/ParallelHybridSolver.cpp:13-131) for the dyad, jSR, nSR and cytosol.
  * base_dir resolves relative "Coordinates" paths (may be NULL = cwd).
  * sites may be NULL: then "NumBatch" identical sites are built. */
 casim_status casim_b200_create(const char* json_text, const char* base_dir, casim_precision precision,
@@ -107,17 +107,17 @@ casim_status casim_b200_reset(casim_h h);
 /* DyadSeries::InitOpening(site, channel) (CaSim/DyadSeries.h:20, CaSim/DyadChannels.cpp:83-95):
  * consumes n_channels + 1 draws of the site's stream and opens `channel`. */
 casim_status casim_b200_init_opening(casim_h h, int32_t site, int32_t channel);
-/* The solver's Update() (CaSim/ParallelHybridSolver.cpp:270-286): mouth
+/* The solver's Update() (CaSim/ParallelHybridSolver.cpp:159-175): mouth
  * gather, Dirichlet edges, efflux, RyR currents, pool coupling. */
 casim_status casim_b200_update(casim_h h);
 /* reset + init_opening(site, first_channel[site]) for every site + update, as
- * at the start of each batch in RunSimulations* (CaSim/ParallelHybridSolver.cpp:525-529). */
+ * at the start of each batch in RunSimulations* (CaSim/ParallelHybridSolver.cpp:415-418). */
 casim_status casim_b200_start(casim_h h, const int32_t* first_channel);
 /* Per-site initial jSR concentrations (n_ions values per site) used by the
  * next reset/start: a new batch scenario without rebuilding the handle. */
 casim_status casim_b200_set_site_jsr(casim_h h, const double* jsr_init);
 /* Advance every site by n_steps time steps: per step the cytosol, dyad RD,
- * jSR, gating and Update of CaSim/ParallelHybridSolver.cpp:532-540.
+ * jSR, gating and Update of CaSim/ParallelHybridSolver.cpp:421-429.
  * Replaces DyadSeries::RunRD + RunMC + Update, SRSeries::Run/Update and
  * CytosolSeries::RunRD/Update for the whole batch. Asynchronous on the stream. */
 casim_status casim_b200_step(casim_h h, int64_t n_steps);
@@ -155,16 +155,21 @@ casim_status casim_b200_get_efflux(casim_h h, int32_t site, double* out);
 casim_status casim_b200_get_cyto(casim_h h, int32_t site, double* out);
 /* RD3D cytosol: one species of one site, mc^3 values, x fastest. */
 casim_status casim_b200_get_cyto_field(casim_h h, int32_t site, int32_t species, double* out);
+/* write one species of one site's RD3D cytosol (mc^3 values, x fastest); for
+ * tests and restarts. No counterpart in the reference (it has no 3D cytosol). */
+casim_status casim_b200_set_cyto_field(casim_h h, int32_t site, int32_t species, const double* in);
 /* runif() draws consumed so far by the site's stream */
 casim_status casim_b200_get_draws(casim_h h, int32_t site, uint64_t* out);
 /* Ca released from the jSR so far (FP64 accumulator), in uM*nm^3 */
 casim_status casim_b200_get_release(casim_h h, int32_t site, double* out);
 
-/* Scan every field for NaN/Inf; returns CASIM_ENONFINITE and the first bad
- * site in *bad_site (or -1). */
+/* Scan every site's cleft fields, RD3D cytosol grid and FP64 pool values (jSR,
+ * cytosol pool, release accumulator) for NaN/Inf; returns CASIM_ENONFINITE and
+ * the first bad site in *bad_site (or -1). No counterpart in the reference,
+ * which checks nothing. */
 casim_status casim_b200_check_finite(casim_h h, int32_t* bad_site);
 
-/* Batched host views for drop-in output (CaSim/ParallelHybridSolver.cpp:427-448):
+/* Batched host views for drop-in output (CaSim/ParallelHybridSolver.cpp:316-337):
  * all sites' mouth Ca and channel states in one call each. */
 casim_status casim_b200_get_all_mouth(casim_h h, int32_t species, double* out);  /* sum of channels */
 casim_status casim_b200_get_all_states(casim_h h, int32_t* out);
@@ -221,7 +226,9 @@ casim_status casim_b200_last_step_launches(casim_h h, int64_t* out);
 
 /* Diagnostic: n runif() draws of the MRG32k3a stream with the given seed,
  * generated by a device kernel (the generator every site's gating uses).
- * Reproduces RngStream::RandU01 with incPrec = true (CaSim/rngstream.cpp:271-283). */
+ * Reproduces RngStream::RandU01 with incPrec = true (CaSim/rngstream.cpp:271-283).
+ * A seed that RngStream's CheckSeed rejects (CaSim/rngstream.cpp:200-234) gives
+ * CASIM_EINVAL. */
 casim_status casim_b200_debug_rng(const uint32_t seed[6], int64_t n, double* out);
 
 /* The generator of casim_b200_debug_rng for callers that cannot allocate
@@ -229,11 +236,13 @@ casim_status casim_b200_debug_rng(const uint32_t seed[6], int64_t n, double* out
  * real-time hosts, processes that must not grow their device footprint after
  * start-up). No counterpart in the reference. Its device staging buffer is a
  * fixed array of 262144 doubles (2 MiB) that every GPU loading the library
- * holds until exit; n above that is rejected with CASIM_EINVAL. Calls no
- * allocator. The first call on a device resolves the array's device address
- * with that device current; make it before any stream capture. All calls on a
- * device share the array: calls that overlap on the GPU race. out is host
- * memory. */
+ * holds until exit; n above that is rejected with CASIM_EINVAL, and so is a
+ * seed that RngStream's CheckSeed rejects (CaSim/rngstream.cpp:200-234). Calls
+ * no allocator. Every call looks up the array's device address on the calling
+ * thread's current device, launches on the legacy default stream and copies
+ * the draws back synchronously, so no call may be made while a stream capture
+ * is in progress on that device. All calls on a device share the array: calls
+ * that overlap on the GPU race. out is host memory. */
 casim_status casim_b200_rng_draws_static(const uint32_t seed[6], int64_t n, double* out);
 
 /* ---- Surrogate of the quasi-steady Ca at the RyR mouths (no counterpart in

@@ -17,7 +17,7 @@
  *   cytosol pool         CaSim/CytosolPool.cpp:217-288
  *   RNG                  CaSim/rngstream.cpp:242-283 (MRG32k3a with incPrec = true, U01d)
  *
- * Deliberate differences from the reference, all documented in DESIGN.md:
+ * Deliberate differences from the reference (each one listed here):
  *   - each site draws from its own MRG32k3a stream (the reference hands one
  *     stream to each OpenMP thread); with one site per run they coincide;
  *   - SRPool's beta and NSR lookups use the site's own values (the reference

@@ -5,8 +5,8 @@
  *
  * Every site is an independent dyad with its own grid extents, RyR positions,
  * MRG32k3a stream and jSR/cytosol state. One step follows the reference loop
- * body CaSim/ParallelHybridSolver.cpp:532-540 followed by Update()
- * (CaSim/ParallelHybridSolver.cpp:270-286).
+ * body CaSim/ParallelHybridSolver.cpp:421-429 followed by Update()
+ * (CaSim/ParallelHybridSolver.cpp:159-175).
  */
 #ifndef CASIM_ORACLE_H
 #define CASIM_ORACLE_H

@@ -48,7 +48,7 @@ def lib():
 
 class RefSim:
     """One reference run of `n_batch` sites (NumBatch) driven like
-    ParallelHybridSolver::RunSimulationsCPU (CaSim/ParallelHybridSolver.cpp:519-548)."""
+    ParallelHybridSolver::RunSimulationsCPU (CaSim/ParallelHybridSolver.cpp:408-437)."""
 
     def __init__(self, params: dict, n_batch: int = 1, n_cores: int = 1):
         L = lib()

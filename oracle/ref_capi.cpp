@@ -6,11 +6,11 @@
  *
  * The driver restates only the orchestration of ParallelHybridSolver, which
  * cannot be compiled here (it needs H5Cpp.h):
- *   compartment construction  CaSim/ParallelHybridSolver.cpp:169-241
- *   ResetSystem               CaSim/ParallelHybridSolver.cpp:260-268
- *   Update                    CaSim/ParallelHybridSolver.cpp:270-286
- *   one loop iteration        CaSim/ParallelHybridSolver.cpp:532-540 (RunSimulationsCPU)
- *   initial channel choice    CaSim/ParallelHybridSolver.cpp:521-528
+ *   compartment construction  CaSim/ParallelHybridSolver.cpp:13-131
+ *   ResetSystem               CaSim/ParallelHybridSolver.cpp:149-157
+ *   Update                    CaSim/ParallelHybridSolver.cpp:159-175
+ *   one loop iteration        CaSim/ParallelHybridSolver.cpp:421-429 (RunSimulationsCPU)
+ *   initial channel choice    CaSim/ParallelHybridSolver.cpp:411-417
  * Everything numeric runs inside the reference classes themselves.
  */
 #include <nlohmann/json.hpp>

@@ -39,6 +39,34 @@ def golden_case(z):
     return params, sites
 
 
+def example_case(z):
+    """A fixture of one of the reference's example configs: its Parameters.json text
+    (unchanged), a directory holding the files it names (byte for byte), and the
+    (params, sites) of the one-site run the fixture was made from, for the oracle
+    (absolute file names; the package seed's first stream, as the reference falls
+    back to when the config names no seed)."""
+    import tempfile
+    td = tempfile.mkdtemp(prefix="casim_example_")
+    for k, fn in enumerate(z["file_names"]):
+        with open(os.path.join(td, str(fn)), "wb") as f:
+            f.write(bytes(z["file%d" % k]))
+    text = bytes(z["json_text"]).decode()
+    params = json.loads(text)
+    ch = params["Dyad"]["Channels"]["RyR"]
+    for key in ("Kopen filename", "Kclose filename"):
+        if key in ch:
+            ch[key] = os.path.join(td, ch[key])
+    coords = np.loadtxt(os.path.join(td, ch["Coordinates"]))
+    d = params["Dyad"]
+    sites = {
+        "nx": np.array([int(d["x"] / d["dx"] + 1)], np.int32), "ny": np.array([int(d["y"] / d["dy"] + 1)], np.int32),
+        "nz": np.array([1], np.int32), "n_ch": np.array([len(coords)], np.int32),
+        "ch_x": coords[:, 0].copy(), "ch_y": coords[:, 1].copy(),
+        "seeds": np.full((1, 6), 12345, np.uint32), "jsr_init": None, "first_channel": np.array([0], np.int32),
+    }
+    return text, td, params, sites
+
+
 def species_index(params):
     """name -> species index in the shared order: ions, then ion-buffer pairs (ion-major)."""
     d = params["Dyad"]

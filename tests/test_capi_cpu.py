@@ -64,3 +64,19 @@ def test_unknown_gating_model_is_einval():
     with pytest.raises(cb.CasimError) as e:
         cb.ReleaseSiteBatch(params, sites)
     assert e.value.status == cb.EINVAL
+
+
+@pytest.mark.parametrize("entry", ["casim_b200_debug_rng", "casim_b200_rng_draws_static"])
+@pytest.mark.parametrize("seed", [[0, 0, 0, 1, 1, 1], [1, 1, 1, 0, 0, 0], [4294967087, 1, 1, 1, 1, 1],
+                                  [1, 1, 1, 1, 4294944443, 1]])
+def test_generator_entry_points_apply_checkseed(entry, seed):
+    """RngStream's CheckSeed rules (CaSim/rngstream.cpp:200-234) hold for the stand-alone
+    generator entry points: an invalid seed is EINVAL before any device work."""
+    import ctypes
+    import numpy as np
+    s = np.asarray(seed, dtype=np.uint32)
+    out = np.zeros(4)
+    st = getattr(cb.lib(), entry)(s.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), 4,
+                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert st == cb.EINVAL
+    assert "seed" in cb.last_error()

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle
-from tests.helpers import golden_case, load_golden, species_index
+from tests.helpers import example_case, golden_case, load_golden, species_index
 
 CASES = ["ref2d_sheep", "ref2d_sheep_s3", "ref3d_sheep", "ref2d_mwc", "ref2d_ahtg", "ref2d_spline"]
 # the spline coefficients are solved here by another elimination order than the
@@ -70,3 +70,27 @@ def test_oracle_gating_trajectory():
         assert np.array_equal(sim.states(0), z["states"][k]), "step %d" % ((k + 1) * every)
         assert np.array_equal(sim.mouth(0, 0), z["mouth"][k])
     assert np.array_equal(sim.field(0, 0), z["ca_final"])
+
+
+@pytest.mark.parametrize("name", ["ex_spline_gpu", "ex_iaparov_gpu"])
+def test_oracle_reproduces_reference_examples(name):
+    """The reference's own example configs (examples/SplineGPU: two ions, three buffers,
+    spline-tabulated rates from kopen/kclose_data_v2.txt; examples/IaparovGPU: 60-state
+    SingleSiteMWC gating): the restatement matches the reference's run bit for bit,
+    micro-states included."""
+    z = load_golden(name)
+    _, _, params, sites = example_case(z)
+    sim = oracle.OracleSim(params, sites)
+    sim.start(sites["first_channel"])
+    idx = species_index(params)
+    done = 0
+    for k, n in enumerate(z["steps"]):
+        sim.step(int(n) - done)
+        done = int(n)
+        for key in z.files:
+            if key.startswith("f%d_" % k):
+                assert np.array_equal(sim.field(0, idx[key.split("_", 1)[1]]), z[key]), key
+        states = sim.micro_states(0) if "iaparov" in name else sim.states(0)
+        assert np.array_equal(states, z["s%d" % k])
+        assert np.array_equal(sim.mouth(0, idx["Calcium"]), z["m%d_Calcium" % k])
+        assert np.array_equal(sim.jsr(0)[:2], z["sr%d" % k][[0, 20]])

@@ -60,3 +60,29 @@ def test_single_site_mwc_site_matches_reference(tmp_path):
         assert np.max(np.abs(a - b)) <= 1e-11 * np.max(np.abs(b))
     assert changed >= 10  # the run does make transitions
     assert np.array_equal(o.states(0), (o.micro_states(0) >= 45).astype(np.int32))
+
+
+def test_oracle_matches_reference_on_config1_geometry(tmp_path):
+    """The restatement against the reference's own CPU classes on the exact config-1
+    sites (64 x 64, 20 jittered RyRs, seeds [s]*6, s = 1..4; one NumBatch = 1
+    reference run per site) after 2000 steps, bit for bit."""
+    params, sites = configs.config1(n_sites=4, seed0=1)
+    orc = oracle.OracleSim(params, sites)
+    orc.start(sites["first_channel"])
+    orc.step(2000, threads=4)
+    off = np.concatenate([[0], np.cumsum(sites["n_ch"])])
+    for s in range(4):
+        q = json.loads(json.dumps(params))
+        cpath = os.path.join(str(tmp_path), "c%d.txt" % s)
+        np.savetxt(cpath, np.c_[sites["ch_x"][off[s]:off[s + 1]], sites["ch_y"][off[s]:off[s + 1]]], fmt="%.17g")
+        q["Dyad"]["Channels"]["RyR"]["Coordinates"] = cpath
+        q["Dyad"]["Seed"] = [int(v) for v in sites["seeds"][s]]
+        q["Dyad"]["Type"] = "CPU2D"
+        r = ref.RefSim(q, 1, 1)
+        r.start([int(sites["first_channel"][s])])
+        r.step(2000)
+        assert np.array_equal(r.states(), orc.states(s))
+        assert np.array_equal(r.get("dyad:Calcium"), orc.field(s, 0))
+        assert np.array_equal(r.get("mouth:Calcium"), orc.mouth(s, 0))
+        assert r.get("sr")[0] == orc.jsr(s)[0]
+        r.close()

@@ -1,0 +1,157 @@
+"""Parity of the exact kernel instances the benchmark times, on the benchmark's
+own sites, against the CPU restatement (oracle/, bit-exact to the reference's
+CPU classes where the reference has a counterpart).
+
+* Config-2 sites taken from the bench workload itself (same generator and seed),
+  sides from 45 to 120 nodes x 3 layers, up to 100 RyRs, the full 25^3 RD3D
+  cytosol: the resident path splits them over clusters of 4, 8 and 16 blocks,
+  the classes of the benchmark line. FP32 fields within 1e-5 relative at every
+  node holding more than 1e-3 of its species' largest value, FP64 within 1e-11
+  at every node, after 200 time steps (one bench step).
+* The exact config-1 geometry (64 x 64, 20 jittered RyRs, seeds [s]*6 for
+  s = 1..4), FP64 on both paths against the oracle to 1e-12 over 2000 steps
+  (tests/test_oracle_live_ref.py holds the oracle to the reference's own CPU
+  classes on the same sites).
+"""
+import numpy as np
+import pytest
+
+import casim_b200 as cb
+from casim_b200 import configs
+from oracle import oracle
+from tests.helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+FP32_NODE_TOL = 1e-5     # relative, at nodes above FP32_FLOOR of the species' largest value
+FP32_FLOOR = 1e-3
+FP64_TOL = 1e-11
+
+
+def node_rel_err(a, b, floor=FP32_FLOOR):
+    """Largest relative error over the nodes where |b| exceeds `floor` times max|b|."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    keep = np.abs(b) > floor * np.max(np.abs(b))
+    return float(np.max(np.abs(a[keep] - b[keep]) / np.abs(b[keep]))) if keep.any() else 0.0
+
+
+def bench_sites():
+    """Seven sites of the bench workload (configs.config2 with the bench's seed), the
+    largest site and sites near sides 45, 55, 70, 85, 100 and 110."""
+    params, sites = configs.config2(n_sites=4096, seed=2024)
+    side = np.asarray(sites["nx"])
+    nch = np.asarray(sites["n_ch"])
+    big = int(np.lexsort((nch, side))[-1])  # side 120 with the most RyRs
+    pick = [big]
+    for target in (110, 100, 85, 70, 55, 45):
+        cand = np.where(side == target)[0]
+        pick.append(int(cand[np.argmax(nch[cand])]))
+    return params, configs.subset_sites(sites, pick), pick
+
+
+HORIZONS = (200, 2000)  # one bench step, and 0.1 ms
+
+
+def snapshot(sim, S, F, n_cyto):
+    """States, draw counts, stored cleft species, cytosol species, mouth Ca and jSR of
+    every site (the oracle and the library expose the same getters)."""
+    out = {}
+    for s in range(S):
+        out[("states", s)] = np.asarray(sim.states(s)).copy()
+        out[("draws", s)] = int(sim.draws(s))
+        for sp in range(F):
+            out[("cleft", s, sp)] = np.asarray(sim.field(s, sp)).copy()
+        for c in range(n_cyto):
+            out[("cyto", s, c)] = np.asarray(sim.cyto_field(s, c)).copy()
+        out[("mouth", s)] = np.asarray(sim.mouth(s, 0)).copy()
+        out[("jsr", s)] = np.asarray(sim.jsr(s)).copy()
+    return out
+
+
+@pytest.fixture(scope="module")
+def oracle_snapshots():
+    params, sites, pick = bench_sites()
+    orc = oracle.OracleSim(params, sites)
+    orc.start(sites["first_channel"])
+    snaps, done = {}, 0
+    m = orc.model
+    for h in HORIZONS:
+        orc.step(h - done, threads=8)
+        done = h
+        snaps[h] = snapshot(orc, orc.S, m.n_ions + m.n_pairs, m.n_ions + m.c_n_pairs)
+    return params, sites, snaps, orc.S
+
+
+def test_bench_sites_are_split_like_the_bench(cuda_device, oracle_snapshots):
+    params, sites, _, _ = oracle_snapshots
+    assert int(np.max(sites["nx"])) == 120 and int(np.max(sites["n_ch"])) >= 90
+    sim = cb.ReleaseSiteBatch(params, sites, precision="fp32", path="auto")
+    note = sim.path_note()
+    assert sim.path == "resident", note
+    for c in (4, 8, 16):
+        assert "clusters of %d " % c in note, note
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_bench_sites_match_oracle(cuda_device, oracle_snapshots, precision):
+    """FP32: 1e-5 per node (above 1e-3 of the species' largest value) after one bench
+    step of 200 time steps, 1e-4 after 2000; FP64: 1e-11 at every node at both."""
+    params, sites, snaps, S = oracle_snapshots
+    sim = cb.ReleaseSiteBatch(params, sites, precision=precision, path="auto")
+    if precision == "fp32":  # FP64 side-120 sites fit no 16-block cluster: the plain path
+        assert sim.path == "resident", sim.path_note()
+    sim.start(sites["first_channel"])
+    done = 0
+    for h in HORIZONS:
+        n = h - done
+        if done == 0:  # a one-step launch first, as the oracle's first Update boundary
+            sim.step(1)
+            n -= 1
+        sim.step(n)
+        done = h
+        got = snapshot(sim, S, sim.info.n_ions + sim.info.n_pairs, sim.info.n_cyto_species)
+        ref_ = snaps[h]
+        worst = {}
+        for key, b in ref_.items():
+            a = got[key]
+            if key[0] in ("states",):
+                assert np.array_equal(a, b), (h, key)
+            elif key[0] == "draws":
+                assert a == b, (h, key)
+            else:
+                field = key[0] in ("cleft", "cyto")
+                err = node_rel_err(a, b) if (precision == "fp32" and field) else rel_err(a, b)
+                name = key[0] if not field else (key[0], key[2])
+                worst[name] = max(worst.get(name, 0.0), err)
+        print(precision, h, worst)
+        tol = FP64_TOL if precision == "fp64" else (FP32_NODE_TOL if h <= 200 else 10 * FP32_NODE_TOL)
+        for k, err in worst.items():
+            assert err <= tol, (h, k, err)
+
+
+def _config1_sites():
+    return configs.config1(n_sites=4, seed0=1)
+
+
+@pytest.mark.parametrize("path", ["plain", "resident"])
+def test_config1_geometry_fp64_2000_steps(cuda_device, path):
+    params, sites = _config1_sites()
+    sim = cb.ReleaseSiteBatch(params, sites, precision="fp64", path=path)
+    assert sim.path == path
+    orc = oracle.OracleSim(params, sites)
+    sim.start(sites["first_channel"])
+    orc.start(sites["first_channel"])
+    for chunk in (1, 999, 1000):
+        sim.step(chunk)
+        orc.step(chunk, threads=4)
+    m = orc.model
+    for s in range(4):
+        assert np.array_equal(sim.states(s), orc.states(s))
+        assert sim.draws(s) == orc.draws(s)
+        for sp in range(m.n_ions + m.n_pairs):
+            err = rel_err(sim.field(s, sp), orc.field(s, sp))
+            assert err <= 1e-12, (s, sp, err)
+        assert rel_err(sim.mouth(s, 0), orc.mouth(s, 0)) <= 1e-12
+        assert rel_err(sim.jsr(s), orc.jsr(s)) <= 1e-12
+        assert rel_err(sim.cyto(s), orc.cyto(s)) <= 1e-12

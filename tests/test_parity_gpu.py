@@ -8,7 +8,7 @@ import pytest
 import casim_b200 as cb
 from casim_b200 import configs
 from oracle import oracle
-from tests.helpers import golden_case, load_golden, rel_err, species_index
+from tests.helpers import example_case, golden_case, load_golden, rel_err, species_index
 
 pytestmark = pytest.mark.gpu
 
@@ -61,6 +61,33 @@ def test_fp64_matches_reference_fixture(cuda_device, name, path):
         assert rel_err(sim.jsr(0)[:1], z["sr%d" % k][:1]) <= FP64_TOL
         assert rel_err(sim.cyto(0)[:1], z["cy%d" % k][:1]) <= FP64_TOL
         assert rel_err(sim.total_current(0)[:1], z["tc%d" % k][:1]) <= 1e-10
+
+
+@pytest.mark.parametrize("name", ["ex_spline_gpu", "ex_iaparov_gpu"])
+def test_reference_example_config_loads_unchanged(cuda_device, name):
+    """examples/SplineGPU and examples/IaparovGPU of the reference, their Parameters.json
+    text passed to casim_b200_create as shipped (NumBatch 100, no seed, relative file
+    names resolved from base_dir): site 0 follows the reference's own one-site run
+    (FP64) field for field, RyR for RyR (micro-states for the 60-state model)."""
+    z = load_golden(name)
+    text, base, params, _ = example_case(z)
+    sim = cb.ReleaseSiteBatch(json_text=text, base_dir=base, precision="fp64", path="auto")
+    assert sim.S == int(params["NumBatch"])
+    sim.start(np.zeros(sim.S, np.int32))
+    idx = species_index(params)
+    done = 0
+    for k, n in enumerate(z["steps"]):
+        sim.step(int(n) - done)
+        done = int(n)
+        for key in z.files:
+            if key.startswith("f%d_" % k):
+                err = rel_err(sim.field(0, idx[key.split("_", 1)[1]]), z[key])
+                assert err <= FP64_TOL, (key, err)
+        states = sim.micro_states(0) if "iaparov" in name else sim.states(0)
+        assert np.array_equal(states, z["s%d" % k])
+        assert rel_err(sim.mouth(0, idx["Calcium"]), z["m%d_Calcium" % k]) <= FP64_TOL
+        assert rel_err(sim.jsr(0)[:2], z["sr%d" % k][[0, 20]]) <= FP64_TOL
+    sim.close()
 
 
 @pytest.mark.parametrize("path", PATHS)
@@ -259,3 +286,25 @@ def test_autotune_keeps_the_state_and_the_results(cuda_device):
     sim.step(150)
     orc.step(150)
     _compare_batch(sim, orc, 1e-11)
+
+
+@pytest.mark.parametrize("where", ["cleft", "cytosol"])
+def test_nonfinite_value_is_reported_with_its_site(cuda_device, where):
+    """A NaN written from the host (no device fault involved) is found by
+    casim_b200_check_finite, which names the site and returns CASIM_ENONFINITE."""
+    import ctypes
+    params, sites = configs.small_mixed(n_sites=3, seed=5, dim=3, cytosol="RD3D")
+    sim = cb.ReleaseSiteBatch(params, sites, precision="fp32", path="auto")
+    sim.start(sites["first_channel"])
+    sim.step(20)
+    assert sim.check_finite() == (True, -1)
+    if where == "cleft":
+        f = sim.field(1, 0)
+        f[len(f) // 2] = np.nan
+        sim.set_field(1, 0, f)
+    else:
+        sim.set_cyto_field(1, 0, np.where(np.arange(sim.info.cyto_nodes) == 7, np.inf, sim.cyto_field(1, 0)))
+    bad = ctypes.c_int32(-1)
+    st = cb.lib().casim_b200_check_finite(sim.h, ctypes.byref(bad))
+    assert st == cb.ENONFINITE and bad.value == 1
+    assert "site 1" in cb.last_error(sim.h)
