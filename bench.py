@@ -51,18 +51,62 @@ def parse():
     return ap.parse_args()
 
 
-def workload(args, rank=0):
+def workload(args, world=1):
+    """The global site table of a run on `world` GPUs: `--sites` (default: the
+    config's size) sites per GPU, drawn by one seeded generator, so every rank
+    builds the same table and takes its cost-balanced share (weak scaling)."""
     from casim_b200 import configs
+    per = args.sites
     if args.config == "c1":
-        p, s = configs.config1(n_sites=args.sites or 100, seed0=1 + rank * 100000)
+        p, s = configs.config1(n_sites=(per or 100) * world, seed0=1)
         name = "2D 64x64 cleft, 20 RyR, pool cytosol (config 1 geometry)"
     elif args.config == "c3":
-        p, s = configs.config3(n_sites=args.sites or 1024, seed=3 + rank)
+        p, s = configs.config3(n_sites=(per or 1024) * world, seed=3)
         name = "1024 2D 64x64 clefts, 50 RyR, jSR Ca ~U[0.5,1.5] mM"
     else:
-        p, s = configs.config2(n_sites=args.sites or 4096, seed=2024 + rank)
+        p, s = configs.config2(n_sites=(per or 4096) * world, seed=2024)
         name = "4096 3D dyads side~U{40..120}x3 layers, 10..100 RyR, 25^3 RD cytosol"
     return p, s, name
+
+
+def cyto_nodes_of(params):
+    c = params.get("Cytosol", {})
+    return int(c.get("Nodes", 0)) ** 3 if c.get("Type") == "RD3D" else 0
+
+
+def sharded_run(params, sites, world, rank, make_sim, run):
+    """One rank of a multi-GPU run: this rank's share of the global site table
+    (casim_b200.dist.partition by node-steps), a batch of it from make_sim, the
+    work run(sim, shard) does on it, and the per-site outputs of every rank
+    gathered on rank 0 (None elsewhere). There is no exchange inside the time
+    loop: sites are independent. Returns (sim, shard, run's result, outputs)."""
+    from casim_b200 import dist as cdist
+    idx, mine = cdist.shard_of_rank(sites, cyto_nodes_of(params), world, rank)
+    sim = make_sim(params, mine)
+    res = run(sim, mine)
+    full = cdist.gather_sites(cdist.site_outputs(sim, len(idx)), idx, len(sites["nx"]))
+    return sim, mine, res, full
+
+
+def outputs_summary(full):
+    from casim_b200.dist import SITE_OUTPUT_COLUMNS
+    return {"sites": int(full.shape[0]),
+            **{"sum_" + c: float(full[:, k].sum()) for k, c in enumerate(SITE_OUTPUT_COLUMNS)}}
+
+
+def launch_ranks(args):
+    """`--gpus N` without a torchrun environment: start N ranks of this script
+    under torch.distributed.run (one process per GPU, rendezvous on 127.0.0.1),
+    bounded by a timeout, and return their exit status."""
+    import socket
+    so = socket.socket()
+    so.bind(("127.0.0.1", 0))
+    port = so.getsockname()[1]
+    so.close()
+    cmd = ["timeout", "-k", "60", "1800", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node", str(args.gpus), "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
 
 
 class Clocks:
@@ -134,31 +178,50 @@ def algorithmic_bytes_per_step(sim, sites, params):
     return 2 * w * (cleft * F + cyto * CS)
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_baseline(args, params, sites, budget_s):
     """The CPU restatement (oracle/) on a bounded sample of the same sites,
-    all host threads (one site per thread), timed by wall clock."""
+    all host threads (one site per thread), timed by wall clock; then one site
+    on one thread, the per-core figure."""
     from oracle import oracle
     n_threads = os.cpu_count() or 1
     S = len(sites["nx"])
     sample = min(S, max(n_threads, 8))
-    idx = np.arange(sample)
-    off = np.concatenate([[0], np.cumsum(sites["n_ch"])])
-    sub = {k: (v[idx] if (isinstance(v, np.ndarray) and v.shape[:1] == (S,)) else v) for k, v in sites.items()}
-    sub["ch_x"] = np.concatenate([sites["ch_x"][off[i]:off[i + 1]] for i in idx])
-    sub["ch_y"] = np.concatenate([sites["ch_y"][off[i]:off[i + 1]] for i in idx])
-    o = oracle.OracleSim(params, sub)
-    o.start(sub["first_channel"])
-    o.step(2, n_threads)
-    steps, t0 = 0, time.time()
-    n = 5
-    while time.time() - t0 < budget_s:
-        o.step(n, n_threads)
-        steps += n
-        n = min(n * 2, 200)
-    dt = time.time() - t0
-    site_ms = sample * steps * params_dt_ms(params)
-    return {"value": site_ms / dt, "unit": "site-ms/s", "cores": n_threads, "kind": "port",
-            "sample": "%d of the workload's sites x %d time steps (CPU restatement, OpenMP over sites)" % (sample, steps)}
+    from casim_b200.configs import subset_sites
+
+    def timed(idx, threads, budget):
+        sub = subset_sites(sites, idx)
+        o = oracle.OracleSim(params, sub)
+        o.start(sub["first_channel"])
+        o.step(2, threads)
+        steps, t0 = 0, time.time()
+        n = 5
+        while time.time() - t0 < budget:
+            o.step(n, threads)
+            steps += n
+            n = min(n * 2, 200)
+        dt = time.time() - t0
+        o.close()
+        return len(idx) * steps * params_dt_ms(params) / dt, steps
+
+    v_all, steps = timed(np.arange(sample), n_threads, budget_s)
+    v_one, steps1 = timed(np.arange(1), 1, max(budget_s / 3, 3.0))
+    return {"value": v_all, "unit": "site-ms/s", "cores": n_threads, "kind": "port", "cpu_model": cpu_model(),
+            "sample": "%d of the workload's sites x %d time steps (CPU restatement, OpenMP over sites, %d threads)"
+                      % (sample, steps, n_threads),
+            "one_thread": {"value": v_one, "unit": "site-ms/s",
+                           "sample": "site 0 of the workload x %d time steps on 1 thread" % steps1}}
 
 
 def surrogate_report(sites=2048, sim_steps=20000, batches=8, train_steps=4000):
@@ -314,20 +377,31 @@ def reference_arm(args):
         "impl": "reference", "metric": "simulated site-ms/s", "value": value, "unit": "site-ms/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": name, "cpu_sample": sample_txt},
-        "cpu_baseline": {"value": value, "unit": "site-ms/s", "cores": sample, "kind": "reference", "sample": sample_txt},
+        "config": {"workload": name, "cpu_sample": sample_txt,
+                   "cytosol": "the reference's well-mixed cytosol pool (CaSim/CytosolPool.cpp) in place of the 25^3 RD3D "
+                              "grid, which the reference does not have: about 43 % fewer node-steps per site than the GPU arm"
+                   if cyto_nodes_of(p) else "the reference's well-mixed cytosol pool, as the GPU arm"},
+        "cpu_baseline": {"value": value, "unit": "site-ms/s", "cores": sample, "kind": "reference", "sample": sample_txt,
+                         "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": "site-ms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
 def main():
     args = parse()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    env_world = int(os.environ.get("WORLD_SIZE", "0"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
+        # the reference's CPU classes on the host cores: rank 0 alone (the others exit 0)
         if rank == 0:
             print(json.dumps(reference_arm(args)))
-        return
+        return 0
+    if args.gpus > 1 and env_world == 0:
+        return launch_ranks(args)
+    world = env_world or 1
+    if world != args.gpus:
+        sys.stderr.write("bench.py: --gpus %d but WORLD_SIZE %d\n" % (args.gpus, world))
+        return 2
     import torch
     import casim_b200 as cb
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -336,37 +410,43 @@ def main():
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    p, s, name = workload(args, rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    p, s_global, name = workload(args, world)
     stream = torch.cuda.Stream()
-    sim = cb.ReleaseSiteBatch(p, s, precision=args.precision, path=args.path)
-    sim.set_stream(stream.cuda_stream)
-    sim.start(s["first_channel"])
-    dt_ms = sim.info.dt_ms
-    for _ in range(args.warmup):
-        sim.step(args.chunk)
-    sim.synchronize()
-    launches_per = sim.last_step_launches()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    kernel_ms = []
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with Clocks(local) as clk:
-        with torch.cuda.stream(stream):
-            ev0.record(stream)
-            for _ in range(args.steps):
-                sim.step(args.chunk)
-            ev1.record(stream)
+    timing = {}
+
+    def make_sim(params, sites):
+        sim = cb.ReleaseSiteBatch(params, sites, precision=args.precision, path=args.path)
+        sim.set_stream(stream.cuda_stream)
+        return sim
+
+    def run(sim, sites):
+        sim.start(sites["first_channel"])
+        for _ in range(args.warmup):
+            sim.step(args.chunk)
+        sim.synchronize()
+        timing["launches_per"] = sim.last_step_launches()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    total_sites = sim.S * world
+        with Clocks(local) as clk:
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+                for _ in range(args.steps):
+                    sim.step(args.chunk)
+                ev1.record(stream)
+            torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        from casim_b200 import dist as cdist
+        timing["ms"] = cdist.max_over_ranks(ev0.elapsed_time(ev1), device="cuda")
+        timing["clocks"] = clk.summary()
+
+    sim, s, _, outputs = sharded_run(p, s_global, world, rank, make_sim, run)
+    ms = timing["ms"]
+    dt_ms = sim.info.dt_ms
+    total_sites = len(s_global["nx"])
     value = total_sites * args.chunk * args.steps * dt_ms / (ms / 1e3)
     ok_finite, _ = sim.check_finite()
     # per-launch kernel time of the dominant kernel (resident path: one kernel per bench step)
@@ -375,21 +455,21 @@ def main():
     kms = sim.last_step_ms()
     bytes_step = algorithmic_bytes_per_step(sim, s, p)
     peak, peak_kind = measured_peak_hbm()
-    if sim.path == "resident":
-        achieved = bytes_step * args.chunk / (kms / 1e3) / 1e9
-        kernel_name = "k_resident"
-    else:
-        achieved = bytes_step * args.chunk / (kms / 1e3) / 1e9
-        kernel_name = "plain step (k_pre+k_cyto+k_rd+k_update)"
+    achieved = bytes_step * args.chunk / (kms / 1e3) / 1e9
+    kernel_name = "k_resident" if sim.path == "resident" else "plain step (k_pre+k_cyto+k_rd+k_update)"
     result = {
         "metric": "simulated site-ms/s", "value": value, "unit": "site-ms/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
-        "config": {"workload": name, "sites_per_gpu": sim.S, "time_steps_per_bench_step": args.chunk,
+        "config": {"workload": name, "sites_per_gpu": sim.S, "sites_total": total_sites,
+                   "sharding": "one global table, cost-balanced partition by node-steps (casim_b200.dist.partition); "
+                               "no exchange in the time loop",
+                   "time_steps_per_bench_step": args.chunk,
                    "dt_ns": float(p["dt, ns"]), "path": sim.path, "precision": args.precision,
                    "l2": "state of %.2f GB per GPU is larger than the 126 MB L2" % (bytes_step / 2 / 1e9)},
-        "gpu_launches": int(launches_per * args.steps),
+        "gpu_launches": int(timing["launches_per"] * args.steps),
         "finite": bool(ok_finite),
+        "outputs": outputs_summary(outputs) if rank == 0 else None,
         "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": (RESIDENT_DRAM_BYTES_PER_SITE * sim.S
@@ -398,7 +478,7 @@ def main():
                              "time; the resident path keeps fields on chip, so this is an effective bandwidth; traffic = "
                              "ncu DRAM bytes of the launches of one bench step (0.63 MB per site per launch, measured "
                              "on 512 sites of this workload and scaled by sites)"},
-        "clocks": clk.summary(),
+        "clocks": timing["clocks"],
     }
     if not args.no_e2e:
         # batch scenarios through the public API: new initial conditions in,
@@ -423,7 +503,7 @@ def main():
             el = cdist.max_over_ranks(el, device="cuda")
         result["e2e"] = {"value": total_sites * args.chunk * n_e2e * dt_ms / el, "unit": "site-ms/s",
                          "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": n_e2e}
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             result["cpu_baseline"] = cpu_baseline(args, p, s, args.cpu_seconds)
         except Exception as e:  # the baseline is reported, never required
@@ -443,7 +523,8 @@ def main():
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(result))
+    return 0
 
 
 if __name__ == "__main__":
-    main()
+    sys.exit(main())

@@ -47,6 +47,29 @@ def shard(sites, idx):
     return out
 
 
+def shard_of_rank(sites, cyto_nodes, world, rank):
+    """This rank's sites of a global table: the cost-balanced partition's part
+    `rank` (indices into the global table) and the table restricted to them."""
+    parts = partition(site_cost(sites, cyto_nodes), world)
+    idx = parts[rank]
+    return idx, shard(sites, idx)
+
+
+SITE_OUTPUT_COLUMNS = ("released_ca", "open_ryrs", "draws", "jsr_ca")
+
+
+def site_outputs(sim, n_sites):
+    """Per-site result rows of a batch (library handle or oracle, same getters):
+    released Ca, open RyRs, draws consumed, jSR Ca; [n_sites, 4] float64."""
+    out = np.zeros((n_sites, len(SITE_OUTPUT_COLUMNS)))
+    for k in range(n_sites):
+        out[k, 0] = sim.release(k)
+        out[k, 1] = float(np.sum(sim.states(k)))
+        out[k, 2] = float(sim.draws(k))
+        out[k, 3] = float(sim.jsr(k)[0])
+    return out
+
+
 def max_over_ranks(value, device=None):
     """Maximum of a float over all ranks (the device-time reduction of a timed region)."""
     import torch
