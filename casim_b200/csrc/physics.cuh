@@ -22,17 +22,36 @@ __device__ __forceinline__ double cb_spline(const double* __restrict__ x, const 
     return ((q[3] * h + q[2]) * h + q[1]) * h + q[0];
 }
 
+// x^e for the rate laws: exponents that are multiples of 1/2 up to 8 (the power laws of the
+// shipped configs, 2.5 and 0.5) by repeated squaring and one sqrt, x^(n + 1/2) = x^n sqrt(x);
+// any other exponent by pow. Both agree with pow to a few ulp, far below what could move a
+// gating decision u < rate*dt.
+__device__ __forceinline__ double cb_pow(double x, double e) {
+    const double e2 = 2.0 * e;
+    if (e2 >= 0.0 && e2 <= 16.0 && e2 == (double)(int)e2 && x >= 0.0) {
+        int n = (int)e2 >> 1;
+        double r = (int)e2 & 1 ? sqrt(x) : 1.0, b = x;
+        while (n) {
+            if (n & 1) r *= b;
+            b *= b;
+            n >>= 1;
+        }
+        return r;
+    }
+    return pow(x, e);
+}
+
 __device__ __forceinline__ double cb_rate(const cb_model& m, const double* __restrict__ spx0, const double* __restrict__ spc0,
                                           const double* __restrict__ spx1, const double* __restrict__ spc1, int state, double ca,
                                           double mg) {
     const double* p = m.ch_par;
     switch (m.ch_model) {
     case CB_SHEEP_CANNELL: {
-        // one pow per lane whatever the state (no divergence between open and
-        // closed channels); pow(x, 0) == 1 exactly, so a zero exponent skips it
+        // one power per lane whatever the state (no divergence between open and
+        // closed channels); x^0 == 1 exactly, so a zero exponent skips it
         const double k0 = state ? p[3] : p[0];
         const double ex = state ? p[4] : p[1];
-        const double k = k0 * (ex == 0.0 ? 1.0 : pow(ca * 1e-3, ex));
+        const double k = k0 * (ex == 0.0 ? 1.0 : cb_pow(ca * 1e-3, ex));
         return (state ? k : (p[2] < k ? p[2] : k)) * 1e-3;
     }
     case CB_TWO_STATE_MWC: {
@@ -41,8 +60,9 @@ __device__ __forceinline__ double cb_rate(const cb_model& m, const double* __res
         double inac = p[5] * p[5] / (p[5] * p[5] + mg * mg);
         double a = ca + p[1] * p[0] * (1 + mg / (p[2] * p[3]));
         double b = p[0] * (ca + p[1] * (1 + mg / p[3]));
-        double open = pow(a, 4.0);
-        double close = p[4] * pow(b, 4.0);
+        double a2 = a * a, b2 = b * b;
+        double open = a2 * a2;
+        double close = p[4] * (b2 * b2);
         double P = inac * open / (open + close);
         return kclose * P / (1 - P);
     }

@@ -50,11 +50,11 @@ constexpr int JUMP_ROW = 64;             // pow table row holding A^(2*31*LANE_D
 // Threads per block a kernel is compiled for. A stencil lane keeps three rows
 // of CSM species x NZ layers in registers; FP64 3D layouts with many species
 // get 255 registers per thread (256 threads) instead of 128 (512 threads).
-// block size bound of a specialisation; 16-block clusters stop at 384 threads (three warps
-// per SM sub-partition) so that the step loop keeps its values in registers (168 per
-// thread instead of 128)
+// block size bound of a specialisation; clusters of 4 and more blocks stop at 384 threads
+// (three warps per SM sub-partition) so that the step loop keeps its values in registers (168
+// per thread instead of 128)
 __host__ __device__ constexpr int max_threads(int rbytes, int csm, int nz, int C) {
-    return 3 * nz * csm * rbytes / 4 > 60 ? 256 : C == 16 ? 384 : 512;
+    return 3 * nz * csm * rbytes / 4 > 60 ? 256 : C >= 4 ? 384 : 512;
 }
 // pair capacity of the kernel specialisation that serves NI ions and NP pairs
 __host__ __device__ constexpr int npm_of(int NI, int NP) { return NP <= 2 ? 2 : 4; }
@@ -344,9 +344,21 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                 for (int i = 0; i < nx - 2; ++i) add(2 * ny + nx - 2 + i);
             s_nu = nu;
             if (rank == r0) {
+                // nodes receiving deposits, the longest term lists first (their items go to
+                // different threads of warps 0 and 1)
                 int nd = 0;
                 for (int cn = 0; cn < mc2; ++cn)
                     if (dptr[cn + 1] > dptr[cn]) dnode[nd++] = (unsigned short)cn;
+                for (int i = 1; i < nd; ++i) {
+                    const unsigned short v = dnode[i];
+                    const int lv = dptr[v + 1] - dptr[v];
+                    int j = i - 1;
+                    while (j >= 0 && dptr[dnode[j] + 1] - dptr[dnode[j]] < lv) {
+                        dnode[j + 1] = dnode[j];
+                        --j;
+                    }
+                    dnode[j + 1] = v;
+                }
                 s_nd = nd;
             }
         }
@@ -579,26 +591,41 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                     }
                 }
                 __syncwarp();
-            } else {
+            }
+            if (warp < 2 && rd3d && rank == r0) {
+                // ---- warps 0 and 1, after the gating and the pools: the efflux deposits of the
+                // previous Update per receiving layer-0 cytosol node and deposit slot (each sum
+                // replaces its node's first term, which is all plane 0 reads); the worker warps
+                // meet this at named barrier 1 before their cytosol planes
+                if (it > 0) {
+                    R* tp = terms + (size_t)prv * a.max_terms * FD;
+                    for (int t = tid; t < s_nd * FD; t += 64) {
+                        const int k = t / FD, sl = t - k * FD;
+                        const int cn = dnode[k];
+                        const int q1 = dptr[cn + 1];
+                        int q2 = dptr[cn];
+                        // four interleaved partial sums: under a cleft wider than the cytosol the
+                        // nodes at the cytosol's edge take dozens of terms
+                        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+                        for (; q2 + 4 <= q1; q2 += 4) {
+                            const R t0v = tp[q2 * FD + sl], t1v = tp[(q2 + 1) * FD + sl], t2v = tp[(q2 + 2) * FD + sl],
+                                    t3v = tp[(q2 + 3) * FD + sl];
+                            s0 += (double)t0v;
+                            s1 += (double)t1v;
+                            s2 += (double)t2v;
+                            s3 += (double)t3v;
+                        }
+                        for (; q2 < q1; ++q2) s0 += (double)tp[q2 * FD + sl];
+                        tp[dptr[cn] * FD + sl] = (R)((s0 + s1) + (s2 + s3));
+                    }
+                }
+                asm volatile("bar.arrive 1, %0;" ::"r"(blockDim.x) : "memory");
+            }
+            if (warp >= 2) {
                 // ---- worker warps: cleft stencil, strips of rows with a lane per x.
                 // All FP = NI + NPM species slots are stepped (unused slots hold zeros and
                 // have zero coefficients), so the loops carry no species-count tests;
                 // constants are kernel-parameter operands.
-                if (rd3d && rank == r0 && it > 0) {
-                    // efflux deposits of the previous Update per receiving layer-0 cytosol node
-                    // and deposit slot, summed in the oracle's term order over all worker warps;
-                    // each sum replaces its node's first term, which is all plane 0 reads
-                    R* tp = terms + (size_t)prv * a.max_terms * FD;
-                    for (int t = tid - 64; t < s_nd * FD; t += NWT) {
-                        const int k = t / FD, sl = t - k * FD;
-                        const int cn = dnode[k];
-                        double dep = 0;
-                        for (int q2 = dptr[cn]; q2 < dptr[cn + 1]; ++q2) dep += (double)tp[q2 * FD + sl];
-                        tp[dptr[cn] * FD + sl] = (R)dep;
-                    }
-                    // the worker warps only (warps 0 and 1 do not take part)
-                    asm volatile("bar.sync 1, %0;" ::"r"(NWT) : "memory");
-                }
                 const int wk = warp - 2;
                 for (int t = wk * 32 + lane; t < nxi * nchunk; t += NW * 32) {
                     const int ch = fdiv(t, fd_nxi);
@@ -691,6 +718,7 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                             }
                     }
                 }
+                if (rd3d && rank == r0) asm volatile("bar.sync 1, %0;" ::"r"(blockDim.x) : "memory");
                 if (rd3d) {
                     // RD3D cytosol of this rank (no reference analog; see the oracle):
                     // a thread per (i, j) column marching along z through a chunk of
@@ -804,7 +832,6 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
             double epart[CSM];
 #pragma unroll
             for (int f = 0; f < CSM; ++f) epart[f] = 0;
-            bool did_e = false;
             {
                 R* t0 = peer<C>(terms + (size_t)par * a.max_terms * FD, r0);
                 // one-block sites: the last warps hold the channels (and their rate laws), so
@@ -838,7 +865,6 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                                 if (f < F) fb[f * cap + n] = rim_value(f, ri0 + i);
                         }
                     } else {
-                        did_e = true;
                         int len, x0, y0, dxs, dys, gt0;
                         double sf;
                         if (e < 2) {
@@ -900,7 +926,6 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
 #pragma unroll
             for (int j = 0; j < NI; ++j) tpart[j] = 0;
             const int ct = blockDim.x - 1 - tid;
-            const bool did_t = (W - 1 - warp) * 32 < nch;
             double* pcur = pg + par * a.max_ch;
             for (int c = ct; c < nch; c += blockDim.x) {
                 const int n = chn[c];
@@ -935,25 +960,42 @@ __global__ void __launch_bounds__(max_threads(sizeof(R), NI + NPM, NZ, C), 1) k_
                     for (int b = 0; b < m.n_buf; ++b) mo[F + b] = fr[b];
                 }
             }
-            // warp partials (warps without terms or channels contribute exact zeros)
+            // warp partials (warps without terms or channels contribute exact zeros): the
+            // butterflies of all values run round by round, so their shuffles overlap
+            {
+                double wv[CSM + NI];
 #pragma unroll
-            for (int f = 0; f < CSM; ++f) {
-                if (f < F) {
-                    const double v = did_e ? warp_sum(epart[f]) : 0.0;
-                    if (lane == 0) redw[warp * FDn + f] = v;
+                for (int f = 0; f < CSM; ++f) wv[f] = epart[f];
+#pragma unroll
+                for (int j = 0; j < NI; ++j) wv[CSM + j] = tpart[j];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                    for (int k = 0; k < CSM + NI; ++k) wv[k] += __shfl_xor_sync(0xffffffffu, wv[k], o);
+                if (lane == 0) {
+#pragma unroll
+                    for (int f = 0; f < CSM; ++f)
+                        if (f < F) redw[warp * FDn + f] = wv[f];
+#pragma unroll
+                    for (int j = 0; j < NI; ++j) redw[warp * FDn + F + j] = wv[CSM + j];
                 }
-            }
-#pragma unroll
-            for (int j = 0; j < NI; ++j) {
-                const double v = did_t ? warp_sum(tpart[j]) : 0.0;
-                if (lane == 0) redw[warp * FDn + F + j] = v;
             }
             __syncthreads();
             // rank partials (fixed warp order) into every rank's slot
             if (warp == 0) {
                 double v = 0;
-                if (lane < FDn)
-                    for (int w = 0; w < W; ++w) v += redw[w * FDn + lane];
+                if (lane < FDn) {
+                    // four interleaved sums over the warps (a fixed order: every run and every
+                    // rank forms the same total)
+                    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+                    for (int w = 0; w < W; w += 4) {
+                        s0 += redw[w * FDn + lane];
+                        if (w + 1 < W) s1 += redw[(w + 1) * FDn + lane];
+                        if (w + 2 < W) s2 += redw[(w + 2) * FDn + lane];
+                        if (w + 3 < W) s3 += redw[(w + 3) * FDn + lane];
+                    }
+                    v = (s0 + s1) + (s2 + s3);
+                }
                 // FDn (at most 20) values x C ranks: one store per lane
                 for (int b0 = 0; b0 < FDn * C; b0 += 32) {
                     const int idx = b0 + lane;
