@@ -156,7 +156,7 @@ class Clocks:
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_resident launches of one
 # bench step on 512 sites of the config-2 workload, per site (FP32): each launch loads
 # and stores every site once, so the traffic scales with the sites, not with the steps
-RESIDENT_DRAM_BYTES_PER_SITE = 322.4e6 / 512
+RESIDENT_DRAM_BYTES_PER_SITE = 319.7e6 / 512
 
 
 def measured_peak_hbm():

@@ -30,7 +30,7 @@ _STATUS = {OK: "OK", EINVAL: "EINVAL", ECUDA: "ECUDA", ENOMEM: "ENOMEM", EUNSTAB
 
 # every extern "C" symbol of include/casim_b200.h
 EXPORTS = (
-    "casim_b200_create", "casim_b200_destroy", "casim_b200_info", "casim_b200_species_name",
+    "casim_b200_create", "casim_b200_destroy", "casim_b200_info", "casim_b200_species_name", "casim_b200_cyto_species_name",
     "casim_b200_last_error", "casim_b200_set_stream", "casim_b200_reset", "casim_b200_init_opening",
     "casim_b200_update", "casim_b200_start", "casim_b200_step", "casim_b200_synchronize",
     "casim_b200_get_field", "casim_b200_set_field", "casim_b200_get_mouth", "casim_b200_get_states",
@@ -99,6 +99,7 @@ def lib():
         L.casim_b200_destroy.argtypes = [vp]
         L.casim_b200_info.argtypes = [vp, ctypes.POINTER(Info)]
         L.casim_b200_species_name.argtypes = [vp, i32, ctypes.c_char_p, ctypes.c_size_t]
+        L.casim_b200_cyto_species_name.argtypes = [vp, i32, ctypes.c_char_p, ctypes.c_size_t]
         L.casim_b200_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         L.casim_b200_set_stream.argtypes = [vp, vp]
         L.casim_b200_reset.argtypes = [vp]
@@ -273,6 +274,11 @@ class ReleaseSiteBatch:
     def species_name(self, k):
         buf = ctypes.create_string_buffer(256)
         self._ck(lib().casim_b200_species_name(self.h, k, buf, 256))
+        return buf.value.decode()
+
+    def cyto_species_name(self, k):
+        buf = ctypes.create_string_buffer(256)
+        self._ck(lib().casim_b200_cyto_species_name(self.h, k, buf, 256))
         return buf.value.decode()
 
     @property

@@ -337,6 +337,18 @@ casim_status casim_b200_species_name(casim_h h, int32_t index, char* buf, size_t
     return CASIM_OK;
 }
 
+casim_status casim_b200_cyto_species_name(casim_h h, int32_t index, char* buf, size_t n) {
+    if (!h || !buf || !n) return CASIM_EINVAL;
+    const cb_config& c = h->cfg;
+    int ni = (int)c.ion_names.size(), np = (int)c.cyto_pair_names.size();
+    if (index < 0 || index >= ni + np) return set_err(h, CASIM_EINVAL, "cytosol species index out of range");
+    const std::string& name = index < ni ? c.ion_names[index] : c.cyto_pair_names[index - ni];
+    size_t k = std::min(n - 1, name.size());
+    std::memcpy(buf, name.data(), k);
+    buf[k] = 0;
+    return CASIM_OK;
+}
+
 casim_status casim_b200_set_stream(casim_h h, void* s) {
     if (!h) return CASIM_EINVAL;
     cudaStreamSynchronize(h->stream);

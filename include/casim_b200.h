@@ -94,6 +94,10 @@ casim_status casim_b200_destroy(casim_h h);
 casim_status casim_b200_info(casim_h h, casim_info* out);
 /* Name of species `index` (ions, pairs as "<ion>-<buffer>", free buffers). */
 casim_status casim_b200_species_name(casim_h h, int32_t index, char* buf, size_t n);
+/* Name of cytosol species `index` (ions, then the cytosol's ion-buffer pairs as
+ * "<ion>-<buffer>"), the keys of CytosolSeries::GetConcentrations
+ * (CaSim/CytosolPool.cpp:331-357). */
+casim_status casim_b200_cyto_species_name(casim_h h, int32_t index, char* buf, size_t n);
 casim_status casim_b200_last_error(casim_h h, char* buf, size_t n);
 
 /* Use this CUDA stream (a cudaStream_t) for all work of the handle; NULL = the
