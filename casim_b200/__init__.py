@@ -31,6 +31,9 @@ _STATUS = {OK: "OK", EINVAL: "EINVAL", ECUDA: "ECUDA", ENOMEM: "ENOMEM", EUNSTAB
 # every extern "C" symbol of include/casim_b200.h
 EXPORTS = (
     "casim_b200_create", "casim_b200_destroy", "casim_b200_info", "casim_b200_species_name", "casim_b200_cyto_species_name",
+    "casim_b200_qs_create", "casim_b200_qs_destroy", "casim_b200_qs_last_error", "casim_b200_qs_info", "casim_b200_qs_increments",
+    "casim_b200_qs_run", "casim_b200_qs_last_run_ms", "casim_b200_qs_event_count", "casim_b200_qs_events", "casim_b200_qs_draws",
+    "casim_b200_qs_analysis",
     "casim_b200_last_error", "casim_b200_set_stream", "casim_b200_reset", "casim_b200_init_opening",
     "casim_b200_update", "casim_b200_start", "casim_b200_step", "casim_b200_synchronize",
     "casim_b200_get_field", "casim_b200_set_field", "casim_b200_get_mouth", "casim_b200_get_states",
@@ -100,6 +103,18 @@ def lib():
         L.casim_b200_info.argtypes = [vp, ctypes.POINTER(Info)]
         L.casim_b200_species_name.argtypes = [vp, i32, ctypes.c_char_p, ctypes.c_size_t]
         L.casim_b200_cyto_species_name.argtypes = [vp, i32, ctypes.c_char_p, ctypes.c_size_t]
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        L.casim_b200_qs_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, u32p, i64, ctypes.POINTER(vp)]
+        L.casim_b200_qs_destroy.argtypes = [vp]
+        L.casim_b200_qs_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+        L.casim_b200_qs_info.argtypes = [vp, ip, ip, dp]
+        L.casim_b200_qs_increments.argtypes = [vp, dp]
+        L.casim_b200_qs_run.argtypes = [vp, ip]
+        L.casim_b200_qs_last_run_ms.argtypes = [vp, dp]
+        L.casim_b200_qs_event_count.argtypes = [vp, i32, ctypes.POINTER(i64)]
+        L.casim_b200_qs_events.argtypes = [vp, i32, dp, ip, ip]
+        L.casim_b200_qs_draws.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_uint64)]
+        L.casim_b200_qs_analysis.argtypes = [vp, i32, dp, ip]
         L.casim_b200_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         L.casim_b200_set_stream.argtypes = [vp, vp]
         L.casim_b200_reset.argtypes = [vp]
@@ -447,3 +462,92 @@ class ReleaseSiteBatch:
         bad = ctypes.c_int32(-1)
         st = lib().casim_b200_check_finite(self.h, ctypes.byref(bad))
         return st == OK, bad.value
+
+
+class QuasiStationarySites:
+    """Quasi-stationary release sites simulated with Gillespie's method on the device:
+    the reference's ParallelSolver path (CaSim/ParallelSolver.cpp:51-143,
+    CaSim/QuasyStationaryReleaseSite.cpp:89-133) with the mouth Ca of the linearised
+    Naraghi-Neher model (CaSim/LinearNaraghiNeher.cpp:9-75), one scenario per warp."""
+
+    def __init__(self, params, n_scenarios, base_dir=None, seeds=None, max_events=4096, json_text=None):
+        L = lib()
+        raw = json_text.encode() if json_text is not None else json.dumps(params).encode()
+        sd = None
+        if seeds is not None:
+            self._seeds = np.ascontiguousarray(seeds, dtype=np.uint32).reshape(n_scenarios, 6)
+            sd = _p(self._seeds, ctypes.c_uint32)
+        h = ctypes.c_void_p()
+        st = L.casim_b200_qs_create(raw, (base_dir or "").encode(), int(n_scenarios), sd, int(max_events), ctypes.byref(h))
+        if st:
+            raise CasimError(st, self._err(None))
+        self.h = h
+        self.S = int(n_scenarios)
+        nc, ns, mt = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+        L.casim_b200_qs_info(self.h, ctypes.byref(nc), ctypes.byref(ns), ctypes.byref(mt))
+        self.n_ch, self.max_time = nc.value, mt.value
+        self.max_events = int(max_events)
+
+    @staticmethod
+    def _err(h):
+        buf = ctypes.create_string_buffer(1024)
+        lib().casim_b200_qs_last_error(h, buf, 1024)
+        return buf.value.decode()
+
+    def _ck(self, st):
+        if st:
+            raise CasimError(st, self._err(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().casim_b200_qs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def increments(self):
+        out = np.zeros((self.n_ch, self.n_ch))
+        self._ck(lib().casim_b200_qs_increments(self.h, _p(out, ctypes.c_double)))
+        return out
+
+    def run(self, first_channel):
+        fc = np.ascontiguousarray(first_channel, dtype=np.int32).reshape(self.S)
+        self._ck(lib().casim_b200_qs_run(self.h, _p(fc, ctypes.c_int32)))
+
+    def last_run_ms(self):
+        v = ctypes.c_double()
+        self._ck(lib().casim_b200_qs_last_run_ms(self.h, ctypes.byref(v)))
+        return v.value
+
+    def events(self, scenario):
+        """(times, channels, new states) of the scenario's stored events, in order
+        (the first max_events of them)."""
+        k = min(self.event_count(scenario), self.max_events)
+        t = np.zeros(k)
+        c = np.zeros(k, dtype=np.int32)
+        s = np.zeros(k, dtype=np.int32)
+        self._ck(lib().casim_b200_qs_events(self.h, scenario, _p(t, ctypes.c_double), _p(c, ctypes.c_int32), _p(s, ctypes.c_int32)))
+        return t, c, s
+
+    def event_count(self, scenario):
+        """Events of the scenario's last run, stored or not."""
+        n = ctypes.c_int64()
+        self._ck(lib().casim_b200_qs_event_count(self.h, scenario, ctypes.byref(n)))
+        return n.value
+
+    def draws(self, scenario):
+        v = ctypes.c_uint64()
+        self._ck(lib().casim_b200_qs_draws(self.h, scenario, ctypes.byref(v)))
+        return int(v.value)
+
+    def analysis(self, nadir):
+        """per scenario [amplitude, time to peak, time to end, integral, mean] and the
+        class counts (quarks, blips, sparks)."""
+        out = np.zeros((self.S, 5))
+        cls = np.zeros(3, dtype=np.int32)
+        self._ck(lib().casim_b200_qs_analysis(self.h, int(nadir), _p(out, ctypes.c_double), _p(cls, ctypes.c_int32)))
+        return out, cls

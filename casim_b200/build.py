@@ -13,7 +13,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcasim_b200.so")
 SOURCES = ["resident_f64_z3.cu", "resident_f32_z3.cu", "resident_f64_z1.cu", "resident_f32_z1.cu", "capi.cu", "plain.cu",
-           "resident.cu", "noalloc.cu", "surrogate.cu", "sg_gate.cu", "analysis.cu", "parse.cpp"]
+           "resident.cu", "noalloc.cu", "surrogate.cu", "sg_gate.cu", "analysis.cu", "qs.cu", "parse.cpp"]
 HEADERS = ["model.h", "engine.h", "physics.cuh", "mrg32k3a.cuh", "parse.h", "resident_kernel.cuh", "pools.cuh", "mwc.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -41,11 +41,14 @@ __device__ __forceinline__ double cb_pow(double x, double e) {
     return pow(x, e);
 }
 
+// MODEL >= 0 fixes the rate law at compile time (kernels instantiated per model);
+// the default reads it from m.ch_model.
+template <int MODEL = -1>
 __device__ __forceinline__ double cb_rate(const cb_model& m, const double* __restrict__ spx0, const double* __restrict__ spc0,
                                           const double* __restrict__ spx1, const double* __restrict__ spc1, int state, double ca,
                                           double mg) {
     const double* p = m.ch_par;
-    switch (m.ch_model) {
+    switch (MODEL >= 0 ? MODEL : m.ch_model) {
     case CB_SHEEP_CANNELL: {
         // one power per lane whatever the state (no divergence between open and
         // closed channels); x^0 == 1 exactly, so a zero exponent skips it

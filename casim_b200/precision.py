@@ -132,11 +132,29 @@ def distribution_study(n_sites=2000, t_ms=1.0, every=100, nadir=2):
                       "release": np.array([sim.release(k) for k in range(sim.S)])}
         sim.close()
     out = {"workload": "config 1, %d runs per precision, %.3g ms, seeds disjoint" % (n_sites, t_ms), "metrics": {}}
+    rng = np.random.default_rng(12345)
     for k in runs["fp32"]:
-        a, b = runs["fp32"][k], runs["fp64"][k]
-        out["metrics"][k] = {"mean_fp32": float(np.mean(a)), "mean_fp64": float(np.mean(b)),
-                             "ks_p": float(ks_2samp(a, b).pvalue)}
+        a, b = np.asarray(runs["fp32"][k], float), np.asarray(runs["fp64"][k], float)
+        row = {"mean_fp32": float(np.mean(a)), "mean_fp64": float(np.mean(b))}
+        if k == "time_to_end" and np.all(a >= t_ms - 1e-9) and np.all(b >= t_ms - 1e-9):
+            # no event ended inside the window: censored at t_ms in every run, no test
+            row["censored_at_ms"] = t_ms
+        else:
+            row["ks_p"] = float(ks_2samp(a, b).pvalue)
+            row.update(bootstrap_mean_difference(a, b, rng))
+        out["metrics"][k] = row
     return out
+
+
+def bootstrap_mean_difference(a, b, rng, n_boot=2000, level=0.95):
+    """Percentile bootstrap interval of mean(a) - mean(b) (the two samples resampled
+    independently): whether a difference of the means is inside sampling noise."""
+    d = np.empty(n_boot)
+    for i in range(n_boot):
+        d[i] = np.mean(rng.choice(a, a.size)) - np.mean(rng.choice(b, b.size))
+    lo, hi = np.percentile(d, [50 * (1 - level), 50 * (1 + level)])
+    return {"mean_difference": float(np.mean(a) - np.mean(b)), "ci95": [float(lo), float(hi)],
+            "difference_inside_noise": bool(lo <= 0.0 <= hi)}
 
 
 def main():

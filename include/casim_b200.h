@@ -249,6 +249,44 @@ casim_status casim_b200_debug_rng(const uint32_t seed[6], int64_t n, double* out
  * that overlap on the GPU race. out is host memory. */
 casim_status casim_b200_rng_draws_static(const uint32_t seed[6], int64_t n, double* out);
 
+/* ---- Quasi-stationary release sites: the reference's ParallelSolver path
+ * (CaSim/ParallelSolver.cpp:51-143, CaSim/QuasyStationaryReleaseSite.cpp:89-133)
+ * batched on the device, one scenario per warp. The mouth Ca of every RyR is the
+ * background plus the linearised Naraghi-Neher increments of the open RyRs
+ * (CaSim/LinearNaraghiNeher.cpp:9-75, computed on the host); gating is simulated
+ * exactly with Gillespie's method (total rate, exponential waiting time, channel
+ * picked by its share, its transition) until no RyR is open or "Max Time" is
+ * reached. The JSON is the reference's ParallelSolver schema ("Calcium Release
+ * Site" with "Parameters" / "Channels" / "Dyadic Cleft" / "Open Concentration");
+ * two-state models (TwoStateMWC, TwoStateaHTG, SheepCannell), 1 to 1024 RyRs. seeds: 6 words per
+ * scenario, or NULL for stream s of the package seed 12345 x 6; the streams carry on
+ * from run to run. Each scenario keeps up to max_events events (time, channel, new
+ * state). */
+typedef struct casim_qs_s* casim_qs;
+casim_status casim_b200_qs_create(const char* json_text, const char* base_dir, int32_t n_scenarios, const uint32_t* seeds,
+                                  int64_t max_events, casim_qs* out);
+casim_status casim_b200_qs_destroy(casim_qs h);
+casim_status casim_b200_qs_last_error(casim_qs h, char* buf, size_t n);
+casim_status casim_b200_qs_info(casim_qs h, int32_t* n_channels, int32_t* n_scenarios, double* max_time);
+/* the increments [i][j]: Ca (uM) at RyR j from open RyR i (the "Open Concentration" at i itself) */
+casim_status casim_b200_qs_increments(casim_qs h, double* out);
+/* one run of every scenario, RyR first_channel[s] opened at t = 0
+ * (CaSim/QuasyStationaryReleaseSite.cpp:92-98); synchronous. CASIM_EUNSUPPORTED when a
+ * scenario had more events than max_events (its trace is truncated), CASIM_ETIMEOUT when
+ * one was stopped after 64 x max_events events. */
+casim_status casim_b200_qs_run(casim_qs h, const int32_t* first_channel);
+casim_status casim_b200_qs_last_run_ms(casim_qs h, double* out);
+/* events of the scenario's last run, stored or not (at most max_events are stored) */
+casim_status casim_b200_qs_event_count(casim_qs h, int32_t scenario, int64_t* n);
+/* the scenario's stored events in order: time (ms), channel, its new state (1 open);
+ * min(event count, max_events) of them */
+casim_status casim_b200_qs_events(casim_qs h, int32_t scenario, double* t, int32_t* channel, int32_t* state);
+casim_status casim_b200_qs_draws(casim_qs h, int32_t scenario, uint64_t* out);
+/* per scenario [5]: amplitude (most open RyRs), time to peak, time to end, integral of
+ * the open count, its mean, and the class counts (quarks, blips up to nadir, sparks), as
+ * IndChannelCREAnalyzer::RunAnalysis (CaSim/IndChannelCREAnalyzer.cpp:64-118). */
+casim_status casim_b200_qs_analysis(casim_qs h, int32_t nadir, double* per_scenario, int32_t* class_counts);
+
 /* ---- Surrogate of the quasi-steady Ca at the RyR mouths (no counterpart in
  * the reference; the plain RD step above generates its training snapshots and
  * judges its error). An MLP n_in -> depth x width (GELU) -> n_out with BF16

@@ -1035,3 +1035,71 @@ long or_get_cyto_field(const or_sim* s, int site, int species, double* out) {
 
 uint64_t or_draws(const or_sim* s, int site) { return s->site[site].draws; }
 double or_release(const or_sim* s, int site) { return s->site[site].release; }
+
+/* ------------------------------------------ quasi-stationary release site (Gillespie)
+ * One scenario of CaSim/QuasyStationaryReleaseSite.cpp:89-133 with two-state channels:
+ * every channel set closed (one draw each), `first` opened (one draw); then, while a
+ * channel is open and t < max_time: mouth Ca c_j = sum over open i of added[i][j] (in
+ * channel order) + bg, rates at (c_j, mg), total in channel order, t += -log(u) / total
+ * (ParallelRng::rexp), channel picked by the running share p <= r <= p + rate/total, its
+ * transition (one more draw). The stream state in seed6 is advanced in place. Events
+ * (time, channel, new state) beyond max_events are counted but not stored. Returns the
+ * event count. */
+long or_qs_run(const or_model* m, int n_ch, const double* added, double bg, double mg, double max_time, uint32_t* seed6,
+               int first, long max_events, double* ev_t, int* ev_c, int* ev_s, uint64_t* draws) {
+    mrg_t g;
+    for (int i = 0; i < 6; ++i) g.s[i] = seed6[i];
+    int* st = (int*)calloc((size_t)n_ch, sizeof(int));
+    double* rt = (double*)malloc(sizeof(double) * (size_t)n_ch);
+    double ions[OR_MAX_IONS] = {0};
+    uint64_t nd = 0;
+    for (int i = 0; i < n_ch; ++i) {
+        mrg_u01d(&g);
+        st[i] = 0;
+    }
+    mrg_u01d(&g);
+    st[first] = 1;
+    nd = (uint64_t)n_ch + 1;
+    int n_open = 1;
+    double t = 0;
+    long ne = 0;
+    while (n_open >= 1 && t < max_time) {
+        double total = 0;
+        for (int j = 0; j < n_ch; ++j) {
+            double c = 0;
+            for (int i = 0; i < n_ch; ++i) c += st[i] * added[(long)i * n_ch + j];
+            c += bg;
+            ions[m->ca_idx] = c;
+            if (m->mg_idx >= 0) ions[m->mg_idx] = mg;
+            rt[j] = rate(m, st[j], ions, NULL);
+        }
+        for (int j = 0; j < n_ch; ++j) total += rt[j];
+        double theta = 1 / total;
+        t += -log(mrg_u01d(&g)) * theta;
+        double r = mrg_u01d(&g);
+        double p = 0;
+        int idx = 0;
+        for (int i = 0; i < n_ch; ++i) {
+            if (p <= r && r <= p + rt[i] / total) {
+                idx = i;
+                break;
+            }
+            p += rt[i] / total;
+        }
+        mrg_u01d(&g);
+        nd += 3;
+        st[idx] = 1 - st[idx];
+        n_open += st[idx] ? 1 : -1;
+        if (ne < max_events) {
+            ev_t[ne] = t;
+            ev_c[ne] = idx;
+            ev_s[ne] = st[idx];
+        }
+        ++ne;
+    }
+    for (int i = 0; i < 6; ++i) seed6[i] = (uint32_t)g.s[i];
+    if (draws) *draws = nd;
+    free(st);
+    free(rt);
+    return ne;
+}

@@ -107,4 +107,7 @@ double or_release(const or_sim* s, int site);                       /* accumulat
 /* MRG32k3a (L'Ecuyer 1999 / RngStreams 2002) helpers for tests */
 void or_mrg_u01d(const uint32_t seed[6], long n, double* out);
 void or_mrg_jump(const uint32_t seed[6], int log2_steps, long mult, uint32_t out[6]);
+/* one quasi-stationary Gillespie scenario (CaSim/QuasyStationaryReleaseSite.cpp:89-133) */
+long or_qs_run(const or_model* m, int n_ch, const double* added, double bg, double mg, double max_time, uint32_t* seed6,
+               int first, long max_events, double* ev_t, int* ev_c, int* ev_s, uint64_t* draws);
 #endif

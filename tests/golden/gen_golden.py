@@ -194,6 +194,56 @@ def run_example(name, example, steps, n_fields_every=None):
     print("wrote", name, "transitions over", steps, [int(out["s%d" % k].sum()) for k in range(len(steps))])
 
 
+QS_PARAMS = {"Calcium Release Site": {
+    "Type": "QuasyStationary", "Name": "LinearNaraghiNeher", "Max Time": 50.0,
+    "Parameters": {
+        "Channels": {"RyR": {"Coordinates": "coords.txt", "Model": "TwoStateMWC", "Current": 4.0,
+                             "Parameters": {"fCa": 0.00583687, "KCa": 4.1834575, "fMg": 3.2517014, "KMg": 92.2954937,
+                                            "KO0": 10800, "KMgI": 546.4, "kclose": 0.59}}},
+        "Dyadic Cleft": {"Ions": {"Calcium": {"Concentration": 0.1, "D": 2.2e-6}, "Magnesium": {"Concentration": 1000.0}},
+                         "Buffers": {"ATP": {"kon": 0.225, "koff": 45.0, "D": 1.408e-6, "Total Concentration": 2000.0},
+                                     "Calmodulin": {"kon": 0.1, "koff": 0.038, "D": 2.42e-7, "Total Concentration": 24.0}}},
+        "Open Concentration": 100.0}}}
+
+
+def qs_fixture(name, n_scen=40):
+    """The reference's own quasi-stationary Gillespie loop (CaSim/QuasyStationaryReleaseSite.cpp)
+    over n_scen scenarios on one stream (a one-thread ParallelSolver), with the increments
+    of the CPU restatement installed in place of the Eigen-based LinearNaraghiNeher
+    constructor (oracle/ref_qs.cpp): the channel-state rows of every scenario."""
+    from casim_b200 import configs
+    from oracle import qs_oracle
+    xs, ys = configs.lattice(20, 150.0, 150.0, np.random.default_rng(1))
+    coords = np.c_[xs, ys]
+    with tempfile.TemporaryDirectory() as td:
+        np.savetxt(os.path.join(td, "coords.txt"), coords, fmt="%.17g")
+        p = json.loads(json.dumps(QS_PARAMS))
+        p["Calcium Release Site"]["Parameters"]["Channels"]["RyR"]["Coordinates"] = os.path.join(td, "coords.txt")
+        added = np.ascontiguousarray(qs_oracle.naraghi_neher(qs_oracle.parse(p)))
+        L = ref.lib()
+        L.qsref_set_increments.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.qsref_run.restype = ctypes.c_long
+        L.qsref_run.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_ulong), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                ctypes.c_long]
+        L.qsref_set_increments(len(coords), added.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        first = (np.arange(n_scen) % len(coords)).astype(np.int32)
+        mr = 200000
+        rt = np.zeros(mr)
+        rs = np.zeros(mr * len(coords), dtype=np.int32)
+        rps = np.zeros(n_scen, dtype=np.int32)
+        seed = (ctypes.c_ulong * 6)(*([12345] * 6))
+        tot = L.qsref_run(json.dumps(p).encode(), seed, n_scen, first.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                          rt.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                          rps.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), mr)
+        assert 0 < tot <= mr
+    out = {"params": np.frombuffer(json.dumps(QS_PARAMS).encode(), dtype=np.uint8), "coords": coords,
+           "increments": added, "first": first, "rows_per_scenario": rps, "row_t": rt[:tot],
+           "row_states": rs[:tot * len(coords)].reshape(tot, len(coords)).astype(np.int8)}
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print("wrote", name, "rows", tot)
+
+
 def main():
     global REF_DIR
     ap = argparse.ArgumentParser()
@@ -253,6 +303,8 @@ def main():
     pf["Dyad"]["Channels"]["RyR"]["Parameters"].update({"kopen0": 4e5, "ncaopen": 0.5, "kopenmax": 8e5, "kclose0": 245.0 * 40})
     if want("ref2d_fastgating"):
         run_trajectory("ref2d_fastgating", pf, coords_text(), 4000, 50, [21] * 6, first=2)
+    if want("qs_mwc"):
+        qs_fixture("qs_mwc")
     # the reference's own example configs, loaded unchanged (two ions, three buffers,
     # spline-tabulated and 60-state MWC gating)
     # spline-tabulated and 60-state MWC gating). They name no seed, so the reference
