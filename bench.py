@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate-versus-RD report")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the mouth-Ca error check against FP64")
+    ap.add_argument("--no-qs", action="store_true", help="skip the quasi-stationary (Gillespie) report")
     return ap.parse_args()
 
 
@@ -319,6 +320,90 @@ def accuracy_report(args, params, sites, n_sites=64, steps=2000):
             "mouth_ca_rel_err_median": r["mouth_ca_rel_err"]["median"], "release_rel_err_max": r["release_rel_err"]["max"]}
 
 
+def qs_cpu_baseline(params, coords, added, budget_s):
+    """Scenarios per second of one host thread: the reference's own quasi-stationary
+    loop (oracle/_ref) where it was built, else the CPU restatement."""
+    import tempfile
+    td = tempfile.mkdtemp()
+    np.savetxt(os.path.join(td, "coords.txt"), coords, fmt="%.17g")
+    from oracle import ref
+    p = json.loads(json.dumps(params))
+    p["Calcium Release Site"]["Parameters"]["Channels"]["RyR"]["Coordinates"] = os.path.join(td, "coords.txt")
+    L = ref.lib() if ref.available() else None
+    s6 = (12345,) * 6  # every chunk replays the package seed's stream from its start
+    if L is not None and hasattr(L, "qsref_run"):
+        L.qsref_set_increments.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.qsref_run.restype = ctypes.c_long
+        L.qsref_run.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_ulong), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                ctypes.c_long]
+        a = np.ascontiguousarray(added)
+        L.qsref_set_increments(len(coords), a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        n, done, t0 = 64, 0, time.time()
+        while time.time() - t0 < budget_s:
+            mr = 400 * n
+            rt, rs, rps = np.zeros(mr), np.zeros(mr * len(coords), np.int32), np.zeros(n, np.int32)
+            fc = (np.arange(done, done + n) % len(coords)).astype(np.int32)
+            seed = (ctypes.c_ulong * 6)(*s6)
+            L.qsref_run(json.dumps(p).encode(), seed, n, fc.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                        rt.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                        rps.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), mr)
+            done += n
+            n *= 2
+        kind = "reference"
+        what = "the reference's QuasyStationaryReleaseSite loop (oracle/_ref), trace rows recorded as its solver does"
+    else:
+        from oracle import qs_oracle
+        cfg = qs_oracle.parse(p, td)
+        g = np.asarray(s6, np.uint32)
+        done, t0 = 0, time.time()
+        while time.time() - t0 < budget_s:
+            g = qs_oracle.run(cfg, added, g, done % len(coords), max_events=4096)[4]
+            done += 1
+        kind = "port"
+        what = "the CPU restatement of the reference's loop"
+    el = time.time() - t0
+    cpu = done / el
+    return {"value": cpu, "unit": "scenarios/s", "cores": 1, "kind": kind, "cpu_model": cpu_model(),
+            "sample": "%d scenarios on one stream, one thread: %s" % (done, what)}
+
+
+def qs_report(n_scen=262144, runs=3, cpu_budget_s=8.0):
+    """Quasi-stationary release sites (Gillespie gating, casim_b200.QuasiStationarySites)
+    on the 20-RyR MWC site of configs.quasi_stationary: scenarios per second on the
+    device (CUDA events around each run, inputs resident), against the reference's own
+    QuasyStationaryReleaseSite loop (oracle/_ref, one thread, as one ParallelSolver
+    thread runs it) or, where that was not built, the CPU restatement, on a bounded
+    sample of scenarios."""
+    import tempfile
+    import casim_b200 as cb
+    from casim_b200 import configs
+    params, coords = configs.quasi_stationary(20, seed=1)
+    td = tempfile.mkdtemp()
+    np.savetxt(os.path.join(td, "coords.txt"), coords, fmt="%.17g")
+    q = cb.QuasiStationarySites(params, n_scen, base_dir=td, max_events=512)
+    first = (np.arange(n_scen) % q.n_ch).astype(np.int32)
+    for _ in range(2):
+        q.run(first)
+    ms = []
+    for _ in range(runs):
+        q.run(first)
+        ms.append(q.last_run_ms())
+    events = sum(q.event_count(s) for s in range(0, n_scen, 64)) * 64
+    per, cls = q.analysis(nadir=3)
+    added = q.increments()
+    q.close()
+    dev = n_scen / (np.median(ms) * 1e-3)
+    out = {"workload": "%d scenarios of a 20-RyR TwoStateMWC site, 50 ms limit, 1 mM Mg, ATP + calmodulin, "
+                       "first RyR s %% 20" % n_scen,
+           "scenarios_per_s": dev, "events_per_s": events / (np.median(ms) * 1e-3), "run_ms": ms,
+           "mean_events_per_scenario": events / n_scen, "classes": {"quarks": int(cls[0]), "blips": int(cls[1]),
+                                                                    "sparks": int(cls[2])}}
+    out["cpu_baseline"] = qs_cpu_baseline(params, coords, added, cpu_budget_s)
+    out["device_vs_one_cpu_thread"] = dev / out["cpu_baseline"]["value"]
+    return out
+
+
 def params_dt_ms(params):
     return float(params["dt, ns"]) * 1e-6
 
@@ -513,6 +598,11 @@ def main():
             result["accuracy"] = accuracy_report(args, p, s)
         except Exception as e:  # reported next to the headline, never required
             result["accuracy"] = {"error": str(e)}
+    if rank == 0 and world == 1 and not args.no_qs:
+        try:
+            result["quasi_stationary"] = qs_report()
+        except Exception as e:  # reported next to the headline, never required
+            result["quasi_stationary"] = {"error": str(e)}
     if rank == 0 and world == 1 and not args.no_surrogate:
         try:
             result["surrogate"] = surrogate_report()

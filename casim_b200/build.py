@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcasim_b200.so")
 SOURCES = ["resident_f64_z3.cu", "resident_f32_z3.cu", "resident_f64_z1.cu", "resident_f32_z1.cu", "capi.cu", "plain.cu",
            "resident.cu", "noalloc.cu", "surrogate.cu", "sg_gate.cu", "analysis.cu", "qs.cu", "parse.cpp"]
-HEADERS = ["model.h", "engine.h", "physics.cuh", "mrg32k3a.cuh", "parse.h", "resident_kernel.cuh", "pools.cuh", "mwc.h"]
+HEADERS = ["model.h", "engine.h", "physics.cuh", "mrg32k3a.cuh", "parse.h", "resident_kernel.cuh", "pools.cuh", "mwc.h", "stream_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -305,3 +305,23 @@ def small_mixed(n_sites=6, seed=11, dim=2, cytosol="Pool", side=(12, 24), ryr=(2
         jsr.append([rng.uniform(700.0, 1300.0)])
     nz = [3] * n_sites
     return _clean(p), sites_table(n, m, nz, nr, xs, ys, seeds, jsr_init=jsr, first=first)
+
+
+def quasi_stationary(n_ryr=20, seed=1, max_time=50.0, coordinates="coords.txt"):
+    """A quasi-stationary release site in the reference's ParallelSolver schema
+    ("Calcium Release Site", LinearNaraghiNeher): n_ryr RyRs on the jittered lattice,
+    TwoStateMWC gating at 1 mM Mg, ATP and calmodulin buffering, 4 pA per open RyR.
+    Returns (params, coords [n_ryr, 2] in nm); write coords to `coordinates`, relative
+    to the base directory given to QuasiStationarySites."""
+    xs, ys = lattice(n_ryr, 150.0, 150.0, np.random.default_rng(seed))
+    params = {"Calcium Release Site": {
+        "Type": "QuasyStationary", "Name": "LinearNaraghiNeher", "Max Time": float(max_time),
+        "Parameters": {
+            "Channels": {"RyR": {"Coordinates": coordinates, "Model": "TwoStateMWC", "Current": 4.0,
+                                 "Parameters": {"fCa": 0.00583687, "KCa": 4.1834575, "fMg": 3.2517014, "KMg": 92.2954937,
+                                                "KO0": 10800, "KMgI": 546.4, "kclose": 0.59}}},
+            "Dyadic Cleft": {"Ions": {"Calcium": {"Concentration": 0.1, "D": 2.2e-6}, "Magnesium": {"Concentration": 1000.0}},
+                             "Buffers": {"ATP": {"kon": 0.225, "koff": 45.0, "D": 1.408e-6, "Total Concentration": 2000.0},
+                                         "Calmodulin": {"kon": 0.1, "koff": 0.038, "D": 2.42e-7, "Total Concentration": 24.0}}},
+            "Open Concentration": 100.0}}}
+    return params, np.c_[xs, ys]

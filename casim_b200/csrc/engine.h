@@ -51,6 +51,11 @@ struct cb_dev {
     int* rs_counter = nullptr;
     unsigned long long* rs_pow2 = nullptr;
     struct cb_rs_plan* rs_plan = nullptr;  // host-side launch plan (resident.cu)
+    // plain path, specialised stencils: (site, first column) of every cleft block;
+    // st_nz = the cleft layers every site shares (0: mixed), -1 before the first step
+    int2* st_tiles = nullptr;
+    int st_ntiles = 0;
+    int st_nz = -1;
 };
 
 // plain path (plain.cu)

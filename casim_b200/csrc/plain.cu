@@ -12,13 +12,16 @@
 // This is the straightforward GPU formulation of the reference step and the
 // denominator of the resident path's speed-up; it handles any site size.
 #include <algorithm>
+#include <climits>
 #include <cstring>
+#include <vector>
 
 #include "engine.h"
 #include "mrg32k3a.cuh"
 #include "mwc.h"
 #include "physics.cuh"
 #include "pools.cuh"
+#include "stream_kernels.cuh"
 
 namespace {
 
@@ -421,17 +424,96 @@ cudaError_t launch_update(cb_dev& d, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// The specialised stencils (stream_kernels.cuh) serve 1-2 ions with up to 4 pairs
+// and a cleft of one layer (2D) or three (3D) at every site; the first step lists
+// the cleft blocks (site, first column). Returns the tile count, 0 if not covered.
+int stream_tiles(cb_dev& d) {
+    if (d.st_nz >= 0) return d.st_nz > 0 ? d.st_ntiles : 0;
+    d.st_nz = 0;
+    const int np = d.m.n_pairs, ncp = d.m.c_n_pairs;
+    if (d.m.n_ions < 1 || d.m.n_ions > 2 || np > 4 || ncp > 4) return 0;
+    std::vector<cb_site> hs(d.S);
+    if (cudaMemcpy(hs.data(), d.sites, sizeof(cb_site) * d.S, cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+    const int nz = d.m.dim == 2 ? 1 : 3;
+    std::vector<int2> tiles;
+    for (int s = 0; s < d.S; ++s) {
+        if (hs[s].nz != nz) return 0;
+        const int cols = hs[s].nx * hs[s].ny;
+        for (int c = 0; c < cols; c += stream::RD_THREADS) tiles.push_back(make_int2(s, c));
+    }
+    if (tiles.empty() || tiles.size() > (size_t)INT32_MAX) return 0;
+    if (cudaMalloc(&d.st_tiles, sizeof(int2) * tiles.size()) != cudaSuccess) return 0;
+    if (cudaMemcpy(d.st_tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d.st_tiles);
+        d.st_tiles = nullptr;
+        return 0;
+    }
+    d.st_ntiles = (int)tiles.size();
+    d.st_nz = nz;
+    return d.st_ntiles;
+}
+
+template <typename R, int NI, int NP>
+void launch_rd_s(cb_dev& d, cudaStream_t st) {
+    const R* in = (const R*)d.fields[d.cur];
+    R* out = (R*)d.fields[1 - d.cur];
+    if (d.st_nz == 1)
+        stream::k_rd_s<R, NI, NP, 1><<<d.st_ntiles, stream::RD_THREADS, 0, st>>>(d.m, d.sites, d.st_tiles, in, out, (const R*)d.curgrid);
+    else
+        stream::k_rd_s<R, NI, NP, 3><<<d.st_ntiles, stream::RD_THREADS, 0, st>>>(d.m, d.sites, d.st_tiles, in, out, (const R*)d.curgrid);
+}
+
+template <typename R, int NI>
+void launch_rd_np(cb_dev& d, cudaStream_t st) {
+    switch (d.m.n_pairs) {
+    case 0: launch_rd_s<R, NI, 0>(d, st); break;
+    case 1: launch_rd_s<R, NI, 1>(d, st); break;
+    case 2: launch_rd_s<R, NI, 2>(d, st); break;
+    case 3: launch_rd_s<R, NI, 3>(d, st); break;
+    default: launch_rd_s<R, NI, 4>(d, st); break;
+    }
+}
+
+template <typename R, int NI, int NCP>
+void launch_cyto_s(cb_dev& d, cudaStream_t st) {
+    const int bps = (d.m.mc * d.m.mc + stream::CY_THREADS - 1) / stream::CY_THREADS;
+    stream::k_cyto_s<R, NI, NCP><<<bps * d.S, stream::CY_THREADS, 0, st>>>(d.m, d.nc, bps, (const R*)d.cyto[d.ccur],
+                                                                           (R*)d.cyto[1 - d.ccur], d.cin);
+}
+
+template <typename R, int NI>
+void launch_cyto_np(cb_dev& d, cudaStream_t st) {
+    switch (d.m.c_n_pairs) {
+    case 0: launch_cyto_s<R, NI, 0>(d, st); break;
+    case 1: launch_cyto_s<R, NI, 1>(d, st); break;
+    case 2: launch_cyto_s<R, NI, 2>(d, st); break;
+    case 3: launch_cyto_s<R, NI, 3>(d, st); break;
+    default: launch_cyto_s<R, NI, 4>(d, st); break;
+    }
+}
+
 template <typename R>
 cudaError_t launch_step(cb_dev& d, cudaStream_t st) {
     k_pre<<<(d.S + 127) / 128, 128, 0, st>>>(d.m, d.S, d.NS, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0],
                                                d.spx[1], d.spc[1], d.ch_micro, d.mwc);
+    const bool fast = stream_tiles(d) > 0;
     if (d.m.cyto_type == CB_CYTO_RD3D) {
-        dim3 g((d.nc + 255) / 256, d.S);
-        k_cyto<R><<<g, 256, 0, st>>>(d.m, d.nc, (const R*)d.cyto[d.ccur], (R*)d.cyto[1 - d.ccur], d.cin);
+        if (fast) {
+            if (d.m.n_ions == 1) launch_cyto_np<R, 1>(d, st);
+            else launch_cyto_np<R, 2>(d, st);
+        } else {
+            dim3 g((d.nc + 255) / 256, d.S);
+            k_cyto<R><<<g, 256, 0, st>>>(d.m, d.nc, (const R*)d.cyto[d.ccur], (R*)d.cyto[1 - d.ccur], d.cin);
+        }
         d.ccur ^= 1;
     }
-    dim3 g((d.max_nodes + 255) / 256, d.S);
-    k_rd<R><<<g, 256, 0, st>>>(d.m, d.sites, (const R*)d.fields[d.cur], (R*)d.fields[1 - d.cur], (const R*)d.curgrid);
+    if (fast) {
+        if (d.m.n_ions == 1) launch_rd_np<R, 1>(d, st);
+        else launch_rd_np<R, 2>(d, st);
+    } else {
+        dim3 g((d.max_nodes + 255) / 256, d.S);
+        k_rd<R><<<g, 256, 0, st>>>(d.m, d.sites, (const R*)d.fields[d.cur], (R*)d.fields[1 - d.cur], (const R*)d.curgrid);
+    }
     d.cur ^= 1;
     return launch_update<R>(d, st);
 }

@@ -194,18 +194,6 @@ def run_example(name, example, steps, n_fields_every=None):
     print("wrote", name, "transitions over", steps, [int(out["s%d" % k].sum()) for k in range(len(steps))])
 
 
-QS_PARAMS = {"Calcium Release Site": {
-    "Type": "QuasyStationary", "Name": "LinearNaraghiNeher", "Max Time": 50.0,
-    "Parameters": {
-        "Channels": {"RyR": {"Coordinates": "coords.txt", "Model": "TwoStateMWC", "Current": 4.0,
-                             "Parameters": {"fCa": 0.00583687, "KCa": 4.1834575, "fMg": 3.2517014, "KMg": 92.2954937,
-                                            "KO0": 10800, "KMgI": 546.4, "kclose": 0.59}}},
-        "Dyadic Cleft": {"Ions": {"Calcium": {"Concentration": 0.1, "D": 2.2e-6}, "Magnesium": {"Concentration": 1000.0}},
-                         "Buffers": {"ATP": {"kon": 0.225, "koff": 45.0, "D": 1.408e-6, "Total Concentration": 2000.0},
-                                     "Calmodulin": {"kon": 0.1, "koff": 0.038, "D": 2.42e-7, "Total Concentration": 24.0}}},
-        "Open Concentration": 100.0}}}
-
-
 def qs_fixture(name, n_scen=40):
     """The reference's own quasi-stationary Gillespie loop (CaSim/QuasyStationaryReleaseSite.cpp)
     over n_scen scenarios on one stream (a one-thread ParallelSolver), with the increments
@@ -213,11 +201,10 @@ def qs_fixture(name, n_scen=40):
     constructor (oracle/ref_qs.cpp): the channel-state rows of every scenario."""
     from casim_b200 import configs
     from oracle import qs_oracle
-    xs, ys = configs.lattice(20, 150.0, 150.0, np.random.default_rng(1))
-    coords = np.c_[xs, ys]
+    qs_params, coords = configs.quasi_stationary(20, seed=1)
     with tempfile.TemporaryDirectory() as td:
         np.savetxt(os.path.join(td, "coords.txt"), coords, fmt="%.17g")
-        p = json.loads(json.dumps(QS_PARAMS))
+        p = json.loads(json.dumps(qs_params))
         p["Calcium Release Site"]["Parameters"]["Channels"]["RyR"]["Coordinates"] = os.path.join(td, "coords.txt")
         added = np.ascontiguousarray(qs_oracle.naraghi_neher(qs_oracle.parse(p)))
         L = ref.lib()
@@ -237,7 +224,7 @@ def qs_fixture(name, n_scen=40):
                           rt.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                           rps.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), mr)
         assert 0 < tot <= mr
-    out = {"params": np.frombuffer(json.dumps(QS_PARAMS).encode(), dtype=np.uint8), "coords": coords,
+    out = {"params": np.frombuffer(json.dumps(qs_params).encode(), dtype=np.uint8), "coords": coords,
            "increments": added, "first": first, "rows_per_scenario": rps, "row_t": rt[:tot],
            "row_states": rs[:tot * len(coords)].reshape(tot, len(coords)).astype(np.int8)}
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
