@@ -96,6 +96,30 @@ __device__ __forceinline__ double u01d_fold(State& g) {
     u = __dadd_rn(u, __dmul_rn(v, 5.9604644775390625e-8));
     return (u < 1.0) ? u : (u - 1.0);
 }
+
+// v = A v (mod M) for a 3x3 jump matrix A (row-major, entries < M) of one component
+template <uint64_t M>
+__device__ __forceinline__ void mat_apply(const unsigned long long* A, unsigned int* v) {
+    unsigned long long r[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        unsigned long long acc = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            acc += fold_mod<M>(A[3 * i + k] * (unsigned long long)v[k]);
+            if (acc >= M) acc -= M;
+        }
+        r[i] = acc;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = (unsigned int)r[i];
+}
+
+// advance both components by the jump stored at J (18 entries: A1 then A2)
+__device__ __forceinline__ void jump_by(const unsigned long long* J, State& g) {
+    mat_apply<M1>(J, g.s);
+    mat_apply<M2>(J + 9, g.s + 3);
+}
 #endif
 
 // ---- host-side jump-ahead (3x3 matrix powers of the two recurrences) ----

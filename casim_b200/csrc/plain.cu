@@ -409,21 +409,6 @@ __global__ void __launch_bounds__(256) k_update(cb_model m, int NS, const cb_sit
         }
 }
 
-template <typename R>
-cudaError_t launch_update(cb_dev& d, cudaStream_t st) {
-    size_t smem = 256 * sizeof(double);
-    if (d.m.cyto_type == CB_CYTO_RD3D) smem += (size_t)d.max_terms * d.m.F * sizeof(double);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    // the rim reads the cytosol as it was before its latest step (RD3D coupling)
-    k_update<R><<<d.S, 256, smem, st>>>(d.m, d.NS, d.sites, (R*)d.fields[d.cur], (R*)d.curgrid, d.ch_node, d.ch_owner,
-                                        d.ch_state, d.mouth, d.sc, d.nc, (const R*)d.cyto[1 - d.ccur], d.cin, d.rim_cnode,
-                                        d.dep_ptr, d.dep_term);
-    return cudaGetLastError();
-}
-
 // The specialised stencils (stream_kernels.cuh) serve 1-2 ions with up to 4 pairs
 // and a cleft of one layer (2D) or three (3D) at every site; the first step lists
 // the cleft blocks (site, first column). Returns the tile count, 0 if not covered.
@@ -451,6 +436,81 @@ int stream_tiles(cb_dev& d) {
     d.st_ntiles = (int)tiles.size();
     d.st_nz = nz;
     return d.st_ntiles;
+}
+
+// jump table of k_pre_r: row l < 32 holds A^(2l), both components (row 31, A^62, also
+// takes a lane from one chunk of 32 draws to the next)
+bool pre_jump(cb_dev& d) {
+    if (d.pre_jump) return true;
+    std::vector<unsigned long long> t(32 * 18);
+    const cbrng::Mat3 a1 = cbrng::step_matrix1(), a2 = cbrng::step_matrix2();
+    cbrng::Mat3 p1{{{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}}, p2 = p1;  // A^(2l)
+    for (int l = 0; l < 32; ++l) {
+        for (int i = 0; i < 9; ++i) {
+            t[18 * l + i] = p1.a[i / 3][i % 3];
+            t[18 * l + 9 + i] = p2.a[i / 3][i % 3];
+        }
+        for (int k = 0; k < 2; ++k) {
+            p1 = cbrng::matmul(a1, p1, cbrng::M1);
+            p2 = cbrng::matmul(a2, p2, cbrng::M2);
+        }
+    }
+    if (cudaMalloc(&d.pre_jump, sizeof(unsigned long long) * t.size()) != cudaSuccess) {
+        d.pre_jump = nullptr;
+        return false;
+    }
+    if (cudaMemcpy(d.pre_jump, t.data(), sizeof(unsigned long long) * t.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d.pre_jump);
+        d.pre_jump = nullptr;
+        return false;
+    }
+    return true;
+}
+
+template <typename R, int NI, int NP, bool RD3D>
+cudaError_t launch_update_s(cb_dev& d, cudaStream_t st) {
+    size_t smem = 8 * (NI + NP + NI) * sizeof(double);
+    if (RD3D) smem += (size_t)d.max_terms * (NI + NP) * sizeof(double);
+    auto kern = stream::k_update_s<R, NI, NP, RD3D>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<d.S, stream::UP_THREADS, smem, st>>>(d.m, d.NS, d.sites, (R*)d.fields[d.cur], (R*)d.curgrid, d.ch_node, d.ch_owner, d.ch_state,
+                                                d.mouth, d.sc, d.nc, (const R*)d.cyto[1 - d.ccur], d.cin, d.rim_cnode, d.dep_ptr,
+                                                d.dep_term);
+    return cudaGetLastError();
+}
+
+template <typename R, int NI, bool RD3D>
+cudaError_t launch_update_np(cb_dev& d, cudaStream_t st) {
+    switch (d.m.n_pairs) {
+    case 0: return launch_update_s<R, NI, 0, RD3D>(d, st);
+    case 1: return launch_update_s<R, NI, 1, RD3D>(d, st);
+    case 2: return launch_update_s<R, NI, 2, RD3D>(d, st);
+    case 3: return launch_update_s<R, NI, 3, RD3D>(d, st);
+    default: return launch_update_s<R, NI, 4, RD3D>(d, st);
+    }
+}
+
+template <typename R>
+cudaError_t launch_update(cb_dev& d, cudaStream_t st) {
+    if (stream_tiles(d) > 0) {
+        const bool rd3d = d.m.cyto_type == CB_CYTO_RD3D;
+        if (d.m.n_ions == 1) return rd3d ? launch_update_np<R, 1, true>(d, st) : launch_update_np<R, 1, false>(d, st);
+        return rd3d ? launch_update_np<R, 2, true>(d, st) : launch_update_np<R, 2, false>(d, st);
+    }
+    size_t smem = 256 * sizeof(double);
+    if (d.m.cyto_type == CB_CYTO_RD3D) smem += (size_t)d.max_terms * d.m.F * sizeof(double);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    // the rim reads the cytosol as it was before its latest step (RD3D coupling)
+    k_update<R><<<d.S, 256, smem, st>>>(d.m, d.NS, d.sites, (R*)d.fields[d.cur], (R*)d.curgrid, d.ch_node, d.ch_owner,
+                                        d.ch_state, d.mouth, d.sc, d.nc, (const R*)d.cyto[1 - d.ccur], d.cin, d.rim_cnode,
+                                        d.dep_ptr, d.dep_term);
+    return cudaGetLastError();
 }
 
 template <typename R, int NI, int NP>
@@ -494,9 +554,13 @@ void launch_cyto_np(cb_dev& d, cudaStream_t st) {
 
 template <typename R>
 cudaError_t launch_step(cb_dev& d, cudaStream_t st) {
-    k_pre<<<(d.S + 127) / 128, 128, 0, st>>>(d.m, d.S, d.NS, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0],
-                                               d.spx[1], d.spc[1], d.ch_micro, d.mwc);
     const bool fast = stream_tiles(d) > 0;
+    if (fast && !d.mwc && pre_jump(d))
+        stream::k_pre_r<<<(d.S + stream::PRE_WARPS - 1) / stream::PRE_WARPS, 32 * stream::PRE_WARPS, 0, st>>>(
+            d.m, d.S, d.NS, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0], d.spx[1], d.spc[1], d.pre_jump);
+    else
+        k_pre<<<(d.S + 127) / 128, 128, 0, st>>>(d.m, d.S, d.NS, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0],
+                                                   d.spx[1], d.spc[1], d.ch_micro, d.mwc);
     if (d.m.cyto_type == CB_CYTO_RD3D) {
         if (fast) {
             if (d.m.n_ions == 1) launch_cyto_np<R, 1>(d, st);

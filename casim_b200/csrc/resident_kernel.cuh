@@ -145,22 +145,7 @@ struct rs_args {
 using cbrng::fold_mod;
 __device__ __forceinline__ double u01d_fast(cbrng::State& g) { return cbrng::u01d_fold(g); }
 
-template <unsigned long long M>
-__device__ __forceinline__ void mat_apply(const unsigned long long* A, unsigned int* v) {
-    unsigned long long r[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        unsigned long long acc = 0;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            acc += fold_mod<M>(A[3 * i + k] * (unsigned long long)v[k]);
-            if (acc >= M) acc -= M;
-        }
-        r[i] = acc;
-    }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) v[i] = (unsigned int)r[i];
-}
+using cbrng::mat_apply;
 
 __device__ __forceinline__ void jump_row(const unsigned long long* pow2, cbrng::State& g, int k) {
     mat_apply<cbrng::M1>(pow2 + 18 * k, g.s);

@@ -193,3 +193,275 @@ __global__ void __launch_bounds__(CY_THREADS) k_cyto_s(const __grid_constant__ c
 }
 
 }  // namespace stream
+
+namespace stream {
+
+constexpr int UP_THREADS = 256;
+
+// Sum of each of the K per-thread values over the block (UP_THREADS threads) in a fixed
+// order: warp butterflies, then the warp partials in warp order; every thread gets the
+// sums. red holds (UP_THREADS / 32) * K doubles.
+template <int K>
+__device__ __forceinline__ void block_sums(double (&v)[K], double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();  // red may still be read from its previous use
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) red[warp * K + k] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = red[k];
+#pragma unroll
+        for (int w = 1; w < UP_THREADS / 32; ++w) s += red[w * K + k];
+        v[k] = s;
+    }
+}
+
+// The Update of one site per block (CaSim/ParallelHybridSolver.cpp:159-175): mouth
+// values, Dirichlet rim from the cytosol, efflux through the rim, the RD3D deposits
+// into cytosol layer 0, RyR currents and the jSR coupling; the steps, their order and
+// the values they read are those of the generic k_update, the per-node quantities in
+// registers and the block sums by warp shuffles.
+template <typename R, int NI, int NP, bool RD3D>
+__global__ void __launch_bounds__(UP_THREADS) k_update_s(const __grid_constant__ cb_model m, int NS, const cb_site* __restrict__ sites,
+                                                         R* __restrict__ fld, R* __restrict__ curg, const int* __restrict__ ch_node,
+                                                         const int* __restrict__ ch_owner, const int* __restrict__ ch_state,
+                                                         double* __restrict__ mouth, cb_site_scalars* __restrict__ sc, int nc,
+                                                         const R* __restrict__ cyto, double* __restrict__ cin,
+                                                         const int* __restrict__ rim_cnode, const int* __restrict__ dep_ptr,
+                                                         const int* __restrict__ dep_term) {
+    constexpr int F = NI + NP;
+    constexpr int CSM = NI + 4;  // cytosol species slots (ions + at most 4 pairs)
+    const int CS = m.n_ions + m.c_n_pairs;
+    extern __shared__ double smem[];
+    double* red = smem;                   // (UP_THREADS / 32) * (F + NI)
+    double* terms = smem + 8 * (F + NI);  // RD3D: [term][F] efflux values
+    const int s = blockIdx.x;
+    const cb_site st = sites[s];
+    cb_site_scalars& q = sc[s];
+    R* u = fld + st.node_base * F;
+    const int nx = st.nx, ny = st.ny, nz = st.nz, nxy = nx * ny;
+    const long long np = st.npad;
+    // 1. mouth values: ions, pairs, free buffers (CaSim/DyadRD2DCPU.cpp:361-380)
+    for (int c = threadIdx.x; c < st.n_ch; c += UP_THREADS) {
+        const int node = ch_node[st.ch_off + c];
+        double* mo = mouth + (long long)(st.ch_off + c) * NS;
+        double v[F];
+#pragma unroll
+        for (int f = 0; f < F; ++f) v[f] = (double)u[f * np + node];
+#pragma unroll
+        for (int f = 0; f < F; ++f) mo[f] = v[f];
+        for (int b = 0; b < m.n_buf; ++b) {
+            double fr = m.Ctot[b];
+#pragma unroll
+            for (int p = 0; p < NP; ++p)
+                if (m.pair_buf[p] == b) fr -= v[NI + p];
+            mo[F + b] = fr;
+        }
+    }
+    __syncthreads();
+    // 2. Dirichlet edges from the cytosol (CaSim/DyadRD2DCPU.cpp:274-303)
+    const int nrim = cb_rim_count(nx, ny);
+    const R* cy = RD3D ? cyto + (long long)s * CS * nc : nullptr;
+    for (int t = threadIdx.x; t < nrim * nz; t += UP_THREADS) {
+        const int z = t / nrim, r = t - z * nrim;
+        int x, y;
+        cb_rim_xy(r, nx, ny, x, y);
+        const int node = x + nx * y + nxy * z;
+        if (!RD3D) {
+#pragma unroll
+            for (int j = 0; j < NI; ++j) u[j * np + node] = (R)q.c_ions[j];
+#pragma unroll
+            for (int p = 0; p < NP; ++p) u[(NI + p) * np + node] = (R)q.c_bnd[p];
+        } else {
+            const int cn = rim_cnode[st.rim_off + r];
+#pragma unroll
+            for (int j = 0; j < NI; ++j) u[j * np + node] = cy[(long long)j * nc + cn];
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const int cq = m.dyad_c_pair[p];
+                u[(NI + p) * np + node] = cq >= 0 ? cy[(long long)(NI + cq) * nc + cn] : (R)m.pair_init[p];
+            }
+        }
+    }
+    __syncthreads();
+    // 3. efflux (CaSim/DyadRD2DCPU.cpp:305-350): per-term values, block sums
+    const int zmax = nz == 1 ? 1 : nz - 1;
+    const int T = cb_efflux_terms(nx, ny, zmax);
+    double part[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) part[f] = 0;
+    for (int t = threadIdx.x; t < T; t += UP_THREADS) {
+        int x0, y0, x1, y1, x2, y2, z;
+        const int sel = cb_efflux_term(t, nx, ny, zmax, x0, y0, x1, y1, x2, y2, z);
+        const double sf = sel == 0 ? m.sx : m.sy;
+        const int n0 = x0 + nx * y0 + nxy * z, n1 = x1 + nx * y1 + nxy * z, n2 = x2 + nx * y2 + nxy * z;
+        double a0[F], a1[F], a2[F];
+#pragma unroll
+        for (int f = 0; f < F; ++f) {
+            a0[f] = (double)u[f * np + n0];
+            a1[f] = (double)u[f * np + n1];
+            a2[f] = (double)u[f * np + n2];
+        }
+#pragma unroll
+        for (int f = 0; f < F; ++f) {
+            const double D = f < NI ? m.D_ion[f] : m.D_pair[f - NI];
+            const double g = 2 * a1[f] - 1.5 * a0[f] - 0.5 * a2[f];
+            if (!RD3D) {
+                part[f] += D * m.grad_mult * sf * g;
+            } else {
+                const double v = D * sf * g * m.inv_hc3;
+                part[f] += v;
+                terms[(long long)t * F + f] = v;
+            }
+        }
+    }
+    block_sums<F>(part, red);  // its barriers also publish the terms
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int f = 0; f < F; ++f) q.efflux[f] = part[f];
+    // 4. RD3D: deposit into the cytosol layer z = 0 in term order
+    if (RD3D) {
+        const int mc2 = m.mc * m.mc;
+        const int* ptr = dep_ptr + (long long)s * (mc2 + 1);
+        const int* dtm = dep_term + st.term_off;
+        for (int cn = threadIdx.x; cn < mc2; cn += UP_THREADS) {
+            const int lo = ptr[cn], hi = ptr[cn + 1];
+            double acc[CSM];
+#pragma unroll
+            for (int c = 0; c < CSM; ++c) acc[c] = 0;
+            for (int k = lo; k < hi; ++k) {
+                const int t = dtm[k];
+#pragma unroll
+                for (int c = 0; c < CSM; ++c) {
+                    if (c >= CS) break;
+                    int f = c < NI ? c : m.c_dyad_pair[c - NI];
+                    if (f >= 0 && c >= NI) f += NI;
+                    if (f >= 0) acc[c] += terms[(long long)t * F + f];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CSM; ++c)
+                if (c < CS) cin[((long long)s * CS + c) * mc2 + cn] = acc[c];
+        }
+    }
+    // 5. RyR currents (CaSim/DyadRD2DCPU.cpp:243-264, CaSim/PassiveIonChannel.cpp:28-34)
+    R* cg = curg + st.node_base * NI;
+    double tot[NI];
+#pragma unroll
+    for (int j = 0; j < NI; ++j) tot[j] = 0;
+    for (int c = threadIdx.x; c < st.n_ch; c += UP_THREADS) {
+        const int node = ch_node[st.ch_off + c];
+        const int state = ch_state[st.ch_off + c];
+        const int own = ch_owner[st.ch_off + c];
+#pragma unroll
+        for (int j = 0; j < NI; ++j) {
+            const double flux = state * (m.g[j] * (q.jsr_new[j] - (double)u[j * np + node]));
+            if (own) cg[j * np + node] = (R)flux;
+            tot[j] += flux;
+        }
+    }
+    block_sums<NI>(tot, red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NI; ++j) q.total[j] = tot[j];
+        // 6. jSR coupling (CaSim/SRPool.cpp:55-68)
+        if (!m.jsr_const)
+#pragma unroll
+            for (int i = 0; i < NI; ++i) {
+                q.IjSR[i] = q.total[i] * m.V_elem;
+                q.nsr[i] = m.nsr[i];
+                q.jsr[i] = q.jsr_new[i];
+            }
+    }
+}
+
+// Pools and two-state gating of one site per warp (CaSim/CytosolPool.cpp:217-268,
+// CaSim/SRPool.cpp:70-89, CaSim/DyadChannels.cpp:97-130). The site's MRG32k3a stream is
+// consumed in the reference's order (one draw per RyR test in RyR order, one more per
+// transition) without a serial loop: lane l jumps to draw l of the stream (jump table J,
+// row l: A^(2l)), the lanes draw 32 consecutive values at a time (then jump by A^62,
+// row 31, to their draw of the next 32), and 32 RyRs are resolved per ballot, one more
+// ballot after each transition. The stream state left behind is that at the first
+// unused draw, as after the serial loop.
+constexpr int PRE_WARPS = 4;
+__global__ void __launch_bounds__(32 * PRE_WARPS) k_pre_r(const __grid_constant__ cb_model m, int S, int NS,
+                                                          const cb_site* __restrict__ sites, cb_site_scalars* __restrict__ sc,
+                                                          int* __restrict__ ch_state, const double* __restrict__ mouth,
+                                                          const double* __restrict__ spx0, const double* __restrict__ spc0,
+                                                          const double* __restrict__ spx1, const double* __restrict__ spc1,
+                                                          const unsigned long long* __restrict__ J) {
+    __shared__ double s_u[PRE_WARPS][64];  // draws [we - 64, we), slot = draw & 63
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int s = blockIdx.x * PRE_WARPS + w;
+    if (s >= S) return;  // whole warp
+    const cb_site st = sites[s];
+    cb_site_scalars& q = sc[s];
+    const double dt = m.dt;
+    if (lane == 0) {
+        if (m.cyto_type == CB_CYTO_POOL) cb_pool_step(m, q, dt);
+        cb_jsr_step(m, q, dt);
+    }
+    cbrng::State gl;  // this lane's draw we + lane
+#pragma unroll
+    for (int i = 0; i < 6; ++i) gl.s[i] = q.rng[i];
+    cbrng::jump_by(J + 18 * lane, gl);
+    cbrng::State gs = gl;  // state at this lane's draw of the latest chunk
+    long long D = 0, we = 0;
+    const int nch = st.n_ch;
+    for (int c0 = 0; c0 < nch; c0 += 32) {
+        const int cnt = min(32, nch - c0);
+        const int c = c0 + lane;
+        const bool act = lane < cnt;
+        double p = 0;
+        int stt = 0;
+        if (act) {
+            const double* mo = mouth + (long long)(st.ch_off + c) * NS;
+            const double mg = m.mg_idx >= 0 ? mo[m.mg_idx] : 0.0;
+            stt = ch_state[st.ch_off + c];
+            p = cb_rate(m, spx0, spc0, spx1, spc1, stt, mo[m.ca_idx], mg) * dt;
+        }
+        int start = 0;
+        while (start < cnt) {
+            // draws D .. D + (cnt - start) - 1 must be in the ring
+            while (we < D + (cnt - start)) {
+                gs = gl;
+                s_u[w][(we + lane) & 63] = cbrng::u01d_fold(gl);
+                cbrng::jump_by(J + 18 * 31, gl);
+                we += 32;
+                __syncwarp();
+            }
+            const bool rem = act && lane >= start;
+            const double u = rem ? s_u[w][(D + (lane - start)) & 63] : 2.0;
+            const unsigned int t = __ballot_sync(0xffffffffu, rem && (u < p));
+            if (t == 0u) {
+                D += cnt - start;
+                break;
+            }
+            const int f = __ffs(t) - 1;
+            if (lane == f) ch_state[st.ch_off + c] = 1 - stt;
+            D += (f - start) + 2;
+            start = f + 1;
+        }
+        __syncwarp();
+    }
+    // the state at draw D: lane D - (we - 32) of the latest chunk before its draw, or, past
+    // the chunk, lane D - we at its next chunk's draw (D - we is 0 or 1)
+    const bool in_chunk = D < we;
+    const int k = in_chunk ? (int)(D - (we - 32)) : (int)(D - we);
+    unsigned int out[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) out[i] = __shfl_sync(0xffffffffu, in_chunk ? gs.s[i] : gl.s[i], k);
+    if (lane == 0) {
+        q.draws += (unsigned long long)D;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) q.rng[i] = out[i];
+    }
+}
+
+}  // namespace stream
