@@ -536,6 +536,10 @@ void launch_rd_np(cb_dev& d, cudaStream_t st) {
 
 template <typename R, int NI, int NCP>
 void launch_cyto_s(cb_dev& d, cudaStream_t st) {
+    if (d.m.mc == 25) {
+        stream::k_cyto_m<R, NI, NCP, 25><<<d.S, 640, 0, st>>>(d.m, (const R*)d.cyto[d.ccur], (R*)d.cyto[1 - d.ccur], d.cin);
+        return;
+    }
     const int bps = (d.m.mc * d.m.mc + stream::CY_THREADS - 1) / stream::CY_THREADS;
     stream::k_cyto_s<R, NI, NCP><<<bps * d.S, stream::CY_THREADS, 0, st>>>(d.m, d.nc, bps, (const R*)d.cyto[d.ccur],
                                                                            (R*)d.cyto[1 - d.ccur], d.cin);

@@ -192,6 +192,116 @@ __global__ void __launch_bounds__(CY_THREADS) k_cyto_s(const __grid_constant__ c
     }
 }
 
+// The cytosol step above for a grid of MC^3 nodes fixed at compile time (MC = 25, the
+// grid of the shipped configs), one block per site so that every x and y neighbour a
+// column reads belongs to the block: the column's MC - 1 planes unrolled, every
+// neighbour at a constant offset from the column's base, and the loop-invariant parts
+// of the reaction and SERCA terms computed once (by the same expressions).
+template <typename R, int NI, int NCP, int MC>
+__global__ void __launch_bounds__((MC * MC + 31) / 32 * 32) k_cyto_m(const __grid_constant__ cb_model m, const R* __restrict__ in,
+                                                                     R* __restrict__ out, const double* __restrict__ cin) {
+    constexpr int CS = NI + NCP, MC2 = MC * MC, NC = MC2 * MC;
+    const int s = blockIdx.x;
+    const int col = (int)threadIdx.x;
+    if (col >= MC2) return;
+    const int j = col / MC, i = col - j * MC;
+    if (i == 0 || i == MC - 1 || j == 0 || j == MC - 1) return;
+    const R* __restrict__ u = in + (long long)s * CS * NC + col;
+    R* __restrict__ o = out + (long long)s * CS * NC + col;
+    const double* __restrict__ ci = cin + (long long)s * CS * MC2 + col;
+    const R ih2 = (R)m.inv_hc2;
+    const R dt = (R)m.dt;
+    R D[CS];
+#pragma unroll
+    for (int c = 0; c < CS; ++c) D[c] = (R)(c < NI ? m.D_ion[c] : m.c_D_pair[c - NI]);
+    R koff[NCP > 0 ? NCP : 1], kon[NCP > 0 ? NCP : 1], ctot[NCP > 0 ? NCP : 1];
+    unsigned same[NCP > 0 ? NCP : 1];  // bit q: pair q binds pair p's buffer
+    int pion[NCP > 0 ? NCP : 1];
+#pragma unroll
+    for (int p = 0; p < NCP; ++p) {
+        const int b = m.c_pair_buf[p];
+        koff[p] = (R)m.c_koff[p];
+        kon[p] = (R)m.c_kon[p];
+        ctot[p] = (R)m.c_Ctot[b];
+        pion[p] = NI == 1 ? 0 : m.c_pair_ion[p];
+        unsigned bits = 0;
+#pragma unroll
+        for (int q = 0; q < NCP; ++q)
+            if (m.c_pair_buf[q] == b) bits |= 1u << q;
+        same[p] = bits;
+    }
+    bool serca[NI];
+    R jmax[NI], k2[NI], bterm[NI];
+    {
+        int is = 0;
+#pragma unroll
+        for (int j2 = 0; j2 < NI; ++j2) {
+            serca[j2] = m.c_serca[j2] != 0;
+            jmax[j2] = k2[j2] = bterm[j2] = 0;
+            if (serca[j2]) {
+                k2[j2] = (R)(m.c_Kup[is] * m.c_Kup[is]);
+                const R b2 = (R)(m.c_bg[is] * m.c_bg[is]);
+                bterm[j2] = b2 / (b2 + k2[j2]);
+                jmax[j2] = (R)m.c_Jmax[is];
+                ++is;
+            }
+        }
+    }
+    R lo[CS], cu[CS], hi[CS];
+#pragma unroll
+    for (int c = 0; c < CS; ++c) {
+        cu[c] = u[c * NC];
+        hi[c] = u[c * NC + MC2];
+        lo[c] = hi[c];
+    }
+#pragma unroll
+    for (int k = 0; k < MC - 1; ++k) {
+        const int n = k * MC2;
+        R evo[CS];
+#pragma unroll
+        for (int c = 0; c < CS; ++c) {
+            const R* v = u + c * NC + n;
+            const R cc = cu[c];
+            evo[c] = D[c] * ((v[1] - 2 * cc + v[-1]) * ih2 + (v[MC] - 2 * cc + v[-MC]) * ih2 + (hi[c] - 2 * cc + lo[c]) * ih2);
+        }
+#pragma unroll
+        for (int j2 = 0; j2 < NI; ++j2) {
+            const R ion = cu[j2];
+            R react = 0;
+#pragma unroll
+            for (int p = 0; p < NCP; ++p) {
+                if (pion[p] != j2) continue;
+                R fr = ctot[p];
+#pragma unroll
+                for (int q = 0; q < NCP; ++q)
+                    if (same[p] >> q & 1u) fr -= cu[NI + q];
+                const R R1 = koff[p] * cu[NI + p] - kon[p] * ion * fr;
+                evo[NI + p] += -R1;
+                react += R1;
+            }
+            evo[j2] += react;
+            if (serca[j2]) {
+                const R i2 = ion * ion;
+                evo[j2] -= jmax[j2] * (i2 / (i2 + k2[j2]) - bterm[j2]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CS; ++c) {
+            R e = evo[c];
+            if (k == 0) e += (R)ci[c * MC2];
+            o[c * NC + n] = cu[c] + e * dt;
+        }
+        if (k + 2 < MC) {
+#pragma unroll
+            for (int c = 0; c < CS; ++c) {
+                lo[c] = cu[c];
+                cu[c] = hi[c];
+                hi[c] = u[c * NC + n + 2 * MC2];
+            }
+        }
+    }
+}
+
 }  // namespace stream
 
 namespace stream {
