@@ -152,12 +152,7 @@ void build_device(casim_b200_sim* h, int precision) {
             for (int r = 0; r < nrim; ++r) {
                 int x, y;
                 cb_rim_xy(r, st.nx, st.ny, x, y);
-                double px = (x - 0.5 * (st.nx - 1)) * cfg.m.dx, py = (y - 0.5 * (st.ny - 1)) * cfg.m.dy;
-                int ci = (int)std::floor(px / cfg.m.hc + 0.5 * (mc - 1) + 0.5);
-                int cj = (int)std::floor(py / cfg.m.hc + 0.5 * (mc - 1) + 0.5);
-                ci = std::min(std::max(ci, 1), mc - 2);
-                cj = std::min(std::max(cj, 1), mc - 2);
-                rim_cnode.push_back(ci + mc * cj);
+                rim_cnode.push_back(cb_rim_cnode(x, y, st.nx, st.ny, cfg.m.dx, cfg.m.dy, cfg.m.hc, mc));
             }
             rimoff += nrim;
             // deposit lists: efflux terms grouped by receiving cytosol node, term order kept

@@ -108,6 +108,18 @@ __host__ __device__ __forceinline__ void cb_rim_xy(int r, int nx, int ny, int& x
         y = ny - 1;
     }
 }
+// RD3D: the layer-0 cytosol node (i + mc*j) nearest below cleft node (x, y), clamped to
+// the updated range; both grids are centred on each other. Host and device evaluate the
+// same expressions to the same node: each step is one correctly rounded operation (the
+// products by 0.5 of small integers are exact).
+__host__ __device__ __forceinline__ int cb_rim_cnode(int x, int y, int nx, int ny, double dx, double dy, double hc, int mc) {
+    const double px = (x - 0.5 * (nx - 1)) * dx, py = (y - 0.5 * (ny - 1)) * dy;
+    int ci = (int)floor(px / hc + 0.5 * (mc - 1) + 0.5);
+    int cj = (int)floor(py / hc + 0.5 * (mc - 1) + 0.5);
+    ci = ci < 1 ? 1 : (ci > mc - 2 ? mc - 2 : ci);
+    cj = cj < 1 ? 1 : (cj > mc - 2 ? mc - 2 : cj);
+    return ci + mc * cj;
+}
 __host__ __device__ __forceinline__ int cb_rim_index(int x, int y, int nx, int ny) {
     if (x == 0) return y;
     if (x == nx - 1) return ny + y;

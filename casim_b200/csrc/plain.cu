@@ -468,7 +468,7 @@ bool pre_jump(cb_dev& d) {
 }
 
 template <typename R, int NI, int NP, bool RD3D>
-cudaError_t launch_update_s(cb_dev& d, cudaStream_t st) {
+cudaError_t launch_update_s(cb_dev& d, cudaStream_t st, bool after_step) {
     size_t smem = 8 * (NI + NP + NI) * sizeof(double);
     if (RD3D) smem += (size_t)d.max_terms * (NI + NP) * sizeof(double);
     auto kern = stream::k_update_s<R, NI, NP, RD3D>;
@@ -478,27 +478,29 @@ cudaError_t launch_update_s(cb_dev& d, cudaStream_t st) {
     }
     kern<<<d.S, stream::UP_THREADS, smem, st>>>(d.m, d.NS, d.sites, (R*)d.fields[d.cur], (R*)d.curgrid, d.ch_node, d.ch_owner, d.ch_state,
                                                 d.mouth, d.sc, d.nc, (const R*)d.cyto[1 - d.ccur], d.cin, d.rim_cnode, d.dep_ptr,
-                                                d.dep_term);
+                                                d.dep_term, after_step ? (const R*)d.fields[1 - d.cur] : nullptr);
     return cudaGetLastError();
 }
 
 template <typename R, int NI, bool RD3D>
-cudaError_t launch_update_np(cb_dev& d, cudaStream_t st) {
+cudaError_t launch_update_np(cb_dev& d, cudaStream_t st, bool after_step) {
     switch (d.m.n_pairs) {
-    case 0: return launch_update_s<R, NI, 0, RD3D>(d, st);
-    case 1: return launch_update_s<R, NI, 1, RD3D>(d, st);
-    case 2: return launch_update_s<R, NI, 2, RD3D>(d, st);
-    case 3: return launch_update_s<R, NI, 3, RD3D>(d, st);
-    default: return launch_update_s<R, NI, 4, RD3D>(d, st);
+    case 0: return launch_update_s<R, NI, 0, RD3D>(d, st, after_step);
+    case 1: return launch_update_s<R, NI, 1, RD3D>(d, st, after_step);
+    case 2: return launch_update_s<R, NI, 2, RD3D>(d, st, after_step);
+    case 3: return launch_update_s<R, NI, 3, RD3D>(d, st, after_step);
+    default: return launch_update_s<R, NI, 4, RD3D>(d, st, after_step);
     }
 }
 
+// after_step: right after k_rd_s, which set the rim already
 template <typename R>
-cudaError_t launch_update(cb_dev& d, cudaStream_t st) {
+cudaError_t launch_update(cb_dev& d, cudaStream_t st, bool after_step = false) {
     if (stream_tiles(d) > 0) {
         const bool rd3d = d.m.cyto_type == CB_CYTO_RD3D;
-        if (d.m.n_ions == 1) return rd3d ? launch_update_np<R, 1, true>(d, st) : launch_update_np<R, 1, false>(d, st);
-        return rd3d ? launch_update_np<R, 2, true>(d, st) : launch_update_np<R, 2, false>(d, st);
+        if (d.m.n_ions == 1)
+            return rd3d ? launch_update_np<R, 1, true>(d, st, after_step) : launch_update_np<R, 1, false>(d, st, after_step);
+        return rd3d ? launch_update_np<R, 2, true>(d, st, after_step) : launch_update_np<R, 2, false>(d, st, after_step);
     }
     size_t smem = 256 * sizeof(double);
     if (d.m.cyto_type == CB_CYTO_RD3D) smem += (size_t)d.max_terms * d.m.F * sizeof(double);
@@ -517,10 +519,14 @@ template <typename R, int NI, int NP>
 void launch_rd_s(cb_dev& d, cudaStream_t st) {
     const R* in = (const R*)d.fields[d.cur];
     R* out = (R*)d.fields[1 - d.cur];
+    // the cytosol as it was before its latest step (k_cyto flipped ccur already)
+    const R* cy = (const R*)d.cyto[1 - d.ccur];
     if (d.st_nz == 1)
-        stream::k_rd_s<R, NI, NP, 1><<<d.st_ntiles, stream::RD_THREADS, 0, st>>>(d.m, d.sites, d.st_tiles, in, out, (const R*)d.curgrid);
+        stream::k_rd_s<R, NI, NP, 1><<<d.st_ntiles, stream::RD_THREADS, 0, st>>>(d.m, d.sites, d.st_tiles, in, out, (const R*)d.curgrid,
+                                                                                 d.sc, cy);
     else
-        stream::k_rd_s<R, NI, NP, 3><<<d.st_ntiles, stream::RD_THREADS, 0, st>>>(d.m, d.sites, d.st_tiles, in, out, (const R*)d.curgrid);
+        stream::k_rd_s<R, NI, NP, 3><<<d.st_ntiles, stream::RD_THREADS, 0, st>>>(d.m, d.sites, d.st_tiles, in, out, (const R*)d.curgrid,
+                                                                                 d.sc, cy);
 }
 
 template <typename R, int NI>
@@ -583,7 +589,7 @@ cudaError_t launch_step(cb_dev& d, cudaStream_t st) {
         k_rd<R><<<g, 256, 0, st>>>(d.m, d.sites, (const R*)d.fields[d.cur], (R*)d.fields[1 - d.cur], (const R*)d.curgrid);
     }
     d.cur ^= 1;
-    return launch_update<R>(d, st);
+    return launch_update<R>(d, st, fast);
 }
 
 // ---- surrogate-driven gating (no RD): the mouth Ca comes from the surrogate network

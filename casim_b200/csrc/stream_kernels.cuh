@@ -19,11 +19,16 @@ namespace stream {
 constexpr int RD_THREADS = 256;
 constexpr int CY_THREADS = 128;
 
-// Cleft step of the columns [tile.y, tile.y + 256) of site tile.x.
+// Cleft step of the columns [tile.y, tile.y + 256) of site tile.x. The rim columns take
+// the Dirichlet values that the Update would set right after this step
+// (CaSim/DyadRD2DCPU.cpp:274-303), from the same sources: the cytosol as it was before
+// its latest step (cyto, RD3D) or the pool values of this step (sc); the Update then
+// leaves the rim alone (k_update_s with prev set).
 template <typename R, int NI, int NP, int NZ>
 __global__ void __launch_bounds__(RD_THREADS) k_rd_s(const __grid_constant__ cb_model m, const cb_site* __restrict__ sites,
                                                      const int2* __restrict__ tiles, const R* __restrict__ in,
-                                                     R* __restrict__ out, const R* __restrict__ curg) {
+                                                     R* __restrict__ out, const R* __restrict__ curg,
+                                                     const cb_site_scalars* __restrict__ sc, const R* __restrict__ cyto) {
     constexpr int F = NI + NP;
     const int2 tl = tiles[blockIdx.x];
     const cb_site st = sites[tl.x];
@@ -34,19 +39,37 @@ __global__ void __launch_bounds__(RD_THREADS) k_rd_s(const __grid_constant__ cb_
     const R* __restrict__ u = in + st.node_base * F;
     R* __restrict__ o = out + st.node_base * F;
     const int y = col / nx, x = col - y * nx;
+    if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1) {
+        R b[F];
+        if (m.cyto_type == CB_CYTO_RD3D) {
+            const int CS = m.n_ions + m.c_n_pairs, nc = m.mc * m.mc * m.mc;
+            const R* cy = cyto + (long long)tl.x * CS * nc;
+            const int cn = cb_rim_cnode(x, y, nx, ny, m.dx, m.dy, m.hc, m.mc);
+#pragma unroll
+            for (int j = 0; j < NI; ++j) b[j] = cy[(long long)j * nc + cn];
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const int cq = m.dyad_c_pair[p];
+                b[NI + p] = cq >= 0 ? cy[(long long)(NI + cq) * nc + cn] : (R)m.pair_init[p];
+            }
+        } else {
+            const cb_site_scalars& q = sc[tl.x];
+#pragma unroll
+            for (int j = 0; j < NI; ++j) b[j] = (R)q.c_ions[j];
+#pragma unroll
+            for (int p = 0; p < NP; ++p) b[NI + p] = (R)q.c_bnd[p];
+        }
+#pragma unroll
+        for (int f = 0; f < F; ++f)
+#pragma unroll
+            for (int z = 0; z < NZ; ++z) o[f * np + col + z * nxy] = b[f];
+        return;
+    }
     R c[F][NZ];
 #pragma unroll
     for (int f = 0; f < F; ++f)
 #pragma unroll
         for (int z = 0; z < NZ; ++z) c[f][z] = u[f * np + col + z * nxy];
-    if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1) {
-        // rim nodes carry over; the Update sets them from the cytosol
-#pragma unroll
-        for (int f = 0; f < F; ++f)
-#pragma unroll
-            for (int z = 0; z < NZ; ++z) o[f * np + col + z * nxy] = c[f][z];
-        return;
-    }
     const R idx2 = (R)m.inv_dx2, idy2 = (R)m.inv_dy2, idz2 = (R)m.inv_dz2;
     const R dt = (R)m.dt;
     const R* __restrict__ cg = curg + st.node_base * NI;
@@ -344,7 +367,7 @@ __global__ void __launch_bounds__(UP_THREADS) k_update_s(const __grid_constant__
                                                          double* __restrict__ mouth, cb_site_scalars* __restrict__ sc, int nc,
                                                          const R* __restrict__ cyto, double* __restrict__ cin,
                                                          const int* __restrict__ rim_cnode, const int* __restrict__ dep_ptr,
-                                                         const int* __restrict__ dep_term) {
+                                                         const int* __restrict__ dep_term, const R* __restrict__ prev) {
     constexpr int F = NI + NP;
     constexpr int CSM = NI + 4;  // cytosol species slots (ions + at most 4 pairs)
     const int CS = m.n_ions + m.c_n_pairs;
@@ -357,13 +380,20 @@ __global__ void __launch_bounds__(UP_THREADS) k_update_s(const __grid_constant__
     R* u = fld + st.node_base * F;
     const int nx = st.nx, ny = st.ny, nz = st.nz, nxy = nx * ny;
     const long long np = st.npad;
-    // 1. mouth values: ions, pairs, free buffers (CaSim/DyadRD2DCPU.cpp:361-380)
+    // 1. mouth values: ions, pairs, free buffers (CaSim/DyadRD2DCPU.cpp:361-380). After
+    // k_rd_s (prev set) the rim holds its Dirichlet values already; a RyR on the rim
+    // reads the value the step carried over there, which is prev's
     for (int c = threadIdx.x; c < st.n_ch; c += UP_THREADS) {
         const int node = ch_node[st.ch_off + c];
         double* mo = mouth + (long long)(st.ch_off + c) * NS;
+        const R* src = u;
+        if (prev) {
+            const int cx = node % nx, cyy = (node / nx) % ny;
+            if (cx == 0 || cx == nx - 1 || cyy == 0 || cyy == ny - 1) src = prev + st.node_base * F;
+        }
         double v[F];
 #pragma unroll
-        for (int f = 0; f < F; ++f) v[f] = (double)u[f * np + node];
+        for (int f = 0; f < F; ++f) v[f] = (double)src[f * np + node];
 #pragma unroll
         for (int f = 0; f < F; ++f) mo[f] = v[f];
         for (int b = 0; b < m.n_buf; ++b) {
@@ -375,8 +405,9 @@ __global__ void __launch_bounds__(UP_THREADS) k_update_s(const __grid_constant__
         }
     }
     __syncthreads();
-    // 2. Dirichlet edges from the cytosol (CaSim/DyadRD2DCPU.cpp:274-303)
-    const int nrim = cb_rim_count(nx, ny);
+    // 2. Dirichlet edges from the cytosol (CaSim/DyadRD2DCPU.cpp:274-303), unless k_rd_s
+    // set them (prev set)
+    const int nrim = prev ? 0 : cb_rim_count(nx, ny);
     const R* cy = RD3D ? cyto + (long long)s * CS * nc : nullptr;
     for (int t = threadIdx.x; t < nrim * nz; t += UP_THREADS) {
         const int z = t / nrim, r = t - z * nrim;
