@@ -11,10 +11,19 @@
 // leave no idle blocks. Arithmetic and its order per node are those of the
 // generic kernels k_rd and k_cyto (the reference's node update,
 // CaSim/DyadRD2DCPU.cpp:394-490, CaSim/DyadRDCPU.cpp:404-506), which stay in use
-// for layouts these do not cover.
+// for layouts these do not cover, except that FP32 fields divide with the approximate
+// reciprocal in the sarcolemmal buffer factor and the SERCA term, as the resident path.
 #pragma once
 
 namespace stream {
+
+// FP32: the approximate reciprocal (2 ulp), as the resident path; FP64: IEEE division
+__device__ __forceinline__ float sdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double sdiv(double a, double b) { return a / b; }
+
+template <typename R, int NI, int NP, int NZ>
+__device__ __forceinline__ void interior_column(const cb_model& m, const cb_site& st, int col, const R* __restrict__ u, R* __restrict__ o,
+                                                const R* __restrict__ curg);
 
 constexpr int RD_THREADS = 256;
 constexpr int CY_THREADS = 128;
@@ -39,8 +48,11 @@ __global__ void __launch_bounds__(RD_THREADS) k_rd_s(const __grid_constant__ cb_
     const R* __restrict__ u = in + st.node_base * F;
     R* __restrict__ o = out + st.node_base * F;
     const int y = col / nx, x = col - y * nx;
-    if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1) {
-        R b[F];
+    // rim columns: their values are loaded first and stored last, so that a warp with rim
+    // and interior lanes does not wait for the rim's loads before the interior's work
+    const bool rim = x == 0 || x == nx - 1 || y == 0 || y == ny - 1;
+    R b[F];
+    if (rim) {
         if (m.cyto_type == CB_CYTO_RD3D) {
             const int CS = m.n_ions + m.c_n_pairs, nc = m.mc * m.mc * m.mc;
             const R* cy = cyto + (long long)tl.x * CS * nc;
@@ -59,12 +71,24 @@ __global__ void __launch_bounds__(RD_THREADS) k_rd_s(const __grid_constant__ cb_
 #pragma unroll
             for (int p = 0; p < NP; ++p) b[NI + p] = (R)q.c_bnd[p];
         }
+    } else {
+        interior_column<R, NI, NP, NZ>(m, st, col, u, o, curg);
+    }
+    if (rim) {
 #pragma unroll
         for (int f = 0; f < F; ++f)
 #pragma unroll
             for (int z = 0; z < NZ; ++z) o[f * np + col + z * nxy] = b[f];
-        return;
     }
+}
+
+// the interior column of k_rd_s
+template <typename R, int NI, int NP, int NZ>
+__device__ __forceinline__ void interior_column(const cb_model& m, const cb_site& st, int col, const R* __restrict__ u, R* __restrict__ o,
+                                                const R* __restrict__ curg) {
+    constexpr int F = NI + NP;
+    const int nx = st.nx, nxy = nx * st.ny;
+    const long long np = st.npad;
     R c[F][NZ];
 #pragma unroll
     for (int f = 0; f < F; ++f)
@@ -124,7 +148,7 @@ __global__ void __launch_bounds__(RD_THREADS) k_rd_s(const __grid_constant__ cb_
             if (sl_layer && m.has_sl[j]) {
                 const R s1 = (R)m.K1[j] + val[j];
                 const R s2 = (R)m.K2[j] + val[j];
-                e *= (R)1 / ((R)1 + (R)(m.N1[j] * m.K1[j]) / (s1 * s1) + (R)(m.N2[j] * m.K2[j]) / (s2 * s2));
+                e *= sdiv((R)1, (R)1 + sdiv((R)(m.N1[j] * m.K1[j]), s1 * s1) + sdiv((R)(m.N2[j] * m.K2[j]), s2 * s2));
             }
             o[j * np + n] = val[j] + e * dt;
         }
@@ -194,7 +218,7 @@ __global__ void __launch_bounds__(CY_THREADS) k_cyto_s(const __grid_constant__ c
                 const R i2 = ion * ion;
                 const R K2 = (R)(m.c_Kup[is] * m.c_Kup[is]);
                 const R b2 = (R)(m.c_bg[is] * m.c_bg[is]);
-                evo[j2] -= (R)m.c_Jmax[is] * (i2 / (i2 + K2) - b2 / (b2 + K2));
+                evo[j2] -= (R)m.c_Jmax[is] * (sdiv(i2, i2 + K2) - b2 / (b2 + K2));
                 ++is;
             }
         }
@@ -305,7 +329,7 @@ __global__ void __launch_bounds__((MC * MC + 31) / 32 * 32) k_cyto_m(const __gri
             evo[j2] += react;
             if (serca[j2]) {
                 const R i2 = ion * ion;
-                evo[j2] -= jmax[j2] * (i2 / (i2 + k2[j2]) - bterm[j2]);
+                evo[j2] -= jmax[j2] * (sdiv(i2, i2 + k2[j2]) - bterm[j2]);
             }
         }
 #pragma unroll
