@@ -64,6 +64,8 @@ cudaError_t cb_plain_reset(cb_dev& d, cudaStream_t st);
 cudaError_t cb_plain_init_opening(cb_dev& d, const int* d_first, int site_lo, int site_hi, cudaStream_t st);
 cudaError_t cb_plain_update(cb_dev& d, cudaStream_t st, long long* launches);
 cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);
+// whether the plain path's specialised streaming kernels serve the batch's layout
+bool cb_plain_streaming(cb_dev& d);
 
 // surrogate-driven gating without the RD step (plain.cu)
 cudaError_t cb_sg_features(cb_dev& d, int max_ch, int ld, float* X, cudaStream_t st);

@@ -722,6 +722,8 @@ cudaError_t cb_plain_update(cb_dev& d, cudaStream_t st, long long* launches) {
     return d.precision == 0 ? launch_update<double>(d, st) : launch_update<float>(d, st);
 }
 
+bool cb_plain_streaming(cb_dev& d) { return stream_tiles(d) > 0; }
+
 cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* launches) {
     const int per = 3 + (d.m.cyto_type == CB_CYTO_RD3D ? 1 : 0);
     for (long long i = 0; i < n; ++i) {

@@ -252,7 +252,10 @@ __global__ void __launch_bounds__((MC * MC + 31) / 32 * 32) k_cyto_m(const __gri
     const int col = (int)threadIdx.x;
     if (col >= MC2) return;
     const int j = col / MC, i = col - j * MC;
-    if (i == 0 || i == MC - 1 || j == 0 || j == MC - 1) return;
+    // the bath columns copy their values plane by plane with the others, so that every
+    // memory sector the block writes is written whole (a partly written sector is read
+    // back from memory when it leaves L2)
+    const bool bath = i == 0 || i == MC - 1 || j == 0 || j == MC - 1;
     const R* __restrict__ u = in + (long long)s * CS * NC + col;
     R* __restrict__ o = out + (long long)s * CS * NC + col;
     const double* __restrict__ ci = cin + (long long)s * CS * MC2 + col;
@@ -294,57 +297,66 @@ __global__ void __launch_bounds__((MC * MC + 31) / 32 * 32) k_cyto_m(const __gri
             }
         }
     }
-    R lo[CS], cu[CS], hi[CS];
+    // planes k-1, k, k+1 of the column and, loaded ahead, k+2 and k+3 (plane -1
+    // reflects to plane 1)
+    R lo[CS], cu[CS], hi[CS], p2[CS], p3[CS];
 #pragma unroll
     for (int c = 0; c < CS; ++c) {
         cu[c] = u[c * NC];
         hi[c] = u[c * NC + MC2];
+        p2[c] = u[c * NC + 2 * MC2];
+        p3[c] = u[c * NC + 3 * MC2];
         lo[c] = hi[c];
     }
 #pragma unroll
     for (int k = 0; k < MC - 1; ++k) {
         const int n = k * MC2;
-        R evo[CS];
+        if (bath) {
 #pragma unroll
-        for (int c = 0; c < CS; ++c) {
-            const R* v = u + c * NC + n;
-            const R cc = cu[c];
-            evo[c] = D[c] * ((v[1] - 2 * cc + v[-1]) * ih2 + (v[MC] - 2 * cc + v[-MC]) * ih2 + (hi[c] - 2 * cc + lo[c]) * ih2);
-        }
-#pragma unroll
-        for (int j2 = 0; j2 < NI; ++j2) {
-            const R ion = cu[j2];
-            R react = 0;
-#pragma unroll
-            for (int p = 0; p < NCP; ++p) {
-                if (pion[p] != j2) continue;
-                R fr = ctot[p];
-#pragma unroll
-                for (int q = 0; q < NCP; ++q)
-                    if (same[p] >> q & 1u) fr -= cu[NI + q];
-                const R R1 = koff[p] * cu[NI + p] - kon[p] * ion * fr;
-                evo[NI + p] += -R1;
-                react += R1;
-            }
-            evo[j2] += react;
-            if (serca[j2]) {
-                const R i2 = ion * ion;
-                evo[j2] -= jmax[j2] * (sdiv(i2, i2 + k2[j2]) - bterm[j2]);
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < CS; ++c) {
-            R e = evo[c];
-            if (k == 0) e += (R)ci[c * MC2];
-            o[c * NC + n] = cu[c] + e * dt;
-        }
-        if (k + 2 < MC) {
+            for (int c = 0; c < CS; ++c) o[c * NC + n] = cu[c];
+        } else {
+            R evo[CS];
 #pragma unroll
             for (int c = 0; c < CS; ++c) {
-                lo[c] = cu[c];
-                cu[c] = hi[c];
-                hi[c] = u[c * NC + n + 2 * MC2];
+                const R* v = u + c * NC + n;
+                const R cc = cu[c];
+                evo[c] = D[c] * ((v[1] - 2 * cc + v[-1]) * ih2 + (v[MC] - 2 * cc + v[-MC]) * ih2 + (hi[c] - 2 * cc + lo[c]) * ih2);
             }
+#pragma unroll
+            for (int j2 = 0; j2 < NI; ++j2) {
+                const R ion = cu[j2];
+                R react = 0;
+#pragma unroll
+                for (int p = 0; p < NCP; ++p) {
+                    if (pion[p] != j2) continue;
+                    R fr = ctot[p];
+#pragma unroll
+                    for (int q = 0; q < NCP; ++q)
+                        if (same[p] >> q & 1u) fr -= cu[NI + q];
+                    const R R1 = koff[p] * cu[NI + p] - kon[p] * ion * fr;
+                    evo[NI + p] += -R1;
+                    react += R1;
+                }
+                evo[j2] += react;
+                if (serca[j2]) {
+                    const R i2 = ion * ion;
+                    evo[j2] -= jmax[j2] * (sdiv(i2, i2 + k2[j2]) - bterm[j2]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CS; ++c) {
+                R e = evo[c];
+                if (k == 0) e += (R)ci[c * MC2];
+                o[c * NC + n] = cu[c] + e * dt;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CS; ++c) {
+            lo[c] = cu[c];
+            cu[c] = hi[c];
+            hi[c] = p2[c];
+            p2[c] = p3[c];
+            if (k + 4 < MC) p3[c] = u[c * NC + n + 4 * MC2];
         }
     }
 }

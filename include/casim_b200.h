@@ -48,7 +48,13 @@ typedef enum { CASIM_FP64 = 0, CASIM_FP32 = 1 } casim_precision;
  *           coupling), fields in HBM. Any site size.
  * RESIDENT: each site lives in one thread block's shared memory for the whole
  *           call; all time steps run inside one persistent launch.
- * AUTO:     RESIDENT when every site fits, else PLAIN. */
+ * AUTO:     PLAIN for 3D clefts or a 3D cytosol whose state (one copy of the
+ *           fields and the cytosol) is larger than the device's L2 cache and whose
+ *           species layout the streaming kernels serve (1-2 ions, at most 4 pairs,
+ *           1 or 3 cleft layers at every site): there the resident kernel's per-step
+ *           chain of phases is slower than streaming the state from HBM. Otherwise
+ *           RESIDENT when every site fits, else PLAIN. casim_b200_path_note says
+ *           which rule chose. */
 typedef enum { CASIM_PATH_AUTO = 0, CASIM_PATH_PLAIN = 1, CASIM_PATH_RESIDENT = 2 } casim_path;
 
 /* Optional per-site table (struct of arrays). Any NULL member falls back to
