@@ -26,6 +26,9 @@ __device__ __forceinline__ void interior_column(const cb_model& m, const cb_site
                                                 const R* __restrict__ curg);
 
 constexpr int RD_THREADS = 256;
+// resident blocks of k_rd_s asked of the compiler: a full SM (32 registers) where the
+// column fits them without spilling (FP32, up to 3 species), fewer for wider columns
+constexpr int rd_min_blocks(int w, int F) { return w == 4 ? (F <= 3 ? 8 : 4) : (F <= 3 ? 4 : 2); }
 constexpr int CY_THREADS = 128;
 
 // Cleft step of the columns [tile.y, tile.y + 256) of site tile.x. The rim columns take
@@ -34,7 +37,7 @@ constexpr int CY_THREADS = 128;
 // its latest step (cyto, RD3D) or the pool values of this step (sc); the Update then
 // leaves the rim alone (k_update_s with prev set).
 template <typename R, int NI, int NP, int NZ>
-__global__ void __launch_bounds__(RD_THREADS) k_rd_s(const __grid_constant__ cb_model m, const cb_site* __restrict__ sites,
+__global__ void __launch_bounds__(RD_THREADS, rd_min_blocks(sizeof(R), NI + NP)) k_rd_s(const __grid_constant__ cb_model m, const cb_site* __restrict__ sites,
                                                      const int2* __restrict__ tiles, const R* __restrict__ in,
                                                      R* __restrict__ out, const R* __restrict__ curg,
                                                      const cb_site_scalars* __restrict__ sc, const R* __restrict__ cyto) {
@@ -82,7 +85,7 @@ __global__ void __launch_bounds__(RD_THREADS) k_rd_s(const __grid_constant__ cb_
     }
 }
 
-// the interior column of k_rd_s
+// the interior column of k_rd_s; the loop-invariant model terms are read once
 template <typename R, int NI, int NP, int NZ>
 __device__ __forceinline__ void interior_column(const cb_model& m, const cb_site& st, int col, const R* __restrict__ u, R* __restrict__ o,
                                                 const R* __restrict__ curg) {
@@ -97,6 +100,25 @@ __device__ __forceinline__ void interior_column(const cb_model& m, const cb_site
     const R idx2 = (R)m.inv_dx2, idy2 = (R)m.inv_dy2, idz2 = (R)m.inv_dz2;
     const R dt = (R)m.dt;
     const R* __restrict__ cg = curg + st.node_base * NI;
+    R D[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) D[f] = (R)(f < NI ? m.D_ion[f] : m.D_pair[f - NI]);
+    R koff[NP > 0 ? NP : 1], kon[NP > 0 ? NP : 1], ctot[NP > 0 ? NP : 1];
+    unsigned same[NP > 0 ? NP : 1];  // bit q: pair q binds pair p's buffer
+    int pion[NP > 0 ? NP : 1];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        const int b = m.pair_buf[p];
+        koff[p] = (R)m.koff[p];
+        kon[p] = (R)m.kon[p];
+        ctot[p] = (R)m.Ctot[b];
+        pion[p] = NI == 1 ? 0 : m.pair_ion[p];
+        unsigned bits = 0;
+#pragma unroll
+        for (int q = 0; q < NP; ++q)
+            if (m.pair_buf[q] == b) bits |= 1u << q;
+        same[p] = bits;
+    }
 #pragma unroll
     for (int z = 0; z < NZ; ++z) {
         const int n = col + z * nxy;
@@ -109,11 +131,10 @@ __device__ __forceinline__ void interior_column(const cb_model& m, const cb_site
             const R* v = u + f * np;
             const R cc = c[f][z];
             val[f] = cc;
-            const R D = (R)(f < NI ? m.D_ion[f] : m.D_pair[f - NI]);
-            if (D != (R)0) {
+            if (D[f] != (R)0) {
                 R lap = (v[n + 1] - 2 * cc + v[n - 1]) * idx2 + (v[n + nx] - 2 * cc + v[n - nx]) * idy2;
                 if (NZ > 1) lap = lap + (c[f][zr] - 2 * cc + c[f][zl]) * idz2;
-                evo[f] = D * lap;
+                evo[f] = D[f] * lap;
             } else {
                 evo[f] = 0;
             }
@@ -124,21 +145,19 @@ __device__ __forceinline__ void interior_column(const cb_model& m, const cb_site
         for (int j = 0; j < NI; ++j) Rj[j] = 0;
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
-            const int b = m.pair_buf[p];
-            R fr = (R)m.Ctot[b];
+            R fr = ctot[p];
 #pragma unroll
             for (int q = 0; q < NP; ++q)
-                if (m.pair_buf[q] == b) fr -= val[NI + q];
-            const int j = m.pair_ion[p];
+                if (same[p] >> q & 1u) fr -= val[NI + q];
             R ion = val[0];
 #pragma unroll
             for (int i = 1; i < NI; ++i)
-                if (j == i) ion = val[i];
-            const R R1 = (R)m.koff[p] * val[NI + p] - (R)m.kon[p] * ion * fr;
+                if (pion[p] == i) ion = val[i];
+            const R R1 = koff[p] * val[NI + p] - kon[p] * ion * fr;
             evo[NI + p] += -R1;
 #pragma unroll
             for (int i = 0; i < NI; ++i)
-                if (j == i) Rj[i] += R1;
+                if (pion[p] == i) Rj[i] += R1;
         }
         const bool sl_layer = NZ == 1 || z == NZ - 1;
 #pragma unroll
