@@ -294,6 +294,7 @@ casim_status casim_b200_destroy(casim_h h) {
     if (h->d.rs_counter) cudaFree(h->d.rs_counter);
     if (h->d.rs_pow2) cudaFree(h->d.rs_pow2);
     if (h->d.st_tiles) cudaFree(h->d.st_tiles);
+    if (h->d.st_chcol) cudaFree(h->d.st_chcol);
     if (h->d.pre_jump) cudaFree(h->d.pre_jump);
     cb_resident_free(h->d);
     if (h->sg_exec) cudaGraphExecDestroy(h->sg_exec);

@@ -56,6 +56,7 @@ struct cb_dev {
     int2* st_tiles = nullptr;
     int st_ntiles = 0;
     int st_nz = -1;
+    unsigned* st_chcol = nullptr;  // bit per cleft column (node_base + x + nx*y): holds a RyR
     unsigned long long* pre_jump = nullptr;  // k_pre_r: MRG32k3a jumps A^(2l), l < 32
 };
 

@@ -434,6 +434,17 @@ int stream_tiles(cb_dev& d) {
         return 0;
     }
     d.st_ntiles = (int)tiles.size();
+    // the columns that hold a RyR: bit (node_base + x + nx*y), one word per 32 nodes
+    std::vector<unsigned> bits((size_t)(d.total_nodes + 31) / 32, 0u);
+    std::vector<int> chn((size_t)d.total_ch);
+    if (d.total_ch && cudaMemcpy(chn.data(), d.ch_node, sizeof(int) * chn.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+    for (int s = 0; s < d.S; ++s)
+        for (int c = 0; c < hs[s].n_ch; ++c) {
+            const long long b = hs[s].node_base + chn[hs[s].ch_off + c] % (hs[s].nx * hs[s].ny);
+            bits[b >> 5] |= 1u << (b & 31);
+        }
+    if (cudaMalloc(&d.st_chcol, sizeof(unsigned) * bits.size()) != cudaSuccess) return 0;
+    if (cudaMemcpy(d.st_chcol, bits.data(), sizeof(unsigned) * bits.size(), cudaMemcpyHostToDevice) != cudaSuccess) return 0;
     d.st_nz = nz;
     return d.st_ntiles;
 }
@@ -523,10 +534,10 @@ void launch_rd_s(cb_dev& d, cudaStream_t st) {
     const R* cy = (const R*)d.cyto[1 - d.ccur];
     if (d.st_nz == 1)
         stream::k_rd_s<R, NI, NP, 1><<<d.st_ntiles, stream::RD_THREADS, 0, st>>>(d.m, d.sites, d.st_tiles, in, out, (const R*)d.curgrid,
-                                                                                 d.sc, cy);
+                                                                                 d.sc, cy, d.st_chcol);
     else
         stream::k_rd_s<R, NI, NP, 3><<<d.st_ntiles, stream::RD_THREADS, 0, st>>>(d.m, d.sites, d.st_tiles, in, out, (const R*)d.curgrid,
-                                                                                 d.sc, cy);
+                                                                                 d.sc, cy, d.st_chcol);
 }
 
 template <typename R, int NI>

@@ -40,7 +40,8 @@ template <typename R, int NI, int NP, int NZ>
 __global__ void __launch_bounds__(RD_THREADS, rd_min_blocks(sizeof(R), NI + NP)) k_rd_s(const __grid_constant__ cb_model m, const cb_site* __restrict__ sites,
                                                      const int2* __restrict__ tiles, const R* __restrict__ in,
                                                      R* __restrict__ out, const R* __restrict__ curg,
-                                                     const cb_site_scalars* __restrict__ sc, const R* __restrict__ cyto) {
+                                                     const cb_site_scalars* __restrict__ sc, const R* __restrict__ cyto,
+                                                     const unsigned* __restrict__ chcol) {
     constexpr int F = NI + NP;
     const int2 tl = tiles[blockIdx.x];
     const cb_site st = sites[tl.x];
@@ -75,7 +76,11 @@ __global__ void __launch_bounds__(RD_THREADS, rd_min_blocks(sizeof(R), NI + NP))
             for (int p = 0; p < NP; ++p) b[NI + p] = (R)q.c_bnd[p];
         }
     } else {
-        interior_column<R, NI, NP, NZ>(m, st, col, u, o, curg);
+        // RyR currents exist only in the columns that hold a RyR (bit col of the site's
+        // words in chcol); elsewhere the current grid is zero and is not read
+        const long long bit = st.node_base + col;
+        const bool has_ch = (chcol[bit >> 5] >> (bit & 31)) & 1u;
+        interior_column<R, NI, NP, NZ>(m, st, col, u, o, has_ch ? curg : nullptr);
     }
     if (rim) {
 #pragma unroll
@@ -99,7 +104,12 @@ __device__ __forceinline__ void interior_column(const cb_model& m, const cb_site
         for (int z = 0; z < NZ; ++z) c[f][z] = u[f * np + col + z * nxy];
     const R idx2 = (R)m.inv_dx2, idy2 = (R)m.inv_dy2, idz2 = (R)m.inv_dz2;
     const R dt = (R)m.dt;
-    const R* __restrict__ cg = curg + st.node_base * NI;
+    // the column's RyR currents (curg null: none in this column)
+    R cur[NI][NZ];
+#pragma unroll
+    for (int j = 0; j < NI; ++j)
+#pragma unroll
+        for (int z = 0; z < NZ; ++z) cur[j][z] = curg ? curg[st.node_base * NI + j * np + col + z * nxy] : (R)0;
     R D[F];
 #pragma unroll
     for (int f = 0; f < F; ++f) D[f] = (R)(f < NI ? m.D_ion[f] : m.D_pair[f - NI]);
@@ -163,7 +173,7 @@ __device__ __forceinline__ void interior_column(const cb_model& m, const cb_site
 #pragma unroll
         for (int j = 0; j < NI; ++j) {
             R e = evo[j] + Rj[j];
-            e += cg[j * np + n];
+            e += cur[j][z];
             if (sl_layer && m.has_sl[j]) {
                 const R s1 = (R)m.K1[j] + val[j];
                 const R s2 = (R)m.K2[j] + val[j];
