@@ -158,6 +158,9 @@ class Clocks:
 # bench step on 512 sites of the config-2 workload, per site (FP32): each launch loads
 # and stores every site once, so the traffic scales with the sites, not with the steps
 RESIDENT_DRAM_BYTES_PER_SITE = 319.7e6 / 512
+# ncu DRAM bytes (read + write) of one k_rd_s launch per cleft node (fp32, config-2 sites):
+# 129.4 MB + 82.6 MB on the 10 352 496 cleft nodes of 512 sites of this workload
+STREAM_CLEFT_DRAM_BYTES_PER_NODE = (129.430016e6 + 82.531840e6) / 10352496
 
 
 def measured_peak_hbm():
@@ -177,6 +180,52 @@ def algorithmic_bytes_per_step(sim, sites, params):
     cyto = sim.S * sim.info.cyto_nodes
     CS = sim.info.n_cyto_species if sim.info.cyto_nodes else 0
     return 2 * w * (cleft * F + cyto * CS)
+
+
+def dominant_kernel(args, sim, sites, bytes_step, peak):
+    """Roofline of the kernel that takes the largest share of a time step, from CUDA
+    events on the library's stream: achieved = its algorithmic bytes per launch / its
+    launch time (plain path: the average of 5 profiled time steps, every kernel timed;
+    resident path: one launch of --chunk time steps)."""
+    w = 4 if sim.info.precision == 1 else 8
+    F = sim.info.n_ions + sim.info.n_pairs
+    cleft_nodes = int(np.sum(np.asarray(sites["nx"], np.int64) * np.asarray(sites["ny"]) * np.asarray(sites["nz"])))
+    CS = sim.info.n_cyto_species if sim.info.cyto_nodes else 0
+    if sim.path == "resident":
+        sim.step(args.chunk)
+        sim.synchronize()
+        kms = sim.last_step_ms()
+        achieved = bytes_step * args.chunk / (kms / 1e3) / 1e9
+        traffic = (RESIDENT_DRAM_BYTES_PER_SITE * sim.S
+                   if args.precision == "fp32" and args.config == "c2" else None)
+        return {"bound": "hbm", "kernel": "k_resident", "achieved": achieved, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "launch_ms": kms,
+                "note": "achieved = algorithmic bytes (2 x field bytes per node-step) of one launch (--chunk time steps) / "
+                        "its device time; the resident path keeps fields on chip, so this is an effective bandwidth; "
+                        "traffic = ncu DRAM bytes of one launch (0.63 MB per site, measured on 512 sites of this "
+                        "workload and scaled by sites)"}
+    prof = {}
+    for _ in range(5):
+        for k, v in sim.profile_step().items():
+            prof[k] = prof.get(k, 0.0) + v / 5
+    kbytes = {"cleft": 2 * w * F * cleft_nodes, "cytosol": 2 * w * CS * sim.S * sim.info.cyto_nodes}
+    names = {"gating": "k_pre_r (RyR gating, pools)", "cytosol": "k_cyto_m (RD3D cytosol)", "cleft": "k_rd_s (cleft stencil)",
+             "update": "k_update_s (Update)"}
+    dom = max(prof, key=prof.get)
+    step_ms = sum(prof.values())
+    kernels = {names[k]: {"ms": v, "share": v / step_ms,
+                          "achieved_gbs": (kbytes[k] / (v / 1e3) / 1e9 if k in kbytes and v > 0 else None)}
+               for k, v in prof.items()}
+    achieved = kbytes.get(dom, bytes_step) / (prof[dom] / 1e3) / 1e9
+    traffic = (STREAM_CLEFT_DRAM_BYTES_PER_NODE * cleft_nodes
+               if STREAM_CLEFT_DRAM_BYTES_PER_NODE and dom == "cleft" and args.precision == "fp32" and args.config == "c2"
+               else None)
+    return {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "launch_ms": prof[dom], "kernels": kernels,
+            "step_achieved_gbs": bytes_step / (step_ms / 1e3) / 1e9,
+            "note": "achieved = the kernel's algorithmic bytes per launch (each stored value of its field read and "
+                    "written once per node-step) / its CUDA-event launch time; traffic = ncu DRAM bytes per launch "
+                    "(measured on 512 sites of this workload, scaled by cleft nodes)"}
 
 
 def cpu_model():
@@ -534,14 +583,9 @@ def main():
     total_sites = len(s_global["nx"])
     value = total_sites * args.chunk * args.steps * dt_ms / (ms / 1e3)
     ok_finite, _ = sim.check_finite()
-    # per-launch kernel time of the dominant kernel (resident path: one kernel per bench step)
-    sim.step(args.chunk)
-    sim.synchronize()
-    kms = sim.last_step_ms()
     bytes_step = algorithmic_bytes_per_step(sim, s, p)
     peak, peak_kind = measured_peak_hbm()
-    achieved = bytes_step * args.chunk / (kms / 1e3) / 1e9
-    kernel_name = "k_resident" if sim.path == "resident" else "plain step (k_pre+k_cyto+k_rd+k_update)"
+    roof = dominant_kernel(args, sim, s, bytes_step, peak)
     result = {
         "metric": "simulated site-ms/s", "value": value, "unit": "site-ms/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -555,14 +599,7 @@ def main():
         "gpu_launches": int(timing["launches_per"] * args.steps),
         "finite": bool(ok_finite),
         "outputs": outputs_summary(outputs) if rank == 0 else None,
-        "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": (RESIDENT_DRAM_BYTES_PER_SITE * sim.S
-                                 if sim.path == "resident" and args.precision == "fp32" and args.config == "c2" else None),
-                     "note": "achieved = algorithmic bytes (2 x field bytes per node-step) of one bench step / its device "
-                             "time; the resident path keeps fields on chip, so this is an effective bandwidth; traffic = "
-                             "ncu DRAM bytes of the launches of one bench step (0.63 MB per site per launch, measured "
-                             "on 512 sites of this workload and scaled by sites)"},
+        "roofline": dict(roof, peak=peak, peak_kind=peak_kind),
         "clocks": timing["clocks"],
     }
     if not args.no_e2e:

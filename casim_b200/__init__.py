@@ -40,7 +40,7 @@ EXPORTS = (
     "casim_b200_get_jsr", "casim_b200_get_total_current", "casim_b200_get_efflux", "casim_b200_get_cyto",
     "casim_b200_get_cyto_field", "casim_b200_set_cyto_field", "casim_b200_get_draws", "casim_b200_get_release", "casim_b200_check_finite",
     "casim_b200_get_all_mouth", "casim_b200_get_all_states", "casim_b200_last_step_ms",
-    "casim_b200_last_step_launches", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
+    "casim_b200_last_step_launches", "casim_b200_profile_step", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
     "casim_b200_rng_draws_static", "casim_b200_path_note",
     "casim_b200_set_all_states", "casim_b200_sg_features", "casim_b200_sg_set_mouth",
     "casim_b200_sg_gate_steps", "casim_b200_sg_run", "casim_b200_sg_create", "casim_b200_sg_destroy", "casim_b200_sg_set_stream", "casim_b200_sg_num_params",
@@ -145,6 +145,7 @@ def lib():
                                                ctypes.POINTER(HybridStats)]
         L.casim_b200_last_step_ms.argtypes = [vp, dp]
         L.casim_b200_last_step_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.casim_b200_profile_step.argtypes = [vp, dp, i32, ip]
         L.casim_b200_debug_rng.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]
         L.casim_b200_set_site_jsr.argtypes = [vp, dp]
         L.casim_b200_path_note.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
@@ -337,6 +338,15 @@ class ReleaseSiteBatch:
         v = ctypes.c_int64()
         self._ck(lib().casim_b200_last_step_launches(self.h, ctypes.byref(v)))
         return v.value
+
+    def profile_step(self):
+        """One time step with each kernel timed: {kernel: ms} (plain path: gating, cytosol,
+        cleft, update; resident path: the one launch)."""
+        ms = np.zeros(4)
+        n = ctypes.c_int32()
+        self._ck(lib().casim_b200_profile_step(self.h, _p(ms, ctypes.c_double), 4, ctypes.byref(n)))
+        names = ("k_resident",) if self.path == "resident" else ("gating", "cytosol", "cleft", "update")
+        return {k: float(ms[i]) for i, k in enumerate(names[:n.value])}
 
     # -- getters ---------------------------------------------------------
     def field(self, site, species):

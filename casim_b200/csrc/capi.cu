@@ -465,6 +465,38 @@ casim_status casim_b200_step(casim_h h, int64_t n) {
     END_GUARD(h)
 }
 
+casim_status casim_b200_profile_step(casim_h h, double* ms, int32_t n, int32_t* count) {
+    GUARD(h)
+    if (!ms || n < 1 || !count) throw std::runtime_error("profile_step: bad argument");
+    if (h->tr) throw std::runtime_error("profile_step: not with an open-RyR trace enabled");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    if (h->path == CASIM_PATH_RESIDENT) {
+        long long launches = 0;
+        ck(cudaEventRecord(h->ev0, h->stream), "cudaEventRecord");
+        ck(cb_resident_step(h->d, 1, h->stream, &launches), "resident step");
+        ck(cudaEventRecord(h->ev1, h->stream), "cudaEventRecord");
+        ck(cudaEventSynchronize(h->ev1), "cudaEventSynchronize");
+        float t = 0;
+        ck(cudaEventElapsedTime(&t, h->ev0, h->ev1), "cudaEventElapsedTime");
+        ms[0] = t;
+        *count = 1;
+    } else {
+        cudaEvent_t ev[5] = {};
+        for (int k = 0; k < 5; ++k) ck(cudaEventCreate(&ev[k]), "cudaEventCreate");
+        cudaError_t e = cb_plain_step_marked(h->d, h->stream, ev);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[4]);
+        float t[4] = {};
+        for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]);
+        for (int k = 0; k < 5; ++k) cudaEventDestroy(ev[k]);
+        ck(e, "profile_step");
+        for (int k = 0; k < 4 && k < n; ++k) ms[k] = t[k];
+        *count = n < 4 ? n : 4;
+    }
+    h->timed = false;
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
 casim_status casim_b200_trace_enable(casim_h h, int64_t every_steps, int64_t max_samples) {
     GUARD(h)
     if (every_steps < 1 || max_samples < 1) throw std::runtime_error("trace needs every_steps >= 1 and max_samples >= 1");

@@ -67,6 +67,8 @@ cudaError_t cb_plain_update(cb_dev& d, cudaStream_t st, long long* launches);
 cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);
 // whether the plain path's specialised streaming kernels serve the batch's layout
 bool cb_plain_streaming(cb_dev& d);
+// one plain time step with ev[0..4] recorded around its four kernels
+cudaError_t cb_plain_step_marked(cb_dev& d, cudaStream_t st, cudaEvent_t* ev);
 
 // surrogate-driven gating without the RD step (plain.cu)
 cudaError_t cb_sg_features(cb_dev& d, int max_ch, int ld, float* X, cudaStream_t st);

@@ -574,7 +574,12 @@ void launch_cyto_np(cb_dev& d, cudaStream_t st) {
 }
 
 template <typename R>
-cudaError_t launch_step(cb_dev& d, cudaStream_t st) {
+// ev (optional, 5 events): recorded before the gating kernel and after each of the
+// gating, cytosol, cleft and Update kernels
+cudaError_t launch_step(cb_dev& d, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+    auto mark = [&](int k) { return ev ? cudaEventRecord(ev[k], st) : cudaSuccess; };
+    cudaError_t e0 = mark(0);
+    if (e0 != cudaSuccess) return e0;
     const bool fast = stream_tiles(d) > 0;
     if (fast && !d.mwc && pre_jump(d))
         stream::k_pre_r<<<(d.S + stream::PRE_WARPS - 1) / stream::PRE_WARPS, 32 * stream::PRE_WARPS, 0, st>>>(
@@ -582,6 +587,7 @@ cudaError_t launch_step(cb_dev& d, cudaStream_t st) {
     else
         k_pre<<<(d.S + 127) / 128, 128, 0, st>>>(d.m, d.S, d.NS, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0],
                                                    d.spx[1], d.spc[1], d.ch_micro, d.mwc);
+    if ((e0 = mark(1)) != cudaSuccess) return e0;
     if (d.m.cyto_type == CB_CYTO_RD3D) {
         if (fast) {
             if (d.m.n_ions == 1) launch_cyto_np<R, 1>(d, st);
@@ -592,6 +598,7 @@ cudaError_t launch_step(cb_dev& d, cudaStream_t st) {
         }
         d.ccur ^= 1;
     }
+    if ((e0 = mark(2)) != cudaSuccess) return e0;
     if (fast) {
         if (d.m.n_ions == 1) launch_rd_np<R, 1>(d, st);
         else launch_rd_np<R, 2>(d, st);
@@ -600,7 +607,9 @@ cudaError_t launch_step(cb_dev& d, cudaStream_t st) {
         k_rd<R><<<g, 256, 0, st>>>(d.m, d.sites, (const R*)d.fields[d.cur], (R*)d.fields[1 - d.cur], (const R*)d.curgrid);
     }
     d.cur ^= 1;
-    return launch_update<R>(d, st, fast);
+    if ((e0 = mark(3)) != cudaSuccess) return e0;
+    if ((e0 = launch_update<R>(d, st, fast)) != cudaSuccess) return e0;
+    return mark(4);
 }
 
 // ---- surrogate-driven gating (no RD): the mouth Ca comes from the surrogate network
@@ -734,6 +743,10 @@ cudaError_t cb_plain_update(cb_dev& d, cudaStream_t st, long long* launches) {
 }
 
 bool cb_plain_streaming(cb_dev& d) { return stream_tiles(d) > 0; }
+
+cudaError_t cb_plain_step_marked(cb_dev& d, cudaStream_t st, cudaEvent_t* ev) {
+    return d.precision == 0 ? launch_step<double>(d, st, ev) : launch_step<float>(d, st, ev);
+}
 
 cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* launches) {
     const int per = 3 + (d.m.cyto_type == CB_CYTO_RD3D ? 1 : 0);

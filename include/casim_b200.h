@@ -233,6 +233,13 @@ casim_status casim_b200_path_note(casim_h h, char* buf, size_t n);
 casim_status casim_b200_last_step_ms(casim_h h, double* out);
 /* Number of kernel launches issued by the last casim_b200_step call. */
 casim_status casim_b200_last_step_launches(casim_h h, int64_t* out);
+/* Profiling (no counterpart in the reference): advance every site by one time step
+ * like casim_b200_step(h, 1) and return the device time in ms of each of its kernels,
+ * from CUDA events on the handle's stream. Plain path: ms[0..3] = RyR gating and pools,
+ * RD3D cytosol (0 without it), cleft stencil, Update; resident path: ms[0] = the one
+ * launch. *count receives how many entries were written (at most n). Synchronous; not
+ * while an open-RyR trace is enabled. */
+casim_status casim_b200_profile_step(casim_h h, double* ms, int32_t n, int32_t* count);
 
 /* Diagnostic: n runif() draws of the MRG32k3a stream with the given seed,
  * generated by a device kernel (the generator every site's gating uses).
