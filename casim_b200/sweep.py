@@ -2,13 +2,14 @@
 Mg, half gated by the tetrameric MWC law (TwoStateMWC) and half by the same
 law tabulated for TwoStateSpline, run side by side on one GPU.
 
-A batch holds one gating model, and the resident path takes a batch only if
-every site fits the shared memory of a 16-block cluster, which the largest
-sites with the second ion do not. So each half is ordered by size and split
-at the largest cleft side whose sites the resident path still takes: the
-smaller sites run resident, the rest on the plain path. The (up to four)
-batches run on their own CUDA streams; the simulated site-ms/s counts all of
-them. After the run the open RyR counts and the released Ca of the halves are
+A batch holds one gating model. By default each half is one batch on the path
+the library picks (a batch this large streams its fields from HBM). With
+--path split each half is ordered by size and split at the largest cleft side
+whose sites the resident path still takes (the largest sites with the second
+ion fit no 16-block cluster): the smaller sites run resident, the rest
+streaming. The batches run on their own CUDA streams; the simulated
+site-ms/s counts all of them. After the run the open RyR counts and the
+released Ca of the halves are
 compared by two-sample KS tests: the tabulated law is the analytic one up to
 the spline's interpolation error, so the distributions should agree.
 
@@ -69,7 +70,9 @@ def run_sweep(n_sites=16384, t_ms=0.2, chunk=200, precision="fp32", seed=5, path
     halves = configs.config5(n_sites=n_sites, seed=seed)
     sims, streams, parts = [], [], []
     for h, (p, s) in enumerate(halves):
-        split = split_resident(p, s, precision) if path == "auto" else [(np.arange(len(s["nx"])), path)]
+        # "auto": one batch per half and the library's choice (large 3D batches stream);
+        # "split": the sites that fit a cluster resident, the rest streaming
+        split = split_resident(p, s, precision) if path == "split" else [(np.arange(len(s["nx"])), path)]
         for idx, pth in split:
             if idx.size == 0:
                 continue
@@ -130,9 +133,10 @@ def main():
     ap.add_argument("--sites", type=int, default=16384)
     ap.add_argument("--ms", type=float, default=0.2, help="simulated time per site")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--path", default="auto", choices=["auto", "split", "plain", "resident"])
     a = ap.parse_args()
     t0 = time.time()
-    res = run_sweep(a.sites, a.ms, precision=a.precision)
+    res = run_sweep(a.sites, a.ms, precision=a.precision, path=a.path)
     res["wall_s"] = time.time() - t0
     print(json.dumps(res))
 

@@ -43,9 +43,10 @@ def test_config5_halves_match_oracle(cuda_device, tmp_path, path, precision):
         sim.close()
 
 
-def test_sweep_runner_small(cuda_device):
+@pytest.mark.parametrize("path", ["auto", "split"])
+def test_sweep_runner_small(cuda_device, path):
     from casim_b200.sweep import run_sweep
-    res = run_sweep(n_sites=64, t_ms=0.02, chunk=100)
+    res = run_sweep(n_sites=64, t_ms=0.02, chunk=100, path=path)
     assert all(res["finite"]), res
     assert res["site_ms_per_s"] > 0
     assert [h["model"] for h in res["halves"]] == ["TwoStateMWC", "TwoStateSpline"]
@@ -54,5 +55,7 @@ def test_sweep_runner_small(cuda_device):
     for half in (0, 1):
         bs = [b for b in res["batches"] if b["half"] == half]
         assert sum(b["sites"] for b in bs) == 32
-        if len(bs) == 2:
+        if path == "auto":
+            assert len(bs) == 1
+        elif len(bs) == 2:
             assert [b["path"] for b in bs] == ["resident", "plain"]
