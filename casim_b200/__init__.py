@@ -40,7 +40,7 @@ EXPORTS = (
     "casim_b200_get_jsr", "casim_b200_get_total_current", "casim_b200_get_efflux", "casim_b200_get_cyto",
     "casim_b200_get_cyto_field", "casim_b200_set_cyto_field", "casim_b200_get_draws", "casim_b200_get_release", "casim_b200_check_finite",
     "casim_b200_get_all_mouth", "casim_b200_get_all_states", "casim_b200_last_step_ms",
-    "casim_b200_last_step_launches", "casim_b200_profile_step", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
+    "casim_b200_last_step_launches", "casim_b200_profile_step", "casim_b200_set_site_gating", "casim_b200_debug_rng", "casim_b200_set_site_jsr",
     "casim_b200_rng_draws_static", "casim_b200_path_note",
     "casim_b200_set_all_states", "casim_b200_sg_features", "casim_b200_sg_set_mouth",
     "casim_b200_sg_gate_steps", "casim_b200_sg_run", "casim_b200_sg_create", "casim_b200_sg_destroy", "casim_b200_sg_set_stream", "casim_b200_sg_num_params",
@@ -146,6 +146,7 @@ def lib():
         L.casim_b200_last_step_ms.argtypes = [vp, dp]
         L.casim_b200_last_step_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.casim_b200_profile_step.argtypes = [vp, dp, i32, ip]
+        L.casim_b200_set_site_gating.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip, i32]
         L.casim_b200_debug_rng.argtypes = [ctypes.POINTER(ctypes.c_uint32), i64, dp]
         L.casim_b200_set_site_jsr.argtypes = [vp, dp]
         L.casim_b200_path_note.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
@@ -338,6 +339,13 @@ class ReleaseSiteBatch:
         v = ctypes.c_int64()
         self._ck(lib().casim_b200_last_step_launches(self.h, ctypes.byref(v)))
         return v.value
+
+    def set_site_gating(self, params, sites, base_dir=None, json_text=None):
+        """Gate the listed sites by the two-state RyR model of `params` (a Parameters
+        dict of the same ions); the other sites keep theirs. Plain path only."""
+        raw = json_text.encode() if json_text is not None else json.dumps(params).encode()
+        idx = np.ascontiguousarray(sites, dtype=np.int32)
+        self._ck(lib().casim_b200_set_site_gating(self.h, raw, (base_dir or "").encode(), _p(idx, ctypes.c_int32), int(idx.size)))
 
     def profile_step(self):
         """One time step with each kernel timed: {kernel: ms} (plain path: gating, cytosol,

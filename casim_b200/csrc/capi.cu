@@ -54,6 +54,11 @@ void ck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw cuda_fail(e, what);
 }
 
+// a request outside what this build serves (CASIM_EUNSUPPORTED)
+struct unsupported : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
 template <typename T>
 T* dalloc(casim_b200_sim* h, size_t n) {
     void* p = nullptr;
@@ -84,6 +89,9 @@ casim_status set_err(casim_b200_sim* h, casim_status s, const std::string& msg) 
     }                                                                       \
     catch (const cuda_fail& e) {                                            \
         return set_err(h, e.code == cudaErrorMemoryAllocation ? CASIM_ENOMEM : CASIM_ECUDA, e.what()); \
+    }                                                                       \
+    catch (const unsupported& e) {                                          \
+        return set_err(h, CASIM_EUNSUPPORTED, e.what());                    \
     }                                                                       \
     catch (const std::exception& e) {                                       \
         return set_err(h, CASIM_EINVAL, e.what());                          \
@@ -497,6 +505,70 @@ casim_status casim_b200_profile_step(casim_h h, double* ms, int32_t n, int32_t* 
     END_GUARD(h)
 }
 
+casim_status casim_b200_set_site_gating(casim_h h, const char* json_text, const char* base_dir, const int32_t* sites, int32_t n) {
+    GUARD(h)
+    if (!json_text || !sites || n < 1) throw std::runtime_error("set_site_gating: bad argument");
+    if (h->path != CASIM_PATH_PLAIN) throw unsupported("per-site gating models run on the plain path (create the handle with it)");
+    if (h->d.mwc || h->d.m.ch_model == CB_SINGLE_SITE_MWC) throw unsupported("per-site gating models are two-state models");
+    if (!cb_plain_gating_ready(h->d)) throw unsupported("per-site gating models need the specialised streaming kernels");
+    for (int k = 0; k < n; ++k) check_site(h, sites[k]);
+    // parse the JSON against a one-site table shaped like site 0 (no coordinates file is
+    // read: only the gating model is taken from it)
+    cb_site s0{};
+    ck(cudaMemcpy(&s0, h->d.sites, sizeof(cb_site), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    int32_t tnx = s0.nx, tny = s0.ny, tnz = s0.nz, tnch = 1;
+    double tx = 0.5 * (s0.nx - 1) * h->d.m.dx, ty = 0.5 * (s0.ny - 1) * h->d.m.dy;
+    uint32_t tseed[6] = {12345, 12345, 12345, 12345, 12345, 12345};
+    casim_site_table tab{};
+    tab.n_sites = 1;
+    tab.nx = &tnx;
+    tab.ny = &tny;
+    tab.nz = &tnz;
+    tab.n_channels = &tnch;
+    tab.ch_x = &tx;
+    tab.ch_y = &ty;
+    tab.seeds = tseed;
+    const cb_config cfg = cb_parse_config(json_text, base_dir ? base_dir : "", &tab);
+    if (cfg.m.ch_model == CB_SINGLE_SITE_MWC) throw unsupported("per-site gating models are two-state models");
+    if (cfg.m.n_ions != h->d.m.n_ions || cfg.m.ca_idx != h->d.m.ca_idx || cfg.m.mg_idx != h->d.m.mg_idx)
+        throw std::runtime_error("the gating model's JSON names other ions than the handle's");
+    std::vector<cb_gate> gates(CB_MAX_GATES);
+    int n_gates = h->d.n_gates;
+    if (n_gates == 0) {  // gate 0: the handle's own model, every site on it
+        cb_gate& g = gates[0];
+        g.ch_model = h->d.m.ch_model;
+        for (int i = 0; i < CB_MAX_CHPAR; ++i) g.ch_par[i] = h->d.m.ch_par[i];
+        for (int w = 0; w < 2; ++w) {
+            g.sp_n[w] = h->d.m.sp_n[w];
+            g.spx[w] = h->d.spx[w];
+            g.spc[w] = h->d.spc[w];
+        }
+        h->d.gates = dalloc<cb_gate>(h, CB_MAX_GATES);
+        h->d.site_gate = dalloc<int>(h, (size_t)h->d.S);
+        ck(cudaMemsetAsync(h->d.site_gate, 0, sizeof(int) * (size_t)h->d.S, h->stream), "cudaMemset");
+        n_gates = 1;
+    } else {
+        ck(cudaMemcpy(gates.data(), h->d.gates, sizeof(cb_gate) * CB_MAX_GATES, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    }
+    if (n_gates >= CB_MAX_GATES) throw unsupported("at most " + std::to_string(CB_MAX_GATES - 1) + " extra gating models per handle");
+    cb_gate& g = gates[n_gates];
+    g.ch_model = cfg.m.ch_model;
+    for (int i = 0; i < CB_MAX_CHPAR; ++i) g.ch_par[i] = cfg.m.ch_par[i];
+    for (int w = 0; w < 2; ++w) {
+        g.sp_n[w] = cfg.m.sp_n[w];
+        g.spx[w] = cfg.sp_x[w].empty() ? nullptr : dupload(h, cfg.sp_x[w]);
+        g.spc[w] = cfg.sp_c[w].empty() ? nullptr : dupload(h, cfg.sp_c[w]);
+    }
+    ck(cudaMemcpy(h->d.gates, gates.data(), sizeof(cb_gate) * CB_MAX_GATES, cudaMemcpyHostToDevice), "cudaMemcpy");
+    ck(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    std::vector<int> idx(n);
+    for (int k = 0; k < n; ++k) idx[k] = n_gates;
+    for (int k = 0; k < n; ++k) ck(cudaMemcpy(h->d.site_gate + sites[k], &idx[k], sizeof(int), cudaMemcpyHostToDevice), "cudaMemcpy");
+    h->d.n_gates = n_gates + 1;
+    return CASIM_OK;
+    END_GUARD(h)
+}
+
 casim_status casim_b200_trace_enable(casim_h h, int64_t every_steps, int64_t max_samples) {
     GUARD(h)
     if (every_steps < 1 || max_samples < 1) throw std::runtime_error("trace needs every_steps >= 1 and max_samples >= 1");
@@ -750,6 +822,7 @@ casim_status casim_b200_sg_gate_steps(casim_h h, int64_t n) {
     if (n < 0) throw std::runtime_error("negative step count");
     if (h->d.m.cyto_type != CB_CYTO_POOL) throw std::runtime_error("surrogate gating needs the pool cytosol");
     if (h->d.m.ch_model == CB_SINGLE_SITE_MWC) throw std::runtime_error("surrogate gating serves two-state RyR models");
+    if (h->d.site_gate) throw unsupported("surrogate gating serves one gating model per batch");
     if (n > 0) ck(cb_sg_steps(h->d, n, h->stream), "surrogate steps");
     return CASIM_OK;
     END_GUARD(h)
@@ -842,6 +915,7 @@ void rd_steps(casim_h h, long long n) {
 
 casim_status casim_b200_sg_run(casim_h h, casim_sg net, int32_t max_channels, int64_t n, int32_t window, double ca_ref) {
     GUARD(h)
+    if (h->d.site_gate) throw unsupported("surrogate gating serves one gating model per batch");
     sg_windows(h, net, max_channels, n, window, ca_ref);
     return sg_net_status(h, net);
     END_GUARD(h)
@@ -851,6 +925,7 @@ casim_status casim_b200_sg_hybrid_run(casim_h h, casim_sg net, int32_t max_chann
                                       int32_t windows_per_check, int32_t rd_correction_steps, double tol, double max_fail_fraction,
                                       double ca_ref, casim_sg_hybrid_stats* stats) {
     GUARD(h)
+    if (h->d.site_gate) throw unsupported("surrogate gating serves one gating model per batch");
     if (windows_per_check < 1 || rd_correction_steps < 1 || !(tol > 0) || !(max_fail_fraction >= 0) || n < 0)
         throw std::runtime_error("bad hybrid run arguments");
     casim_sg_hybrid_stats st{};

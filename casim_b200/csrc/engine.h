@@ -57,6 +57,10 @@ struct cb_dev {
     int st_ntiles = 0;
     int st_nz = -1;
     unsigned* st_chcol = nullptr;  // bit per cleft column (node_base + x + nx*y): holds a RyR
+    // per-site gating models (plain path): gates[0] the batch's own, site_gate[s] the index
+    cb_gate* gates = nullptr;
+    int* site_gate = nullptr;
+    int n_gates = 0;
     unsigned long long* pre_jump = nullptr;  // k_pre_r: MRG32k3a jumps A^(2l), l < 32
 };
 
@@ -67,6 +71,8 @@ cudaError_t cb_plain_update(cb_dev& d, cudaStream_t st, long long* launches);
 cudaError_t cb_plain_step(cb_dev& d, long long n, cudaStream_t st, long long* launches);
 // whether the plain path's specialised streaming kernels serve the batch's layout
 bool cb_plain_streaming(cb_dev& d);
+// whether the warp-parallel gating kernel (the one that serves per-site models) runs
+bool cb_plain_gating_ready(cb_dev& d);
 // one plain time step with ev[0..4] recorded around its four kernels
 cudaError_t cb_plain_step_marked(cb_dev& d, cudaStream_t st, cudaEvent_t* ev);
 

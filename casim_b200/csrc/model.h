@@ -18,6 +18,17 @@
 enum { CB_SHEEP_CANNELL = 0, CB_TWO_STATE_MWC = 1, CB_TWO_STATE_AHTG = 2, CB_TWO_STATE_SPLINE = 3, CB_SINGLE_SITE_MWC = 4 };
 enum { CB_CYTO_POOL = 0, CB_CYTO_RD3D = 1 };
 
+// A two-state RyR gating model of some sites of a batch (per-site gating): the rate
+// law and its parameters as in cb_model, and its spline tables (device pointers).
+#define CB_MAX_GATES 8
+struct cb_gate {
+    int ch_model;
+    double ch_par[24];
+    int sp_n[2];
+    const double* spx[2];
+    const double* spc[2];
+};
+
 struct cb_model {
     int dim;  // 2 or 3
     double dx, dy, dz, z, R, dt, voltage;

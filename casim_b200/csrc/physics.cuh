@@ -43,8 +43,10 @@ __device__ __forceinline__ double cb_pow(double x, double e) {
 
 // MODEL >= 0 fixes the rate law at compile time (kernels instantiated per model);
 // the default reads it from m.ch_model.
-template <int MODEL = -1>
-__device__ __forceinline__ double cb_rate(const cb_model& m, const double* __restrict__ spx0, const double* __restrict__ spc0,
+// G: cb_model, or a cb_gate of a per-site gating model (the same ch_model, ch_par and
+// sp_n members).
+template <int MODEL = -1, typename G = cb_model>
+__device__ __forceinline__ double cb_rate(const G& m, const double* __restrict__ spx0, const double* __restrict__ spc0,
                                           const double* __restrict__ spx1, const double* __restrict__ spc1, int state, double ca,
                                           double mg) {
     const double* p = m.ch_par;

@@ -583,7 +583,10 @@ cudaError_t launch_step(cb_dev& d, cudaStream_t st, cudaEvent_t* ev = nullptr) {
     const bool fast = stream_tiles(d) > 0;
     if (fast && !d.mwc && pre_jump(d))
         stream::k_pre_r<<<(d.S + stream::PRE_WARPS - 1) / stream::PRE_WARPS, 32 * stream::PRE_WARPS, 0, st>>>(
-            d.m, d.S, d.NS, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0], d.spx[1], d.spc[1], d.pre_jump);
+            d.m, d.S, d.NS, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0], d.spx[1], d.spc[1], d.pre_jump, d.gates,
+            d.site_gate);
+    else if (d.site_gate)
+        return cudaErrorNotSupported;  // per-site models need k_pre_r
     else
         k_pre<<<(d.S + 127) / 128, 128, 0, st>>>(d.m, d.S, d.NS, d.sites, d.sc, d.ch_state, d.mouth, d.spx[0], d.spc[0],
                                                    d.spx[1], d.spc[1], d.ch_micro, d.mwc);
@@ -743,6 +746,8 @@ cudaError_t cb_plain_update(cb_dev& d, cudaStream_t st, long long* launches) {
 }
 
 bool cb_plain_streaming(cb_dev& d) { return stream_tiles(d) > 0; }
+
+bool cb_plain_gating_ready(cb_dev& d) { return stream_tiles(d) > 0 && !d.mwc && pre_jump(d); }
 
 cudaError_t cb_plain_step_marked(cb_dev& d, cudaStream_t st, cudaEvent_t* ev) {
     return d.precision == 0 ? launch_step<double>(d, st, ev) : launch_step<float>(d, st, ev);

@@ -594,14 +594,16 @@ __global__ void __launch_bounds__(UP_THREADS) k_update_s(const __grid_constant__
 // row l: A^(2l)), the lanes draw 32 consecutive values at a time (then jump by A^62,
 // row 31, to their draw of the next 32), and 32 RyRs are resolved per ballot, one more
 // ballot after each transition. The stream state left behind is that at the first
-// unused draw, as after the serial loop.
+// unused draw, as after the serial loop. With site_gate set, site s gates by
+// gates[site_gate[s]] (per-site gating models) instead of the batch's model.
 constexpr int PRE_WARPS = 4;
 __global__ void __launch_bounds__(32 * PRE_WARPS) k_pre_r(const __grid_constant__ cb_model m, int S, int NS,
                                                           const cb_site* __restrict__ sites, cb_site_scalars* __restrict__ sc,
                                                           int* __restrict__ ch_state, const double* __restrict__ mouth,
                                                           const double* __restrict__ spx0, const double* __restrict__ spc0,
                                                           const double* __restrict__ spx1, const double* __restrict__ spc1,
-                                                          const unsigned long long* __restrict__ J) {
+                                                          const unsigned long long* __restrict__ J, const cb_gate* __restrict__ gates,
+                                                          const int* __restrict__ site_gate) {
     __shared__ double s_u[PRE_WARPS][64];  // draws [we - 64, we), slot = draw & 63
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int s = blockIdx.x * PRE_WARPS + w;
@@ -630,7 +632,12 @@ __global__ void __launch_bounds__(32 * PRE_WARPS) k_pre_r(const __grid_constant_
             const double* mo = mouth + (long long)(st.ch_off + c) * NS;
             const double mg = m.mg_idx >= 0 ? mo[m.mg_idx] : 0.0;
             stt = ch_state[st.ch_off + c];
-            p = cb_rate(m, spx0, spc0, spx1, spc1, stt, mo[m.ca_idx], mg) * dt;
+            if (site_gate) {  // the site's own gating model
+                const cb_gate& g = gates[site_gate[s]];
+                p = cb_rate(g, g.spx[0], g.spc[0], g.spx[1], g.spc[1], stt, mo[m.ca_idx], mg) * dt;
+            } else {
+                p = cb_rate(m, spx0, spc0, spx1, spc1, stt, mo[m.ca_idx], mg) * dt;
+            }
         }
         int start = 0;
         while (start < cnt) {

@@ -233,6 +233,18 @@ casim_status casim_b200_path_note(casim_h h, char* buf, size_t n);
 casim_status casim_b200_last_step_ms(casim_h h, double* out);
 /* Number of kernel launches issued by the last casim_b200_step call. */
 casim_status casim_b200_last_step_launches(casim_h h, int64_t* out);
+/* Per-site RyR gating models (no counterpart in the reference, whose runs have one
+ * gating model): the sites listed gate by the two-state model of the "Dyad" /
+ * "Channels" / "RyR" block of json_text (a Parameters.json of the reference's schema
+ * naming the same ions; only its gating model is taken, spline tables and relative
+ * file names resolved against base_dir); the other sites keep their model. Up to 7
+ * models besides the handle's own; a later call moves the sites it lists again. For a
+ * parameter sweep over gating laws in one batch: the model is a per-site choice inside
+ * the warp-parallel gating kernel, everything else is shared. Served on the plain path
+ * with its specialised kernels (create the handle with CASIM_PATH_PLAIN);
+ * CASIM_EUNSUPPORTED on the resident path, for 60-state models, for layouts outside the
+ * specialised kernels, and afterwards for the surrogate gating entry points. */
+casim_status casim_b200_set_site_gating(casim_h h, const char* json_text, const char* base_dir, const int32_t* sites, int32_t n);
 /* Profiling (no counterpart in the reference): advance every site by one time step
  * like casim_b200_step(h, 1) and return the device time in ms of each of its kernels,
  * from CUDA events on the handle's stream. Plain path: ms[0..3] = RyR gating and pools,
