@@ -2,8 +2,10 @@
 Mg, half gated by the tetrameric MWC law (TwoStateMWC) and half by the same
 law tabulated for TwoStateSpline, run side by side on one GPU.
 
-A batch holds one gating model. By default each half is one batch on the path
-the library picks (a batch this large streams its fields from HBM). With
+By default (--path mixed) both halves are one batch, the second half's sites
+gated by their own law (casim_b200_set_site_gating). With --path auto each half
+is one batch on the path the library picks (a batch this large streams its
+fields from HBM). With
 --path split each half is ordered by size and split at the largest cleft side
 whose sites the resident path still takes (the largest sites with the second
 ion fit no 16-block cluster): the smaller sites run resident, the rest
@@ -65,10 +67,19 @@ def split_resident(params, sites, precision):
 
 
 def run_sweep(n_sites=16384, t_ms=0.2, chunk=200, precision="fp32", seed=5, path="auto"):
-    import torch
-    from scipy.stats import ks_2samp
     halves = configs.config5(n_sites=n_sites, seed=seed)
-    sims, streams, parts = [], [], []
+    sims, parts = [], []
+    if path == "mixed":
+        # one batch, the second half's sites gated by the second half's law
+        (p0, s0), (p1, s1) = halves
+        both = {k: (None if s0.get(k) is None else np.concatenate([np.asarray(s0[k]), np.asarray(s1[k])]))
+                for k in ("nx", "ny", "nz", "n_ch", "seeds", "jsr_init", "first_channel", "ch_x", "ch_y")}
+        sim = ReleaseSiteBatch(p0, both, precision=precision, path="plain")
+        n0 = len(s0["nx"])
+        sim.set_site_gating(p1, np.arange(n0, n0 + len(s1["nx"])))
+        halves_of = np.r_[np.zeros(n0, int), np.ones(len(s1["nx"]), int)]
+        return _run(sims=[sim], parts=[(None, both)], halves=halves, half_of=[halves_of], n_sites=n_sites, t_ms=t_ms,
+                    chunk=chunk, precision=precision)
     for h, (p, s) in enumerate(halves):
         # "auto": one batch per half and the library's choice (large 3D batches stream);
         # "split": the sites that fit a cluster resident, the rest streaming
@@ -78,12 +89,22 @@ def run_sweep(n_sites=16384, t_ms=0.2, chunk=200, precision="fp32", seed=5, path
                 continue
             sub = configs.subset_sites(s, idx)
             sim = ReleaseSiteBatch(p, sub, precision=precision, path=pth)
-            st = torch.cuda.Stream()
-            sim.set_stream(st.cuda_stream)
-            sim.start(sub["first_channel"])
             sims.append(sim)
-            streams.append(st)
             parts.append((h, sub))
+    return _run(sims, parts, halves, [np.full(sub_["nx"].size, h_, int) for h_, sub_ in parts], n_sites, t_ms, chunk, precision)
+
+
+def _run(sims, parts, halves, half_of, n_sites, t_ms, chunk, precision):
+    """Step the batches side by side on their own streams; half_of[b][k]: the half of
+    batch b's site k."""
+    import torch
+    from scipy.stats import ks_2samp
+    streams = []
+    for sim, (_, sub) in zip(sims, parts):
+        st = torch.cuda.Stream()
+        sim.set_stream(st.cuda_stream)
+        sim.start(sub["first_channel"])
+        streams.append(st)
     dt_ms = sims[0].info.dt_ms
     n_steps = int(round(t_ms / dt_ms))
     torch.cuda.synchronize()
@@ -107,15 +128,19 @@ def run_sweep(n_sites=16384, t_ms=0.2, chunk=200, precision="fp32", seed=5, path
     ms = ev0.elapsed_time(ev1)
     out = {"workload": "%d 3D dyads side~U{40..120}x3, 10..150 RyR, 25^3 RD cytosol, 1 mM Mg; "
                        "half TwoStateMWC, half TwoStateSpline (config 5)" % n_sites,
-           "precision": precision, "batches": [{"half": h, "sites": sim.S, "path": sim.path, "max_side": int(sub["nx"].max())}
+           "precision": precision, "batches": [{"half": h if h is not None else "both", "sites": sim.S, "path": sim.path,
+                                                "max_side": int(sub["nx"].max())}
                                                for sim, (h, sub) in zip(sims, parts)], "t_ms": n_steps * dt_ms,
            "device_ms": ms, "site_ms_per_s": n_sites * n_steps * dt_ms / (ms / 1e3), "gpu_launches": launches,
            "finite": [bool(sim.check_finite()[0]) for sim in sims], "halves": []}
     opens, rels = [[], []], [[], []]
-    for sim, (h, sub) in zip(sims, parts):
+    for sim, (_, sub), hof in zip(sims, parts, half_of):
         off = np.concatenate([[0], np.cumsum(sub["n_ch"])])
-        opens[h].append(np.add.reduceat(sim.all_states(), off[:-1]))
-        rels[h].append(np.array([sim.release(k) for k in range(sim.S)]))
+        o = np.add.reduceat(sim.all_states(), off[:-1])
+        r = np.array([sim.release(k) for k in range(sim.S)])
+        for h in (0, 1):
+            opens[h].append(o[hof == h])
+            rels[h].append(r[hof == h])
     opens = [np.concatenate(o) for o in opens]
     rels = [np.concatenate(r) for r in rels]
     for h, (p, _) in enumerate(halves):
@@ -133,7 +158,7 @@ def main():
     ap.add_argument("--sites", type=int, default=16384)
     ap.add_argument("--ms", type=float, default=0.2, help="simulated time per site")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--path", default="auto", choices=["auto", "split", "plain", "resident"])
+    ap.add_argument("--path", default="mixed", choices=["auto", "mixed", "split", "plain", "resident"])
     a = ap.parse_args()
     t0 = time.time()
     res = run_sweep(a.sites, a.ms, precision=a.precision, path=a.path)

@@ -43,7 +43,7 @@ def test_config5_halves_match_oracle(cuda_device, tmp_path, path, precision):
         sim.close()
 
 
-@pytest.mark.parametrize("path", ["auto", "split"])
+@pytest.mark.parametrize("path", ["auto", "split", "mixed"])
 def test_sweep_runner_small(cuda_device, path):
     from casim_b200.sweep import run_sweep
     res = run_sweep(n_sites=64, t_ms=0.02, chunk=100, path=path)
@@ -52,6 +52,10 @@ def test_sweep_runner_small(cuda_device, path):
     assert [h["model"] for h in res["halves"]] == ["TwoStateMWC", "TwoStateSpline"]
     # every site runs in exactly one batch; resident batches hold the smaller sites of their half
     assert sum(b["sites"] for b in res["batches"]) == 64
+    assert [h["sites"] for h in res["halves"]] == [32, 32]
+    if path == "mixed":
+        assert [b["half"] for b in res["batches"]] == ["both"]
+        return
     for half in (0, 1):
         bs = [b for b in res["batches"] if b["half"] == half]
         assert sum(b["sites"] for b in bs) == 32
