@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate-versus-RD report")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the mouth-Ca error check against FP64")
     ap.add_argument("--no-qs", action="store_true", help="skip the quasi-stationary (Gillespie) report")
+    ap.add_argument("--surrogate-frontier", action="store_true",
+                    help="print only the surrogate report over the tolerance frontier (one GPU)")
     return ap.parse_args()
 
 
@@ -274,7 +276,14 @@ def cpu_baseline(args, params, sites, budget_s):
                            "sample": "site 0 of the workload x %d time steps on 1 thread" % steps1}}
 
 
-def surrogate_report(sites=2048, sim_steps=20000, batches=8, train_steps=4000):
+# hybrid arms of the surrogate report: name -> (windows per check, RD correction steps,
+# residual tolerance, largest fraction of sites allowed above it)
+HYBRID_ARMS = {"hybrid_tol_1pct": (10, 20, 0.01, 0.0), "hybrid_tol_20pct": (10, 20, 0.2, 0.2)}
+# the tolerance frontier (--surrogate-frontier)
+FRONTIER_ARMS = {"tol_%g_fail_%g" % (t, f): (10, 20, t, f) for t in (0.01, 0.03, 0.1, 0.3) for f in (0.0, 0.2)}
+
+
+def surrogate_report(sites=2048, sim_steps=20000, batches=8, train_steps=4000, hybrid=None):
     """Surrogate-gated versus plain-RD release sites on config-1 geometry: the
     network is trained on the device from RD snapshots (frozen open sets), its
     held-out mouth-Ca error is measured, then the same sites (same seeds, one
@@ -300,7 +309,7 @@ def surrogate_report(sites=2048, sim_steps=20000, batches=8, train_steps=4000):
     p, s = configs.config1(n_sites=sites)
     first = np.random.default_rng(5).integers(0, 20, size=sites).astype(np.int32)
     out, stats = {}, {}
-    hybrid = {"hybrid_tol_1pct": (10, 20, 0.01, 0.0), "hybrid_tol_20pct": (10, 20, 0.2, 0.2)}
+    hybrid = HYBRID_ARMS if hybrid is None else hybrid
     for mode in ("rd", "surrogate") + tuple(hybrid):
         sim = cb.ReleaseSiteBatch(p, s, precision="fp32", path="auto")
         sim.start(first)
@@ -525,6 +534,9 @@ def main():
     args = parse()
     env_world = int(os.environ.get("WORLD_SIZE", "0"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.surrogate_frontier:
+        print(json.dumps(surrogate_report(hybrid=FRONTIER_ARMS)))
+        return 0
     if args.impl == "reference":
         # the reference's CPU classes on the host cores: rank 0 alone (the others exit 0)
         if rank == 0:
