@@ -481,7 +481,7 @@ bool pre_jump(cb_dev& d) {
 template <typename R, int NI, int NP, bool RD3D>
 cudaError_t launch_update_s(cb_dev& d, cudaStream_t st, bool after_step) {
     size_t smem = 8 * (NI + NP + NI) * sizeof(double);
-    if (RD3D) smem += (size_t)d.max_terms * (NI + NP) * sizeof(double);
+    if (RD3D) smem += (size_t)d.max_terms * (NI + NP) * sizeof(double) + sizeof(int) * ((size_t)d.m.mc * d.m.mc + 1 + d.max_terms);
     auto kern = stream::k_update_s<R, NI, NP, RD3D>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -489,7 +489,7 @@ cudaError_t launch_update_s(cb_dev& d, cudaStream_t st, bool after_step) {
     }
     kern<<<d.S, stream::UP_THREADS, smem, st>>>(d.m, d.NS, d.sites, (R*)d.fields[d.cur], (R*)d.curgrid, d.ch_node, d.ch_owner, d.ch_state,
                                                 d.mouth, d.sc, d.nc, (const R*)d.cyto[1 - d.ccur], d.cin, d.rim_cnode, d.dep_ptr,
-                                                d.dep_term, after_step ? (const R*)d.fields[1 - d.cur] : nullptr);
+                                                d.dep_term, after_step ? (const R*)d.fields[1 - d.cur] : nullptr, d.max_terms);
     return cudaGetLastError();
 }
 

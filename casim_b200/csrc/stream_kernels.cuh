@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(UP_THREADS) k_update_s(const __grid_constant__
                                                          double* __restrict__ mouth, cb_site_scalars* __restrict__ sc, int nc,
                                                          const R* __restrict__ cyto, double* __restrict__ cin,
                                                          const int* __restrict__ rim_cnode, const int* __restrict__ dep_ptr,
-                                                         const int* __restrict__ dep_term, const R* __restrict__ prev) {
+                                                         const int* __restrict__ dep_term, const R* __restrict__ prev, int max_terms) {
     constexpr int F = NI + NP;
     constexpr int CSM = NI + 4;  // cytosol species slots (ions + at most 4 pairs)
     const int CS = m.n_ions + m.c_n_pairs;
@@ -445,6 +445,20 @@ __global__ void __launch_bounds__(UP_THREADS) k_update_s(const __grid_constant__
     R* u = fld + st.node_base * F;
     const int nx = st.nx, ny = st.ny, nz = st.nz, nxy = nx * ny;
     const long long np = st.npad;
+    // RD3D: the site's deposit lists (per layer-0 cytosol node its efflux terms, in term
+    // order) staged in shared memory behind the terms, loaded here so that the loads
+    // overlap the phases before the deposit sums
+    const int zmax0 = nz == 1 ? 1 : nz - 1;
+    const int T0 = cb_efflux_terms(nx, ny, zmax0);
+    int* s_ptr = (int*)(terms + (size_t)max_terms * F);
+    int* s_term = s_ptr + (RD3D ? m.mc * m.mc + 1 : 0);
+    if (RD3D) {
+        const int mc2 = m.mc * m.mc;
+        const int* ptr = dep_ptr + (long long)s * (mc2 + 1);
+        for (int k = threadIdx.x; k <= mc2; k += UP_THREADS) s_ptr[k] = ptr[k];
+        const int* dtm = dep_term + st.term_off;
+        for (int k = threadIdx.x; k < T0; k += UP_THREADS) s_term[k] = dtm[k];
+    }
     // 1. mouth values: ions, pairs, free buffers (CaSim/DyadRD2DCPU.cpp:361-380). After
     // k_rd_s (prev set) the rim holds its Dirichlet values already; a RyR on the rim
     // reads the value the step carried over there, which is prev's
@@ -534,8 +548,8 @@ __global__ void __launch_bounds__(UP_THREADS) k_update_s(const __grid_constant__
     // 4. RD3D: deposit into the cytosol layer z = 0 in term order
     if (RD3D) {
         const int mc2 = m.mc * m.mc;
-        const int* ptr = dep_ptr + (long long)s * (mc2 + 1);
-        const int* dtm = dep_term + st.term_off;
+        const int* ptr = s_ptr;
+        const int* dtm = s_term;
         for (int cn = threadIdx.x; cn < mc2; cn += UP_THREADS) {
             const int lo = ptr[cn], hi = ptr[cn + 1];
             double acc[CSM];
