@@ -114,6 +114,7 @@ void build_device(casim_b200_sim* h, int precision) {
     d.precision = precision;
     d.min_cluster = cfg.min_cluster;
     d.light_rows = cfg.light_rows;
+    if (cfg.generic_kernels) d.st_nz = 0;  // the specialised streaming kernels stay off
     d.NS = cfg.m.F + cfg.m.n_buf;
     const size_t rs = precision == 0 ? sizeof(double) : sizeof(float);
     std::vector<cb_site> sites(d.S);

@@ -216,6 +216,9 @@ cb_config cb_parse_config(const std::string& json_text, const std::string& base_
         if (cfg.min_cluster != 1 && cfg.min_cluster != 2 && cfg.min_cluster != 4 && cfg.min_cluster != 8 && cfg.min_cluster != 16)
             fail("B200.MinClusterSize must be 1, 2, 4, 8 or 16");
     }
+    if (j.contains("B200") && j.at("B200").contains("GenericKernels")) {
+        cfg.generic_kernels = j.at("B200").at("GenericKernels").get<bool>() ? 1 : 0;
+    }
     if (j.contains("B200") && j.at("B200").contains("LightEdgeRows")) {
         cfg.light_rows = j.at("B200").at("LightEdgeRows").get<bool>() ? 1 : 0;
     }

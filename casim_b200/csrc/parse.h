@@ -23,6 +23,7 @@ struct cb_config {
     int num_batch = 1;
     int min_cluster = 1;  // "B200": {"MinClusterSize": C}: smallest cluster per site on the resident path
     int light_rows = 0;   // "B200": {"LightEdgeRows": true}: fewer rows on the edge and plane-0 blocks
+    int generic_kernels = 0;  // "B200": {"GenericKernels": true}: the plain path's generic kernels only
 };
 
 // Throws std::runtime_error with a readable message on any schema problem.
