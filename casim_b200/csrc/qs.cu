@@ -11,7 +11,9 @@
 // its share of the total rate, its transition; until no channel is open or
 // the time limit is reached.
 //
-// Device work: persistent warps, each taking the next scenario off a counter
+// Device work, sites of up to 32 RyRs: one scenario per lane (k_qs_lane, the open set a
+// bitmask in a register, the reference's operations in its order per lane). Larger
+// sites: persistent warps, each taking the next scenario off a counter
 // when its last one ends (event counts run from 1 to hundreds, so a static
 // warp-per-scenario grid idles behind its longest scenario). Per event, lanes
 // form the mouth Ca and the rate of one channel each (the Ca summed over the
@@ -247,7 +249,7 @@ __global__ void __launch_bounds__(32 * QS_WARPS) k_qs_run(cb_model m, int n_ch, 
         const int f0 = first[s];
         for (int w = lane; w < nw; w += 32) om[w] = w == (f0 >> 5) ? 1u << (f0 & 31) : 0u;
         if (lane == 0)
-            for (int i = 0; i <= n_ch; ++i) cbrng::u01d(g);
+            for (int i = 0; i <= n_ch; ++i) cbrng::u01d_fold(g);
         __syncwarp();
         double t = 0;
         int n_open = 1;
@@ -280,8 +282,8 @@ __global__ void __launch_bounds__(32 * QS_WARPS) k_qs_run(cb_model m, int n_ch, 
             if (lane == 0) {
                 // ParallelRng::rexp(1 / total): -log(runif()) * theta (CaSim/ParallelRng.cpp)
                 const double theta = 1 / total;
-                t += -log(cbrng::u01d(g)) * theta;
-                const double r = cbrng::u01d(g);
+                t += -log(cbrng::u01d_fold(g)) * theta;
+                const double r = cbrng::u01d_fold(g);
                 double p = 0;
                 int idx = 0;
                 for (int i = 0; i < n_ch; ++i) {
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(32 * QS_WARPS) k_qs_run(cb_model m, int n_ch, 
                     }
                     p += q;
                 }
-                cbrng::u01d(g);  // MakeTransition(runif()): a two-state channel flips
+                cbrng::u01d_fold(g);  // MakeTransition(runif()): a two-state channel flips
                 const unsigned bit = 1u << (idx & 31);
                 om[idx >> 5] ^= bit;
                 const int now = (om[idx >> 5] & bit) ? 1 : 0;
@@ -321,12 +323,121 @@ __global__ void __launch_bounds__(32 * QS_WARPS) k_qs_run(cb_model m, int n_ch, 
     }
 }
 
+// Sites of at most 32 RyRs: one scenario per lane. The open set is a bitmask in a
+// register; each event every running lane forms the mouth Ca of all RyRs (the increments
+// of the open RyRs in RyR order, a closed RyR adding +0 as the reference's 0 * increment
+// does), the rates (kept in shared memory, a column per lane), the total in RyR order,
+// the draws and the pick by shares rt[i] / total in order: the reference's operations
+// in its order, for 32 scenarios at once. Lanes take the next scenario off the counter
+// when theirs ends.
+constexpr int QSL_WARPS = 4;
+__host__ __device__ inline size_t qsl_smem(int n_ch) {
+    return sizeof(double) * ((size_t)n_ch * n_ch + (size_t)QSL_WARPS * 32 * n_ch);
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(32 * QSL_WARPS) k_qs_lane(cb_model m, int n_ch, const double* __restrict__ added, double bg, double mg,
+                                                            double max_time, int n_scen, const int* __restrict__ first,
+                                                            uint32_t* __restrict__ seeds, long long max_events,
+                                                            double* __restrict__ ev_t, int* __restrict__ ev_c,
+                                                            long long* __restrict__ nev, unsigned long long* __restrict__ draws,
+                                                            int* __restrict__ flags, int* __restrict__ next) {
+    extern __shared__ __align__(16) unsigned char qsl_raw[];
+    double* A = (double*)qsl_raw;  // [i][j]: the increments
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double* rt = A + (size_t)n_ch * n_ch + (size_t)wib * 32 * n_ch;  // [j][lane]
+    for (int k = threadIdx.x; k < n_ch * n_ch; k += blockDim.x) A[k] = added[k];
+    __syncthreads();
+    const long long cap = 64 * max_events;
+    int s = -1;
+    bool running = false;
+    cbrng::State g;
+    unsigned mask = 0;
+    int n_open = 0;
+    long long ne = 0;
+    double t = 0;
+    int overflow = 0;
+    double* et = nullptr;
+    int* ec = nullptr;
+    for (;;) {
+        if (!running) {
+            if (s >= 0) {
+                for (int i = 0; i < 6; ++i) seeds[6 * (size_t)s + i] = g.s[i];
+                nev[s] = ne;
+                draws[s] = (unsigned long long)n_ch + 1 + 3ull * ne;
+                flags[s] = overflow | (ne >= cap && n_open >= 1 && t < max_time ? 2 : 0);
+            }
+            s = atomicAdd(next, 1);
+            if (s >= n_scen) break;
+            for (int i = 0; i < 6; ++i) g.s[i] = seeds[6 * (size_t)s + i];
+            // every channel set closed (one draw each), then the first one opened (one more
+            // draw) (CaSim/QuasyStationaryReleaseSite.cpp:93-98)
+            for (int i = 0; i <= n_ch; ++i) cbrng::u01d_fold(g);
+            mask = 1u << first[s];
+            n_open = 1;
+            ne = 0;
+            t = 0;
+            overflow = 0;
+            et = ev_t + (size_t)s * max_events;
+            ec = ev_c + (size_t)s * max_events;
+            running = t < max_time;
+            if (!running) continue;
+        }
+        // four RyRs at a time: four independent sums (each in RyR order) keep the FP64
+        // pipeline busy; the total then adds the rates in RyR order
+        for (int j0 = 0; j0 < n_ch; j0 += 4) {
+            double c[4] = {0, 0, 0, 0};
+            for (int i = 0; i < n_ch; ++i) {
+                const bool on = (mask >> i) & 1u;
+                const double* a = A + i * n_ch + j0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (j0 + k < n_ch) c[k] += on ? a[k] : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (j0 + k < n_ch) {
+                    const int j = j0 + k;
+                    rt[j * 32 + lane] = cb_rate<MODEL>(m, nullptr, nullptr, nullptr, nullptr, (int)((mask >> j) & 1u), c[k] + bg, mg);
+                }
+        }
+        double total = 0;
+        for (int j = 0; j < n_ch; ++j) total += rt[j * 32 + lane];
+        // ParallelRng::rexp(1 / total): -log(runif()) * theta (CaSim/ParallelRng.cpp)
+        const double theta = 1 / total;
+        t += -log(cbrng::u01d_fold(g)) * theta;
+        const double r = cbrng::u01d_fold(g);
+        double p = 0;
+        int idx = 0;
+        for (int i = 0; i < n_ch; ++i) {
+            const double q = rt[i * 32 + lane] / total;
+            if (p <= r && r <= p + q) {
+                idx = i;
+                break;
+            }
+            p += q;
+        }
+        cbrng::u01d_fold(g);  // MakeTransition(runif()): a two-state channel flips
+        mask ^= 1u << idx;
+        const int now = (mask >> idx) & 1u;
+        n_open += now ? 1 : -1;
+        if (ne < max_events) {
+            et[ne] = t;
+            ec[ne] = idx | (now << 30);
+        } else {
+            overflow = 1;
+        }
+        ++ne;
+        running = n_open >= 1 && t < max_time && ne < cap;
+    }
+}
+
 using qs_kernel_t = decltype(&k_qs_run<0>);
-qs_kernel_t qs_kernel(int model) {
+qs_kernel_t qs_kernel(int model, bool lane) {
     switch (model) {
-    case CB_TWO_STATE_MWC: return k_qs_run<CB_TWO_STATE_MWC>;
-    case CB_TWO_STATE_AHTG: return k_qs_run<CB_TWO_STATE_AHTG>;
-    default: return k_qs_run<CB_SHEEP_CANNELL>;
+    case CB_TWO_STATE_MWC: return lane ? k_qs_lane<CB_TWO_STATE_MWC> : k_qs_run<CB_TWO_STATE_MWC>;
+    case CB_TWO_STATE_AHTG: return lane ? k_qs_lane<CB_TWO_STATE_AHTG> : k_qs_run<CB_TWO_STATE_AHTG>;
+    default: return lane ? k_qs_lane<CB_SHEEP_CANNELL> : k_qs_run<CB_SHEEP_CANNELL>;
     }
 }
 
@@ -538,8 +649,10 @@ casim_status casim_b200_qs_run(casim_qs h, const int32_t* first_channel) {
             ck(cudaMemcpy(h->d_seed, h->seeds.data(), sizeof(uint32_t) * 6 * S, cudaMemcpyHostToDevice), "cudaMemcpy");
         }
         ck(cudaMemcpyAsync(h->d_first, first_channel, sizeof(int) * h->n_scen, cudaMemcpyHostToDevice, h->stream), "cudaMemcpy");
-        const size_t smem = QS_WARPS * qs_warp_bytes(h->n_ch);
-        const qs_kernel_t kern = qs_kernel(h->m.ch_model);
+        // up to 32 RyRs: a scenario per lane; more: a scenario per warp
+        const bool lane = h->n_ch <= 32;
+        const size_t smem = lane ? qsl_smem(h->n_ch) : QS_WARPS * qs_warp_bytes(h->n_ch);
+        const qs_kernel_t kern = qs_kernel(h->m.ch_model, lane);
         if (smem > 48 * 1024) ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "cudaFuncSetAttribute");
         if (!h->grid) {
             int dev = 0, sms = 0, per_sm = 0;
@@ -548,7 +661,8 @@ casim_status casim_b200_qs_run(casim_qs h, const int32_t* first_channel) {
             ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * QS_WARPS, smem), "cudaOccupancy");
             h->grid = std::max(1, sms * per_sm);
         }
-        const int blocks = std::min(h->grid, (h->n_scen + QS_WARPS - 1) / QS_WARPS);
+        const int blocks = std::min(h->grid, lane ? (h->n_scen + 32 * QSL_WARPS - 1) / (32 * QSL_WARPS)
+                                                  : (h->n_scen + QS_WARPS - 1) / QS_WARPS);
         ck(cudaMemsetAsync(h->d_next, 0, sizeof(int), h->stream), "cudaMemsetAsync");
         ck(cudaEventRecord(h->ev0, h->stream), "cudaEventRecord");
         kern<<<blocks, 32 * QS_WARPS, smem, h->stream>>>(h->m, h->n_ch, h->d_added, h->bg, h->mg, h->max_time, h->n_scen, h->d_first,
