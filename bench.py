@@ -426,7 +426,7 @@ def qs_cpu_baseline(params, coords, added, budget_s):
             "sample": "%d scenarios on one stream, one thread: %s" % (done, what)}
 
 
-def qs_report(n_scen=262144, runs=3, cpu_budget_s=8.0):
+def qs_report(n_scen=1048576, runs=3, cpu_budget_s=8.0):
     """Quasi-stationary release sites (Gillespie gating, casim_b200.QuasiStationarySites)
     on the 20-RyR MWC site of configs.quasi_stationary: scenarios per second on the
     device (CUDA events around each run, inputs resident), against the reference's own

@@ -661,6 +661,8 @@ casim_status casim_b200_qs_run(casim_qs h, const int32_t* first_channel) {
             ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * QS_WARPS, smem), "cudaOccupancy");
             h->grid = std::max(1, sms * per_sm);
         }
+        // one scenario per lane: as many resident lanes as the batch fills (a warp runs until
+        // its longest scenario ends, so large batches, several scenarios per lane, balance best)
         const int blocks = std::min(h->grid, lane ? (h->n_scen + 32 * QSL_WARPS - 1) / (32 * QSL_WARPS)
                                                   : (h->n_scen + QS_WARPS - 1) / QS_WARPS);
         ck(cudaMemsetAsync(h->d_next, 0, sizeof(int), h->stream), "cudaMemsetAsync");
