@@ -88,3 +88,27 @@ def test_odd_batches_and_storage_limits(cuda_device, tmp_path):
     if capped:
         assert e.value.status == cb.ETIMEOUT
     q.close()
+
+
+def test_warp_kernel_for_large_sites(cuda_device, tmp_path):
+    """Sites of more than 32 RyRs run one scenario per warp (k_qs_run): a 40-RyR site
+    against the restatement, scenario by scenario."""
+    from casim_b200 import configs
+    p, coords = configs.quasi_stationary(40, seed=3, max_time=20.0)
+    np.savetxt(os.path.join(str(tmp_path), "coords.txt"), coords, fmt="%.17g")
+    S = 96
+    q = cb.QuasiStationarySites(p, S, base_dir=str(tmp_path), max_events=8192)
+    assert q.n_ch == 40
+    cfg = qs_oracle.parse(p, str(tmp_path))
+    added = q.increments()
+    seeds = qs_oracle.stream_seeds(S)
+    first = ((np.arange(S) * 11) % q.n_ch).astype(np.int32)
+    q.run(first)
+    for s in range(S):
+        t, c, st = q.events(s)
+        to, co, so, d, _ = qs_oracle.run(cfg, added, seeds[s], int(first[s]))
+        assert np.array_equal(c, co) and np.array_equal(st, so), s
+        assert q.draws(s) == d
+        if len(t):
+            assert np.max(np.abs(t - to) / np.abs(to)) <= 1e-12, s
+    q.close()
