@@ -274,3 +274,60 @@ class SurrogateGating:
                                                     int(rd_steps), float(tol), float(max_fail_fraction), CA_REF_UM,
                                                     ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in HybridStats._fields_}
+
+
+def data_parallel_train(grad_fn, params, X, Y, steps, batch=4096, lr=1e-3, seed=0, group=None):
+    """Data-parallel training over the ranks of a torch.distributed process group (NCCL
+    between GPUs, gloo on CPU; one rank when no group is initialised): every step all
+    ranks draw the same global mini-batch of `batch` rows of (X, Y), each takes its equal
+    share, grad_fn(params, x, y) -> (loss, flat gradients) gives the mean-square loss
+    gradient of that share (a Surrogate's `gradients` on the device, see
+    `device_grad_fn`), the shares' gradients are averaged by an all-reduce, and every
+    rank applies the same Adam step (beta 0.9 / 0.999, eps 1e-8) to its FP32 copy of
+    the parameters, which therefore stay identical on all ranks. Returns (params, the
+    averaged loss per step)."""
+    import torch
+    import torch.distributed as tdist
+    world = tdist.get_world_size(group) if tdist.is_available() and tdist.is_initialized() else 1
+    rank = tdist.get_rank(group) if world > 1 else 0
+    n = X.shape[0]
+    share = batch // world
+    if share < 1:
+        raise ValueError("batch smaller than the number of ranks")
+    p = np.array(params, dtype=np.float32, copy=True)
+    m = np.zeros_like(p)
+    v = np.zeros_like(p)
+    b1, b2, eps = 0.9, 0.999, 1e-8
+    hist = []
+    for k in range(steps):
+        idx = np.random.default_rng(seed + k).integers(0, n, size=share * world)
+        mine = idx[rank * share:(rank + 1) * share]
+        loss, g = grad_fn(p, X[mine], Y[mine])
+        buf = torch.from_numpy(np.concatenate([np.asarray(g, np.float32), np.float32([loss])]))
+        if world > 1:
+            tdist.all_reduce(buf, op=tdist.ReduceOp.SUM, group=group)
+            buf /= world
+        g = buf[:-1].numpy()
+        hist.append(float(buf[-1]))
+        m = b1 * m + (1 - b1) * g
+        v = b2 * v + (1 - b2) * g * g
+        mh = m / (1 - b1 ** (k + 1))
+        vh = v / (1 - b2 ** (k + 1))
+        p = (p - lr * mh / (np.sqrt(vh) + eps)).astype(np.float32)
+    return p, hist
+
+
+def device_grad_fn(net):
+    """grad_fn of data_parallel_train for a Surrogate on this rank's GPU: the parameters
+    and this rank's share of the batch go to the device, the gradients come back (the
+    device kernels take batches of a multiple of 128 rows, so each share must be one)."""
+    import torch
+
+    def fn(params, x, y):
+        if x.shape[0] % 128:
+            raise ValueError("each rank's share of the batch must be a multiple of 128 rows")
+        net.set_params(params)
+        xd = torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
+        yd = torch.from_numpy(np.ascontiguousarray(y, np.float32)).cuda()
+        return net.gradients(xd, yd)
+    return fn

@@ -83,6 +83,22 @@ def test_training_lowers_loss(cuda_device):
     net.close()
 
 
+def test_data_parallel_training_on_the_device(cuda_device):
+    """data_parallel_train with the device gradients (one rank here; the all-reduce over
+    ranks is tested on gloo): the loss falls and the parameters stay finite."""
+    n_in, n_out = 16, 8
+    rng = np.random.default_rng(3)
+    x = rng.uniform(-1, 1, size=(2048, n_in)).astype(np.float32)
+    w = rng.normal(size=(n_in, n_out)).astype(np.float32)
+    t = np.sin(x @ w).astype(np.float32)
+    net = sg.Surrogate(n_in, n_out, width=128, depth=3, seed=5)
+    p0 = net.get_params()
+    p, hist = sg.data_parallel_train(sg.device_grad_fn(net), p0, x, t, steps=150, batch=512, lr=1e-3, seed=1)
+    assert np.mean(hist[-10:]) < 0.6 * np.mean(hist[:10]), (hist[:10], hist[-10:])
+    assert np.all(np.isfinite(p))
+    net.close()
+
+
 def test_surrogate_learns_rd_snapshots_and_beats_rd_cost(cuda_device):
     """Snapshots of the plain RD method (frozen open sets, 0.25 ms relaxation)
     train the network on the device; on held-out sites it predicts the mouth
