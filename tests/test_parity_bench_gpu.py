@@ -4,8 +4,9 @@ CPU classes where the reference has a counterpart).
 
 * Config-2 sites taken from the bench workload itself (same generator and seed),
   sides from 45 to 120 nodes x 3 layers, up to 100 RyRs, the full 25^3 RD3D
-  cytosol: the resident path splits them over clusters of 4, 8 and 16 blocks,
-  the classes of the benchmark line. FP32 fields within 1e-5 relative at every
+  cytosol: the resident path splits them over clusters of 4, 8 and 16 blocks, and
+  the streaming path (the bench line's) runs them through its specialised
+  kernels. FP32 fields within 1e-5 relative at every
   node holding more than 1e-3 of its species' largest value, FP64 within 1e-11
   at every node, after 200 time steps (one bench step).
 * The exact config-1 geometry (64 x 64, 20 jittered RyRs, seeds [s]*6 for
@@ -93,14 +94,16 @@ def test_bench_sites_are_split_like_the_bench(cuda_device, oracle_snapshots):
         assert "clusters of %d " % c in note, note
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_bench_sites_match_oracle(cuda_device, oracle_snapshots, precision):
+@pytest.mark.parametrize("precision,path", [("fp32", "auto"), ("fp32", "plain"), ("fp64", "auto")])
+def test_bench_sites_match_oracle(cuda_device, oracle_snapshots, precision, path):
     """FP32: 1e-5 per node (above 1e-3 of the species' largest value) after one bench
-    step of 200 time steps, 1e-4 after 2000; FP64: 1e-11 at every node at both."""
+    step of 200 time steps, 1e-4 after 2000; FP64: 1e-11 at every node at both. FP32
+    runs both the resident kernel (AUTO for these seven sites) and the specialised
+    streaming kernels the full bench workload runs on."""
     params, sites, snaps, S = oracle_snapshots
-    sim = cb.ReleaseSiteBatch(params, sites, precision=precision, path="auto")
+    sim = cb.ReleaseSiteBatch(params, sites, precision=precision, path=path)
     if precision == "fp32":  # FP64 side-120 sites fit no 16-block cluster: the plain path
-        assert sim.path == "resident", sim.path_note()
+        assert sim.path == ("resident" if path == "auto" else "plain"), sim.path_note()
     sim.start(sites["first_channel"])
     done = 0
     for h in HORIZONS:
