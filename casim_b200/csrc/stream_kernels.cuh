@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(RD_THREADS, rd_min_blocks(sizeof(R), NI + NP))
 #pragma unroll
         for (int f = 0; f < F; ++f)
 #pragma unroll
-            for (int z = 0; z < NZ; ++z) o[f * np + col + z * nxy] = b[f];
+            for (int z = 0; z < NZ; ++z) __stcs(&o[f * np + col + z * nxy], b[f]);
     }
 }
 
@@ -179,10 +179,10 @@ __device__ __forceinline__ void interior_column(const cb_model& m, const cb_site
                 const R s2 = (R)m.K2[j] + val[j];
                 e *= sdiv((R)1, (R)1 + sdiv((R)(m.N1[j] * m.K1[j]), s1 * s1) + sdiv((R)(m.N2[j] * m.K2[j]), s2 * s2));
             }
-            o[j * np + n] = val[j] + e * dt;
+            __stcs(&o[j * np + n], val[j] + e * dt);
         }
 #pragma unroll
-        for (int p = 0; p < NP; ++p) o[(NI + p) * np + n] = val[NI + p] + evo[NI + p] * dt;
+        for (int p = 0; p < NP; ++p) __stcs(&o[(NI + p) * np + n], val[NI + p] + evo[NI + p] * dt);
     }
 }
 
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__((MC * MC + 31) / 32 * 32) k_cyto_m(const __gri
         const int n = k * MC2;
         if (bath) {
 #pragma unroll
-            for (int c = 0; c < CS; ++c) o[c * NC + n] = cu[c];
+            for (int c = 0; c < CS; ++c) __stcs(&o[c * NC + n], cu[c]);
         } else {
             R evo[CS];
 #pragma unroll
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__((MC * MC + 31) / 32 * 32) k_cyto_m(const __gri
             for (int c = 0; c < CS; ++c) {
                 R e = evo[c];
                 if (k == 0) e += (R)ci[c * MC2];
-                o[c * NC + n] = cu[c] + e * dt;
+                __stcs(&o[c * NC + n], cu[c] + e * dt);
             }
         }
 #pragma unroll
