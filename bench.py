@@ -161,8 +161,8 @@ class Clocks:
 # and stores every site once, so the traffic scales with the sites, not with the steps
 RESIDENT_DRAM_BYTES_PER_SITE = 319.7e6 / 512
 # ncu DRAM bytes (read + write) of one k_rd_s launch per cleft node (fp32, config-2 sites):
-# 129.4 MB + 82.6 MB on the 10 352 496 cleft nodes of 512 sites of this workload
-STREAM_CLEFT_DRAM_BYTES_PER_NODE = (129.430016e6 + 82.531840e6) / 10352496
+# 129.3 MB + 78.5 MB on the 10 352 496 cleft nodes of 512 sites of this workload
+STREAM_CLEFT_DRAM_BYTES_PER_NODE = (129.278464e6 + 78.518016e6) / 10352496
 
 
 def measured_peak_hbm():
